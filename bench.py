@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 path tracer on the single-large-scene workload.
+
+Workload (one "step" = one full frame): a seeded geodesic icosphere of
+frequency 229 (1,048,820 triangles) radially displaced by 4-octave value
+noise (amplitude 0.1), binned-SAH BVH, 64 metallic-roughness materials
+hashed per triangle, 8 procedural 2048^2 textures with full mips (RGBA16F
+atlas), 16 punctual lights, 512 emissive triangles, a 1024x512 analytic sky
+with a sun disk; 1920x1080, 64 spp, max_bounces 12. Synthetic data.
+
+metric: Msamples/s (camera paths per second, whole job). One process per
+GPU; with N > 1 every rank renders its own frame (seed = rank): weak
+scaling, no collective on the data path; the time is the max over ranks.
+
+The JSON line also carries:
+  e2e          the same metric through the C ABI with host buffers: per
+               step, upload of the flat scene buffers from pinned host
+               memory, tables and params, refine, resolve and the RGBA8
+               readback, all inside the timed region;
+  roofline     the trace kernel's algorithmic bytes (32 B per AABB tested,
+               48 B per triangle tested, 192 B of attributes and 544 B of
+               material record per shaded hit; counted by the counting build
+               of the kernel) per launch over its CUDA-event duration, against
+               the measured HBM copy bandwidth;
+  cpu_baseline the CPU oracle (the same estimator, C++, all host threads) on
+               a bounded sample of the same frame (N = 1, rank 0 only).
+`--impl reference` times that CPU implementation alone.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__  # noqa: E402
+
+BYTES_AABB, BYTES_TRI, BYTES_ATTR, BYTES_MAT = 32, 48, 192, 544
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--freq", type=int, default=229)
+    ap.add_argument("--tex", type=int, default=2048)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(pkg, a, seed=1):
+    scene = pkg.Scene.icosphere(freq=a.freq, seed=seed, n_materials=64, n_textures=8, tex_size=a.tex,
+                                n_punctual=16, n_emissive=512, material_mix=0)
+    env = pkg.EnvironmentMap.sky(1024, 512, sun_dir=(0.3, 0.8, -0.5), sun_radiance=2000.0)
+    return scene, env
+
+
+def options(pkg, a, seed=0, spp=None):
+    return pkg.RenderOptions(width=a.width, height=a.height, scene_camera=0,
+                             path_trace=pkg.PathTraceOptions(samples_per_pixel=spp or a.spp, max_bounces=12,
+                                                             rr_start=3, seed=seed))
+
+
+def config(a, n_gpus):
+    return {"workload": "single large scene, plain tracer", "triangles": 20 * a.freq * a.freq,
+            "materials": 64, "textures": f"8 x {a.tex}^2 RGBA16F + mips", "punctual_lights": 16,
+            "emissive_triangles": 512, "environment": "1024x512 RGBA32F sky + sun",
+            "resolution": f"{a.width}x{a.height}", "spp": a.spp, "max_bounces": 12,
+            "parallelism": f"replicas{n_gpus} (one frame per GPU)",
+            "l2": "inputs (0.6 GB of scene buffers) larger than L2; no flush between steps"}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(pkg, oracle, prep, a, budget_s: float):
+    """Oracle (same estimator, all host threads) on whole rows of the same
+    frame at the same spp, sized to about `budget_s` of CPU work."""
+    threads = os.cpu_count() or 1
+    h, w = a.height, a.width
+    probe_rows = 2
+    acc = np.zeros((h, w, 4), np.float32)
+    t0 = time.perf_counter()
+    oracle.dispatch(prep, prep.params, (0, 1, h // 2, probe_rows), acc, threads)
+    per_path = (time.perf_counter() - t0) / (probe_rows * w)
+    rows = int(max(1, min(h, budget_s / max(per_path * w * a.spp, 1e-9))))
+    spp = a.spp
+    if rows == 1 and per_path * w * a.spp > budget_s:
+        spp = max(1, int(budget_s / (per_path * w)))
+    y0 = max(0, h // 2 - rows // 2)
+    acc[:] = 0
+    t0 = time.perf_counter()
+    oracle.dispatch(prep, prep.params, (0, spp, y0, rows), acc, threads)
+    dt = time.perf_counter() - t0
+    paths = rows * w * spp
+    return {"value": paths / dt / 1e6, "unit": "Msamples/s", "cores": threads, "kind": "port",
+            "sample": f"rows {y0}..{y0 + rows - 1} of the {w}x{h} frame at {spp} spp ({paths} paths, {dt:.1f} s)"}
+
+
+def run_reference(a):
+    """--impl reference: the reference estimator's CPU restatement (the
+    reference's own CPU tracer is an external Rust crate that cannot be
+    built here) on all host threads, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pkg = __graft_entry__.load_package()
+    __graft_entry__.build()
+    import oracle
+    scene, env = workload(pkg, a)
+    prep = pkg.prepare(scene, options(pkg, a), env)
+    threads = os.cpu_count() or 1
+    h, w = a.height, a.width
+    acc = np.zeros((h, w, 4), np.float32)
+    t0 = time.perf_counter()
+    oracle.dispatch(prep, prep.params, (0, 1, h // 2, 2), acc, threads)
+    per_row = (time.perf_counter() - t0) / 2
+    rows = int(max(1, min(h, 4.0 / max(per_row, 1e-9))))
+    times = []
+    for i in range(a.warmup + a.steps):
+        acc[:] = 0
+        t0 = time.perf_counter()
+        oracle.dispatch(prep, prep.params, (0, 1, (i * rows) % (h - rows + 1), rows), acc, threads)
+        if i >= a.warmup:
+            times.append(time.perf_counter() - t0)
+    paths = rows * w
+    value = paths * len(times) / sum(times) / 1e6
+    line = {"metric": "Msamples/s", "value": value, "unit": "Msamples/s", "impl": "reference",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(a, 1),
+            "cpu_baseline": {"value": value, "unit": "Msamples/s", "cores": threads, "kind": "port",
+                             "sample": f"{rows} rows x {w} px x 1 spp per step"},
+            "e2e": {"value": value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    if rank == 0:
+        __graft_entry__.build()
+    if world > 1:
+        dist.barrier()
+    pkg = __graft_entry__.load_package()
+    L = pkg._native.lib()
+
+    scene, env = workload(pkg, a)
+    opts = options(pkg, a, seed=rank)
+    pt = pkg.GpuPathTracer(local)
+    stream = torch.cuda.Stream(device=local)
+    assert L.oxpt_set_stream(pt.ctx, C.c_void_p(stream.cuda_stream)) == 0
+    pt.set_environment(env)
+    pt.sync(scene, opts)
+    prep = pt.prepared()
+
+    # Algorithmic bytes per path from the counting build (untimed, 1 spp).
+    cnt = (C.c_uint64 * 8)()
+    assert L.oxpt_diag_refine_counted(pt.ctx, 1 << 20, 1, cnt) == 0
+    c = [int(x) for x in cnt]
+    bytes_per_path = (BYTES_AABB * c[3] + BYTES_TRI * c[5] + (BYTES_ATTR + BYTES_MAT) * c[6]) / max(c[0], 1)
+    rays_per_path = (c[1] + c[2]) / max(c[0], 1)
+
+    def step():
+        pt.reset()
+        pt.refine(a.spp)
+
+    for _ in range(a.warmup):
+        step()
+    pt.finish()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    L.oxpt_diag_set_timing(pt.ctx, 1)
+    L.oxpt_diag_timing(pt.ctx, None, None, None, None)
+    n0 = C.c_uint64()
+    L.oxpt_diag_launch_count(pt.ctx, C.byref(n0))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    tms, tn, rms, rn = C.c_double(), C.c_uint64(), C.c_double(), C.c_uint64()
+    L.oxpt_diag_timing(pt.ctx, C.byref(tms), C.byref(tn), C.byref(rms), C.byref(rn))
+    L.oxpt_diag_set_timing(pt.ctx, 0)
+    n1 = C.c_uint64()
+    L.oxpt_diag_launch_count(pt.ctx, C.byref(n1))
+    pt.finish()
+    t_max = elapsed
+    if world > 1:
+        t = torch.tensor([elapsed], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    paths_step = a.width * a.height * a.spp
+    value = world * a.steps * paths_step / t_max / 1e6
+
+    # Roofline of the trace kernel.
+    peak, peak_kind = measured_peak()
+    launch_ms = tms.value / max(tn.value, 1)
+    paths_per_launch = paths_step * a.steps / max(tn.value, 1)
+    achieved = bytes_per_path * paths_per_launch / (launch_ms / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "trace_paths_traffic.json"
+    if tf.exists():
+        td = json.loads(tf.read_text())
+        traffic = td.get("bytes_per_path", 0) * paths_per_launch if td.get("bytes_per_path") else None
+
+    # End to end through the C ABI with host buffers.
+    e2e = None
+    if not a.no_e2e:
+        e2e = e2e_measure(pkg, L, pt, prep, a, stream, torch, rank)
+        if world > 1:
+            t = torch.tensor([e2e["seconds"]], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e["seconds"] = float(t.item())
+        e2e = {"value": world * a.steps * paths_step / e2e["seconds"] / 1e6, "unit": "Msamples/s",
+               "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        import oracle
+        cpu = cpu_baseline(pkg, oracle, prep, a, a.cpu_seconds)
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {"metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config(a, world),
+                "mrays_per_s": value * rays_per_path,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic,
+                             "kernel": "trace_paths", "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_path": bytes_per_path, "launch_ms": launch_ms,
+                             "launches": int(tn.value), "reduce_ms_total": rms.value},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(n1.value - n0.value),
+                "clocks": clk.summary(), "rays_per_path": rays_per_path}
+        print(json.dumps(line), flush=True)
+    del pt
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank):
+    """Per step through the C ABI: H2D upload of the flat scene buffers
+    from pinned memory, tables, params, reset, refine, resolve and the
+    RGBA8 readback into pinned memory."""
+    N = pkg._native
+    pin = {k: torch.from_numpy(getattr(prep, k)).pin_memory() for k in ("geom", "attrs", "tables", "atlas")}
+    img = torch.empty((a.height, a.width, 4), dtype=torch.uint8).pin_memory()
+    desc = N.SceneDesc(pin["geom"].data_ptr(), prep.geom.size, pin["attrs"].data_ptr(), prep.attrs.size,
+                       pin["atlas"].data_ptr(), prep.atlas_side, prep.atlas_layers, prep.node_count, prep.slot_count)
+    params = prep.params
+    rp = pt.resolve_params(False)
+    ctx = pt.ctx
+    h2d = prep.geom.nbytes + prep.attrs.nbytes + prep.atlas.nbytes + prep.tables.nbytes
+    d2h = a.width * a.height * 4
+
+    def step(first):
+        assert L.oxpt_upload_scene(ctx, C.byref(desc)) == 0
+        assert L.oxpt_set_tables(ctx, C.c_void_p(pin["tables"].data_ptr()), prep.tables.size) == 0
+        assert L.oxpt_set_params(ctx, C.byref(params)) == 0
+        assert L.oxpt_reset(ctx) == 0
+        assert L.oxpt_refine(ctx, first, a.spp) == 0
+        rp.exposure[1] = float(a.spp)
+        assert L.oxpt_resolve(ctx, C.byref(rp), 0, C.c_void_p(img.data_ptr()), None) == 0
+
+    step(0)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(a.steps):
+        step(0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return {"seconds": ev0.elapsed_time(ev1) / 1e3, "h2d": h2d, "d2h": d2h}
+
+
+if __name__ == "__main__":
+    main()

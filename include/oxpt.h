@@ -1,0 +1,180 @@
+/*
+ * oxpt.h — C ABI of the B200 path tracer (the `-sys` layer).
+ *
+ * This is the surface a Rust `oxideav-render-cuda-sys` crate binds with
+ * `extern "C"` declarations. Everything the wgpu path tracer of
+ * OxideAV/oxideav-render-vulkan hands to wgpu (buffers, uniforms,
+ * dispatches, resolve passes and readbacks) crosses here as plain pointers
+ * and sizes. No C++ or torch types appear in any signature.
+ *
+ * Threading: an oxpt_ctx is used by one thread at a time (the reference's
+ * `&mut self` on every GpuPathTracer method). Distinct contexts may be used
+ * from distinct threads. All launches go to the context's CUDA stream and
+ * return without waiting, except the calls documented as blocking.
+ *
+ * Errors: every entry point returns an oxpt_status. A non-zero status
+ * leaves a message readable with oxpt_last_error(ctx). The Rust side maps
+ * OXPT_E_INVALID to Error::InvalidOptions and every other code to
+ * Error::Backend (the reference's error split, src/pathtrace.rs:252-273,
+ * 536-541, 567-576).
+ */
+#ifndef OXPT_H
+#define OXPT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OXPT_ABI_VERSION 1u
+
+typedef enum oxpt_status {
+    OXPT_OK = 0,
+    OXPT_E_NODEV = 1,   /* no CUDA device / wrong architecture */
+    OXPT_E_NOMEM = 2,   /* device allocation failed */
+    OXPT_E_LIMIT = 3,   /* a size exceeds a device or library limit */
+    OXPT_E_INVALID = 4, /* bad argument (null pointer, inconsistent sizes) */
+    OXPT_E_TIMEOUT = 5, /* a bounded device-side wait gave up */
+    OXPT_E_CUDA = 6     /* any other CUDA runtime error */
+} oxpt_status;
+
+typedef struct oxpt_ctx oxpt_ctx;
+
+/*
+ * Per-launch uniforms. Byte-for-byte the reference's `Params`
+ * (src/pathtrace.rs:100-114, pathtrace.wgsl:17-41): 11 x 16 bytes.
+ *   eye      xyz eye, w = 1 for orthographic
+ *   forward  xyz forward, w = half_w
+ *   side     xyz side, w = half_h
+ *   up       xyz up, w = pixel spread (cone width per unit distance)
+ *   dims     width, height, seed, max_bounces
+ *   cfg      rr_start, strategy (0 MIS, 1 light only, 2 BSDF only),
+ *            punctual light count, emissive triangle count
+ *   env      env width, env height, has env, BVH node count
+ *   offs0    table word offsets: sobol, sheen, materials, punctual lights
+ *   offs1    emissive lights, unused, env marginal, env conditional
+ *   offs2    env mass, env radiance, first triangle vec4 in geom, unused
+ *   fparams  ambient, clamp, P_env, unused
+ */
+typedef struct oxpt_params {
+    float eye[4];
+    float forward[4];
+    float side[4];
+    float up[4];
+    uint32_t dims[4];
+    uint32_t cfg[4];
+    uint32_t env[4];
+    uint32_t offs0[4];
+    uint32_t offs1[4];
+    uint32_t offs2[4];
+    float fparams[4];
+} oxpt_params;
+
+/* One dispatch: samples [first, first + count) of rows [y0, y0 + rows).
+ * The reference's `FrameParams` (src/pathtrace.rs:116-123). */
+typedef struct oxpt_frame {
+    uint32_t first;
+    uint32_t count;
+    uint32_t y0;
+    uint32_t rows;
+} oxpt_frame;
+
+/* Resolve uniforms: the reference's `ResolveParams` (src/pathtrace.rs:
+ * 125-131, 781-791; resolve.wgsl:18-26).
+ *   cfg        x = aa (1), y = class (3), z = tone map (0 clamp,
+ *              1 Reinhard, 2 ACES fitted), w = 1 for HDR output
+ *   exposure   x = exposure, y = samples taken, z = width
+ *   background sRGB-encoded background bytes / 255 */
+typedef struct oxpt_resolve_params {
+    uint32_t cfg[4];
+    float exposure[4];
+    float background[4];
+} oxpt_resolve_params;
+
+/*
+ * Flat scene buffers, in the layouts the reference's `upload` writes
+ * (src/pathtrace.rs:970-1239):
+ *   geom   BVH nodes (8 words each: lo.xyz, first, hi.xyz, count) followed
+ *          by the triangles in leaf-slot order (12 words each: p0.xyz,
+ *          global id, p1.xyz, emissive light index or 0xffffffff, p2.xyz,
+ *          material index). Float words are IEEE bit patterns.
+ *   attrs  48 floats per leaf slot (normals, tangents, uv0|uv1, colours;
+ *          w of the first normal = attribute flags bits).
+ *   atlas  RGBA16F texels, `atlas_layers` square layers of `atlas_side`^2,
+ *          layer-major then row-major, 4 halves per texel.
+ * The library copies everything; the caller may free its buffers when the
+ * call returns.
+ */
+typedef struct oxpt_scene_desc {
+    const uint32_t* geom;
+    size_t geom_words;
+    const float* attrs;
+    size_t attr_floats;
+    const uint16_t* atlas;
+    uint32_t atlas_side;
+    uint32_t atlas_layers;
+    uint32_t node_count;
+    uint32_t slot_count;
+} oxpt_scene_desc;
+
+/* A headless device image (the `draw_texture` result): device pointer,
+ * size and format. Valid until the next resize or destroy. */
+typedef enum oxpt_format { OXPT_FORMAT_RGBA8 = 0, OXPT_FORMAT_RGBA32F = 1 } oxpt_format;
+typedef struct oxpt_devimage {
+    void* data;
+    uint32_t width;
+    uint32_t height;
+    uint32_t pitch_bytes;
+    uint32_t format;
+} oxpt_devimage;
+
+/* ---- context (GpuPathTracer::new / from_device, src/pathtrace.rs:309-455) */
+uint32_t oxpt_abi_version(void);
+oxpt_status oxpt_create(int device, oxpt_ctx** out);
+oxpt_status oxpt_destroy(oxpt_ctx* ctx);
+const char* oxpt_last_error(const oxpt_ctx* ctx);
+/* Run on a caller's stream (a cudaStream_t passed as void*); NULL restores
+ * the context's own stream. */
+oxpt_status oxpt_set_stream(oxpt_ctx* ctx, void* stream);
+void* oxpt_get_stream(const oxpt_ctx* ctx);
+/* "<name> (sm_XX, N SMs, M MiB)" — adapter_summary (src/pathtrace.rs:464). */
+oxpt_status oxpt_device_summary(const oxpt_ctx* ctx, char* buf, size_t len);
+
+/* ---- scene + uniforms (upload, src/pathtrace.rs:970-1239; ensure_binding,
+ * :847-966). `oxpt_set_tables` takes the final word array: the scene
+ * tables with the environment words appended. */
+oxpt_status oxpt_upload_scene(oxpt_ctx* ctx, const oxpt_scene_desc* scene);
+oxpt_status oxpt_set_tables(oxpt_ctx* ctx, const uint32_t* words, size_t count);
+oxpt_status oxpt_set_params(oxpt_ctx* ctx, const oxpt_params* params);
+
+/* ---- accumulation (sync's accumulator, :551-564; reset, :495-502) */
+oxpt_status oxpt_resize(oxpt_ctx* ctx, uint32_t width, uint32_t height);
+oxpt_status oxpt_reset(oxpt_ctx* ctx);
+
+/* ---- tracing (refine, :584-671; trace_main, pathtrace.wgsl:2047-2073).
+ * oxpt_dispatch runs one frame exactly. oxpt_refine takes samples
+ * [first, first + count) of every row, scheduling launches itself.
+ * Both are asynchronous. */
+oxpt_status oxpt_dispatch(oxpt_ctx* ctx, const oxpt_frame* frame);
+oxpt_status oxpt_refine(oxpt_ctx* ctx, uint32_t first_sample, uint32_t count);
+/* Block until all queued work finished (finish, :674-679). */
+oxpt_status oxpt_finish(oxpt_ctx* ctx);
+
+/* ---- resolve (encode_resolve + image/hdr/draw_texture, :687-844;
+ * fs_resolve_pt, resolve.wgsl:151-188). Writes the device image; when
+ * `host_out` is non-null also copies it there (w*h*4 bytes for RGBA8,
+ * w*h*16 for RGBA32F) and blocks. `dev_out` (optional) receives the device
+ * image handle. */
+oxpt_status oxpt_resolve(oxpt_ctx* ctx, const oxpt_resolve_params* params, int hdr,
+                         void* host_out, oxpt_devimage* dev_out);
+
+/* Raw accumulator (w*h*4 floats: sum rgb over covered samples, covered
+ * count). Blocking. */
+oxpt_status oxpt_read_accum(oxpt_ctx* ctx, float* host_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OXPT_H */

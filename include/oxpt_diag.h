@@ -1,0 +1,79 @@
+/*
+ * oxpt_diag.h — diagnostic entry points of the B200 path tracer.
+ *
+ * These have no counterpart in the reference's FFI. They expose single
+ * stages of the device path (Sobol' generation, BVH ray queries, the
+ * portable transcendentals, traversal counters) so that the parity tests
+ * can compare each stage with the CPU oracle on its own. They run on the
+ * context's stream and block until their results are on the host.
+ */
+#ifndef OXPT_DIAG_H
+#define OXPT_DIAG_H
+
+#include "oxpt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*
+ * Owen-scrambled Sobol' points, pathtrace.wgsl:158-228 (make_sampler +
+ * pattern). For each i: sampler = make_sampler(seed, x[i], y[i], index[i]);
+ * out[4i..4i+3] = the four 32-bit scrambled values of pattern(sampler,
+ * pattern_id[i]) before `to_unit` (so both the integers and the floats
+ * `(v >> 8) * 2^-24` can be compared). `sobol_dirs` = 128 direction words.
+ */
+oxpt_status oxpt_diag_sobol(oxpt_ctx* ctx, const uint32_t* sobol_dirs, uint32_t seed, size_t n,
+                            const uint32_t* x, const uint32_t* y, const uint32_t* index,
+                            const uint32_t* pattern_id, uint32_t* out);
+
+/*
+ * BVH ray queries on the uploaded scene and tables (traverse,
+ * pathtrace.wgsl:646-735). rays[8i..8i+7] = o.xyz, t_max, d.xyz, skip
+ * (global triangle id bits, 0xffffffff = none). flags bit 0 = any-hit,
+ * bit 1 = primary (back-face culling of single-sided materials).
+ * Outputs per ray: slot (0xffffffff = miss), global id, t, barycentrics
+ * (3 floats). Any output pointer may be NULL.
+ */
+oxpt_status oxpt_diag_trace_rays(oxpt_ctx* ctx, size_t n, const float* rays, uint32_t flags,
+                                 uint32_t* slot, uint32_t* global_id, float* t, float* bary);
+
+/* Portable transcendental `op` (0 sin, 1 cos, 2 acos, 3 atan2(a, b),
+ * 4 exp, 5 log, 6 log2, 7 pow(a, b)) evaluated on the device. */
+oxpt_status oxpt_diag_math(oxpt_ctx* ctx, int op, size_t n, const float* a, const float* b,
+                           float* out);
+
+/*
+ * Run samples [first, first + count) of every row with the counting build
+ * of the trace kernel and return its totals: out[0] paths, out[1] path
+ * rays, out[2] shadow rays, out[3] AABBs slab-tested (the root, then two
+ * per inner node visited), out[4] leaves visited, out[5] triangle tests,
+ * out[6] shaded hits, out[7] stack pops. The accumulator is updated
+ * exactly as by oxpt_refine.
+ */
+oxpt_status oxpt_diag_refine_counted(oxpt_ctx* ctx, uint32_t first_sample, uint32_t count,
+                                     uint64_t out[8]);
+
+/*
+ * Kernel timing. While enabled, every trace and reduce launch is bracketed
+ * by CUDA events on the context's stream. oxpt_diag_timing synchronises the
+ * stream and returns (then clears) the summed device milliseconds and the
+ * number of launches of each kind since the last call.
+ */
+oxpt_status oxpt_diag_set_timing(oxpt_ctx* ctx, int enabled);
+oxpt_status oxpt_diag_timing(oxpt_ctx* ctx, double* trace_ms, uint64_t* trace_launches,
+                             double* reduce_ms, uint64_t* reduce_launches);
+
+/* Launch-shape override for tuning: threads per block and resident blocks
+ * per SM of the trace kernel (0 = library default), and the largest number
+ * of paths one launch may take. */
+oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t blocks_per_sm,
+                                 uint64_t max_paths_per_launch);
+
+/* Number of trace / reduce / resolve kernels launched by this context. */
+oxpt_status oxpt_diag_launch_count(const oxpt_ctx* ctx, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OXPT_DIAG_H */

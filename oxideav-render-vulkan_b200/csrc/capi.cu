@@ -1,0 +1,570 @@
+// C ABI of the path tracer (include/oxpt.h, include/oxpt_diag.h).
+//
+// One oxpt_ctx owns a CUDA stream and the device buffers that the
+// reference's GpuPathTracer owns through wgpu (src/pathtrace.rs:145-237):
+// geometry, attributes, tables, the texture atlas, the accumulator and the
+// output images. The launch schedule of oxpt_refine replaces the
+// reference's row tiles / sample runs of at most 2^20 paths
+// (src/pathtrace.rs:584-671): a B200 has no display watchdog, so a launch
+// takes up to `max_paths` paths, sized so that its per-path result buffer
+// stays L2-resident, and the persistent grid fills every SM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/oxpt.h"
+#include "../../include/oxpt_diag.h"
+#include "kernels.cuh"
+
+struct oxpt_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sms = 0;
+    // scene
+    float4* geom = nullptr;
+    size_t geom_vec4 = 0;
+    float4* attrs = nullptr;
+    size_t slot_count = 0;
+    uint2* atlas = nullptr;
+    uint32_t side = 1, layers = 1;
+    uint32_t node_count = 0;
+    uint32_t* tables = nullptr;
+    size_t table_words = 0;
+    oxpt_params params{};
+    bool has_scene = false, has_tables = false, has_params = false;
+    // accumulation + outputs
+    float4* accum = nullptr;
+    uint32_t w = 0, h = 0;
+    void* img8 = nullptr;
+    void* img32 = nullptr;
+    // per-launch path results
+    float4* out = nullptr;
+    uint64_t out_cap = 0;
+    // device words: error flags, counters
+    uint32_t* dev_err = nullptr;
+    unsigned long long* dev_counters = nullptr;
+    // launch shape
+    uint32_t threads = oxd::TRACE_THREADS;
+    uint32_t blocks_per_sm = 0;
+    uint64_t max_paths = 1ull << 22;
+    uint64_t launches = 0;
+    // optional per-launch event timing: {start, end, kind (0 trace, 1 reduce)}
+    bool timing = false;
+    struct Timed {
+        cudaEvent_t a, b;
+        int kind;
+    };
+    std::vector<Timed> timed;
+};
+
+namespace {
+
+oxpt_status fail(oxpt_ctx* c, oxpt_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+oxpt_status cuda_fail(oxpt_ctx* c, cudaError_t e, const char* what) {
+    (void)cudaGetLastError();
+    std::string m = std::string("cuda: ") + what + ": " + cudaGetErrorString(e);
+    return fail(c, e == cudaErrorMemoryAllocation ? OXPT_E_NOMEM : OXPT_E_CUDA, m);
+}
+
+#define CK(c, expr, what)                                  \
+    do {                                                   \
+        cudaError_t e_ = (expr);                           \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+    } while (0)
+
+template <class T>
+oxpt_status realloc_dev(oxpt_ctx* c, T** p, size_t bytes, const char* what) {
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (bytes == 0) return OXPT_OK;
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_fail(c, e, what);
+    }
+    return OXPT_OK;
+}
+
+oxd::Scene scene_view(const oxpt_ctx* c) {
+    oxd::Scene s;
+    s.geom = c->geom;
+    s.geom_vec4 = c->geom_vec4;
+    s.attrs = c->attrs;
+    s.slot_count = c->slot_count;
+    s.tables = c->tables;
+    s.table_words = c->table_words;
+    s.atlas = c->atlas;
+    s.side = c->side;
+    s.layers = c->layers;
+    s.P = c->params;
+    return s;
+}
+
+oxpt_status set_device(oxpt_ctx* c) {
+    CK(c, cudaSetDevice(c->device), "cudaSetDevice");
+    return OXPT_OK;
+}
+
+oxpt_status ready(oxpt_ctx* c) {
+    if (!c->has_scene || !c->has_tables || !c->has_params) return fail(c, OXPT_E_INVALID, "scene, tables and params must be set first");
+    if (!c->accum) return fail(c, OXPT_E_INVALID, "no accumulator: call oxpt_resize first");
+    if (c->params.dims[0] != c->w || c->params.dims[1] != c->h)
+        return fail(c, OXPT_E_INVALID, "params dims do not match the accumulator size");
+    return OXPT_OK;
+}
+
+oxpt_status ensure_out(oxpt_ctx* c, uint64_t paths) {
+    if (paths <= c->out_cap) return OXPT_OK;
+    oxpt_status s = realloc_dev(c, &c->out, paths * sizeof(float4), "path result buffer");
+    if (s != OXPT_OK) {
+        c->out_cap = 0;
+        return s;
+    }
+    c->out_cap = paths;
+    return OXPT_OK;
+}
+
+uint32_t trace_grid(oxpt_ctx* c, uint64_t total, bool count) {
+    uint32_t bpsm = c->blocks_per_sm;
+    if (bpsm == 0) bpsm = (uint32_t)std::max(1, oxd::trace_blocks_per_sm(c->threads, count));
+    uint64_t blocks = (uint64_t)c->sms * bpsm;
+    uint64_t need = (total + c->threads - 1) / c->threads;
+    return (uint32_t)std::max<uint64_t>(1, std::min(blocks, need));
+}
+
+// One dispatch = frame {first, count, y0, rows}, split into launches of at
+// most max_paths paths; each launch traces into `out` and reduces in
+// sample order.
+oxpt_status run_frame(oxpt_ctx* c, const oxpt_frame& f, bool count) {
+    if (f.count == 0 || f.rows == 0) return OXPT_OK;
+    if (f.y0 >= c->h || f.rows > c->h - f.y0) return fail(c, OXPT_E_INVALID, "frame rows outside the image");
+    uint64_t cap = std::max<uint64_t>(c->max_paths, c->w);
+    uint32_t rows_per = f.rows, per = f.count;
+    uint64_t row_paths = (uint64_t)c->w * f.rows;
+    if (row_paths > cap) {
+        rows_per = (uint32_t)std::max<uint64_t>(1, cap / c->w);
+        per = 1;
+    } else {
+        per = (uint32_t)std::min<uint64_t>(f.count, cap / row_paths);
+    }
+    oxpt_status st = ensure_out(c, (uint64_t)c->w * rows_per * per);
+    if (st != OXPT_OK) return st;
+    oxd::TraceArgs ta;
+    ta.s = scene_view(c);
+    ta.out = c->out;
+    ta.counters = c->dev_counters;
+    ta.err = c->dev_err;
+    for (uint32_t s0 = 0; s0 < f.count; s0 += per) {
+        uint32_t n = std::min(per, f.count - s0);
+        for (uint32_t r0 = 0; r0 < f.rows; r0 += rows_per) {
+            uint32_t rows = std::min(rows_per, f.rows - r0);
+            ta.first = f.first + s0;
+            ta.count = n;
+            ta.y0 = f.y0 + r0;
+            ta.rows = rows;
+            ta.npix = c->w * rows;
+            ta.total = (uint64_t)ta.npix * n;
+            oxpt_ctx::Timed tt{nullptr, nullptr, 0}, tr{nullptr, nullptr, 1};
+            if (c->timing) {
+                CK(c, cudaEventCreate(&tt.a), "event");
+                CK(c, cudaEventCreate(&tt.b), "event");
+                CK(c, cudaEventCreate(&tr.a), "event");
+                CK(c, cudaEventCreate(&tr.b), "event");
+                CK(c, cudaEventRecord(tt.a, c->stream), "event record");
+            }
+            CK(c, oxd::launch_trace(ta, count, trace_grid(c, ta.total, count), c->threads, c->stream), "trace launch");
+            if (c->timing) {
+                CK(c, cudaEventRecord(tt.b, c->stream), "event record");
+                CK(c, cudaEventRecord(tr.a, c->stream), "event record");
+            }
+            oxd::ReduceArgs ra{c->accum, c->out, c->w, ta.y0, ta.npix, n};
+            CK(c, oxd::launch_reduce(ra, c->stream), "reduce launch");
+            if (c->timing) {
+                CK(c, cudaEventRecord(tr.b, c->stream), "event record");
+                c->timed.push_back(tt);
+                c->timed.push_back(tr);
+            }
+            c->launches += 2;
+        }
+    }
+    return OXPT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t oxpt_abi_version(void) { return OXPT_ABI_VERSION; }
+
+oxpt_status oxpt_create(int device, oxpt_ctx** out) {
+    if (!out) return OXPT_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        return OXPT_E_NODEV;
+    }
+    if (device < 0 || device >= n) return OXPT_E_NODEV;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return OXPT_E_NODEV;
+    if (prop.major < 10) return OXPT_E_NODEV;  // built for sm_100a only
+    auto* c = new oxpt_ctx();
+    c->device = device;
+    c->sms = prop.multiProcessorCount;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc((void**)&c->dev_err, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc((void**)&c->dev_counters, sizeof(unsigned long long) * oxd::C_N) != cudaSuccess ||
+        cudaMemset(c->dev_err, 0, sizeof(uint32_t)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        oxpt_destroy(c);
+        return OXPT_E_CUDA;
+    }
+    c->stream = c->own;
+    *out = c;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_destroy(oxpt_ctx* c) {
+    if (!c) return OXPT_OK;
+    cudaSetDevice(c->device);
+    if (c->own) cudaStreamSynchronize(c->own);
+    if (c->stream && c->stream != c->own) cudaStreamSynchronize(c->stream);
+    for (auto& t : c->timed) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err, c->dev_counters};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->own) cudaStreamDestroy(c->own);
+    (void)cudaGetLastError();
+    delete c;
+    return OXPT_OK;
+}
+
+const char* oxpt_last_error(const oxpt_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+oxpt_status oxpt_set_stream(oxpt_ctx* c, void* stream) {
+    if (!c) return OXPT_E_INVALID;
+    c->stream = stream ? (cudaStream_t)stream : c->own;
+    return OXPT_OK;
+}
+
+void* oxpt_get_stream(const oxpt_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+oxpt_status oxpt_device_summary(const oxpt_ctx* c, char* buf, size_t len) {
+    if (!c || !buf || !len) return OXPT_E_INVALID;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return OXPT_E_CUDA;
+    std::snprintf(buf, len, "%s (sm_%d%d, %d SMs, %zu MiB)", prop.name, prop.major, prop.minor,
+                  prop.multiProcessorCount, (size_t)(prop.totalGlobalMem >> 20));
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
+    if (!c || !d) return fail(c, OXPT_E_INVALID, "null argument");
+    if (!d->geom || d->geom_words < 8 || d->geom_words % 4 != 0) return fail(c, OXPT_E_INVALID, "geom must hold at least one node (8 words), a multiple of 4 words");
+    if (!d->attrs || d->attr_floats < 48 || d->attr_floats % 48 != 0) return fail(c, OXPT_E_INVALID, "attrs must be 48 floats per slot");
+    if ((size_t)d->node_count * 8 + (size_t)d->slot_count * 12 > d->geom_words) return fail(c, OXPT_E_INVALID, "geom smaller than nodes + triangles");
+    if ((size_t)d->slot_count * 48 > d->attr_floats) return fail(c, OXPT_E_INVALID, "attrs smaller than the slot count");
+    if (!d->atlas || d->atlas_side == 0 || d->atlas_layers == 0) return fail(c, OXPT_E_INVALID, "atlas must have at least one layer");
+    if (d->atlas_side > 16384) return fail(c, OXPT_E_LIMIT, "atlas layer side above 16384");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before upload");
+    c->has_scene = false;
+    size_t gbytes = d->geom_words * 4, abytes = d->attr_floats * 4;
+    size_t tbytes = (size_t)d->atlas_side * d->atlas_side * d->atlas_layers * 8;
+    if ((s = realloc_dev(c, &c->geom, gbytes, "geom buffer"))) return s;
+    if ((s = realloc_dev(c, &c->attrs, abytes, "attribute buffer"))) return s;
+    if ((s = realloc_dev(c, &c->atlas, tbytes, "texture atlas"))) return s;
+    CK(c, cudaMemcpyAsync(c->geom, d->geom, gbytes, cudaMemcpyHostToDevice, c->stream), "geom upload");
+    CK(c, cudaMemcpyAsync(c->attrs, d->attrs, abytes, cudaMemcpyHostToDevice, c->stream), "attr upload");
+    CK(c, cudaMemcpyAsync(c->atlas, d->atlas, tbytes, cudaMemcpyHostToDevice, c->stream), "atlas upload");
+    CK(c, cudaStreamSynchronize(c->stream), "upload");
+    c->geom_vec4 = d->geom_words / 4;
+    c->slot_count = d->attr_floats / 48;
+    c->side = d->atlas_side;
+    c->layers = d->atlas_layers;
+    c->node_count = d->node_count;
+    c->has_scene = true;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_set_tables(oxpt_ctx* c, const uint32_t* words, size_t count) {
+    if (!c || !words || count == 0) return fail(c, OXPT_E_INVALID, "empty tables");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before tables");
+    c->has_tables = false;
+    if ((s = realloc_dev(c, &c->tables, count * 4, "tables"))) return s;
+    CK(c, cudaMemcpyAsync(c->tables, words, count * 4, cudaMemcpyHostToDevice, c->stream), "tables upload");
+    CK(c, cudaStreamSynchronize(c->stream), "tables upload");
+    c->table_words = count;
+    c->has_tables = true;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_set_params(oxpt_ctx* c, const oxpt_params* p) {
+    if (!c || !p) return fail(c, OXPT_E_INVALID, "null params");
+    if (c->has_scene && p->env[3] > c->node_count) return fail(c, OXPT_E_INVALID, "node count above the uploaded nodes");
+    if (p->env[2] && (p->env[0] == 0 || p->env[1] == 0)) return fail(c, OXPT_E_INVALID, "environment of zero size");
+    c->params = *p;
+    c->has_params = true;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_resize(oxpt_ctx* c, uint32_t w, uint32_t h) {
+    if (!c) return OXPT_E_INVALID;
+    if (w == 0 || h == 0) return fail(c, OXPT_E_INVALID, "zero-sized image");
+    if (w > 65536 || h > 65536) return fail(c, OXPT_E_LIMIT, "image side above 65536");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    if (c->accum && c->w == w && c->h == h) return OXPT_OK;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before resize");
+    size_t px = (size_t)w * h;
+    if ((s = realloc_dev(c, &c->accum, px * 16, "accumulator"))) return s;
+    if ((s = realloc_dev(c, &c->img8, px * 4, "RGBA8 output"))) return s;
+    if ((s = realloc_dev(c, &c->img32, px * 16, "RGBA32F output"))) return s;
+    c->w = w;
+    c->h = h;
+    CK(c, cudaMemsetAsync(c->accum, 0, px * 16, c->stream), "accumulator clear");
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_reset(oxpt_ctx* c) {
+    if (!c) return OXPT_E_INVALID;
+    if (!c->accum) return OXPT_OK;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaMemsetAsync(c->accum, 0, (size_t)c->w * c->h * 16, c->stream), "accumulator clear");
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_dispatch(oxpt_ctx* c, const oxpt_frame* f) {
+    if (!c || !f) return fail(c, OXPT_E_INVALID, "null frame");
+    oxpt_status s = ready(c);
+    if (s) return s;
+    if ((s = set_device(c))) return s;
+    return run_frame(c, *f, false);
+}
+
+oxpt_status oxpt_refine(oxpt_ctx* c, uint32_t first, uint32_t count) {
+    if (!c) return OXPT_E_INVALID;
+    oxpt_status s = ready(c);
+    if (s) return s;
+    if ((s = set_device(c))) return s;
+    if (count > 0xffffffffu - first) return fail(c, OXPT_E_INVALID, "sample index overflow");
+    oxpt_frame f{first, count, 0, c->h};
+    return run_frame(c, f, false);
+}
+
+oxpt_status oxpt_finish(oxpt_ctx* c) {
+    if (!c) return OXPT_E_INVALID;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "finish");
+    uint32_t e = 0;
+    CK(c, cudaMemcpy(&e, c->dev_err, 4, cudaMemcpyDeviceToHost), "error word");
+    if (e) {
+        cudaMemset(c->dev_err, 0, 4);
+        return fail(c, OXPT_E_LIMIT, "traversal exceeded the node count: malformed BVH");
+    }
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_resolve(oxpt_ctx* c, const oxpt_resolve_params* p, int hdr, void* host_out, oxpt_devimage* dev_out) {
+    if (!c || !p) return fail(c, OXPT_E_INVALID, "null resolve params");
+    if (!c->accum) return fail(c, OXPT_E_INVALID, "no accumulator: call oxpt_resize first");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    oxd::ResolveArgs ra;
+    ra.accum = c->accum;
+    ra.w = c->w;
+    ra.h = c->h;
+    ra.p = *p;
+    ra.hdr = hdr ? 1 : 0;
+    ra.out = hdr ? c->img32 : c->img8;
+    CK(c, oxd::launch_resolve(ra, c->stream), "resolve launch");
+    c->launches += 1;
+    size_t bytes = (size_t)c->w * c->h * (hdr ? 16 : 4);
+    if (dev_out) {
+        dev_out->data = ra.out;
+        dev_out->width = c->w;
+        dev_out->height = c->h;
+        dev_out->pitch_bytes = c->w * (hdr ? 16u : 4u);
+        dev_out->format = hdr ? OXPT_FORMAT_RGBA32F : OXPT_FORMAT_RGBA8;
+    }
+    if (host_out) {
+        CK(c, cudaMemcpyAsync(host_out, ra.out, bytes, cudaMemcpyDeviceToHost, c->stream), "readback");
+        CK(c, cudaStreamSynchronize(c->stream), "readback");
+    }
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_read_accum(oxpt_ctx* c, float* out) {
+    if (!c || !out) return fail(c, OXPT_E_INVALID, "null output");
+    if (!c->accum) return fail(c, OXPT_E_INVALID, "no accumulator");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaMemcpyAsync(out, c->accum, (size_t)c->w * c->h * 16, cudaMemcpyDeviceToHost, c->stream), "accum readback");
+    CK(c, cudaStreamSynchronize(c->stream), "accum readback");
+    return OXPT_OK;
+}
+
+// ---------------------------------------------------------------------
+// Diagnostics (oxpt_diag.h).
+// ---------------------------------------------------------------------
+
+oxpt_status oxpt_diag_sobol(oxpt_ctx* c, const uint32_t* dirs, uint32_t seed, size_t n, const uint32_t* x,
+                            const uint32_t* y, const uint32_t* index, const uint32_t* pattern_id, uint32_t* out) {
+    if (!c || !dirs || (n && (!x || !y || !index || !pattern_id || !out))) return fail(c, OXPT_E_INVALID, "null argument");
+    if (n == 0) return OXPT_OK;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    uint32_t* buf = nullptr;
+    size_t words = 128 + n * 4 + n * 4;
+    CK(c, cudaMalloc((void**)&buf, words * 4), "sobol buffers");
+    uint32_t *dd = buf, *dx = buf + 128, *dy = dx + n, *di = dy + n, *dp = di + n, *dout = dp + n;
+    cudaError_t e = cudaMemcpyAsync(dd, dirs, 512, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = cudaMemcpyAsync(dy, y, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = cudaMemcpyAsync(di, index, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = cudaMemcpyAsync(dp, pattern_id, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = oxd::launch_sobol(dd, seed, n, dx, dy, di, dp, dout, c->stream);
+    if (!e) e = cudaMemcpyAsync(out, dout, n * 16, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (e) return cuda_fail(c, e, "sobol");
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_trace_rays(oxpt_ctx* c, size_t n, const float* rays, uint32_t flags, uint32_t* slot,
+                                 uint32_t* gid, float* t, float* bary) {
+    if (!c || (n && !rays)) return fail(c, OXPT_E_INVALID, "null argument");
+    if (!c->has_scene || !c->has_tables || !c->has_params) return fail(c, OXPT_E_INVALID, "scene, tables and params must be set first");
+    if (n == 0) return OXPT_OK;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    char* buf = nullptr;
+    size_t bytes = n * (32 + 4 + 4 + 4 + 12);
+    CK(c, cudaMalloc((void**)&buf, bytes), "ray buffers");
+    float* dr = (float*)buf;
+    uint32_t* ds = (uint32_t*)(buf + n * 32);
+    uint32_t* dg = ds + n;
+    float* dt = (float*)(dg + n);
+    float* db = dt + n;
+    oxd::RayArgs ra;
+    ra.s = scene_view(c);
+    ra.n = n;
+    ra.rays = dr;
+    ra.flags = flags;
+    ra.slot = ds;
+    ra.gid = dg;
+    ra.t = dt;
+    ra.bary = db;
+    ra.counters = nullptr;
+    ra.err = c->dev_err;
+    cudaError_t e = cudaMemcpyAsync(dr, rays, n * 32, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = oxd::launch_rays(ra, c->stream);
+    if (!e && slot) e = cudaMemcpyAsync(slot, ds, n * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && gid) e = cudaMemcpyAsync(gid, dg, n * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && t) e = cudaMemcpyAsync(t, dt, n * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && bary) e = cudaMemcpyAsync(bary, db, n * 12, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (e) return cuda_fail(c, e, "trace rays");
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_math(oxpt_ctx* c, int op, size_t n, const float* a, const float* b, float* out) {
+    if (!c || (n && (!a || !out))) return fail(c, OXPT_E_INVALID, "null argument");
+    if (n == 0) return OXPT_OK;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    float* buf = nullptr;
+    CK(c, cudaMalloc((void**)&buf, n * 12), "math buffers");
+    float *da = buf, *db = buf + n, *dout = buf + 2 * n;
+    cudaError_t e = cudaMemcpyAsync(da, a, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!e && b) e = cudaMemcpyAsync(db, b, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!e) e = oxd::launch_math(op, n, da, b ? db : nullptr, dout, c->stream);
+    if (!e) e = cudaMemcpyAsync(out, dout, n * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (e) return cuda_fail(c, e, "math");
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_refine_counted(oxpt_ctx* c, uint32_t first, uint32_t count, uint64_t out[8]) {
+    if (!c || !out) return fail(c, OXPT_E_INVALID, "null argument");
+    oxpt_status s = ready(c);
+    if (s) return s;
+    if ((s = set_device(c))) return s;
+    CK(c, cudaMemsetAsync(c->dev_counters, 0, sizeof(unsigned long long) * oxd::C_N, c->stream), "counter clear");
+    oxpt_frame f{first, count, 0, c->h};
+    if ((s = run_frame(c, f, true))) return s;
+    unsigned long long host[oxd::C_N];
+    CK(c, cudaMemcpyAsync(host, c->dev_counters, sizeof(host), cudaMemcpyDeviceToHost, c->stream), "counters");
+    CK(c, cudaStreamSynchronize(c->stream), "counters");
+    for (int k = 0; k < 8; k++) out[k] = k < oxd::C_N ? host[k] : 0;
+    return oxpt_finish(c);
+}
+
+oxpt_status oxpt_diag_set_launch(oxpt_ctx* c, uint32_t threads, uint32_t blocks_per_sm, uint64_t max_paths) {
+    if (!c) return OXPT_E_INVALID;
+    if (threads && (threads % 32 != 0 || threads > oxd::TRACE_THREADS))
+        return fail(c, OXPT_E_INVALID, "threads must be a multiple of 32 and at most the kernel's block bound");
+    c->threads = threads ? threads : oxd::TRACE_THREADS;
+    c->blocks_per_sm = blocks_per_sm;
+    c->max_paths = max_paths ? max_paths : (1ull << 22);
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_set_timing(oxpt_ctx* c, int enabled) {
+    if (!c) return OXPT_E_INVALID;
+    c->timing = enabled != 0;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_timing(oxpt_ctx* c, double* trace_ms, uint64_t* trace_n, double* reduce_ms, uint64_t* reduce_n) {
+    if (!c) return OXPT_E_INVALID;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "timing sync");
+    double ms[2] = {0.0, 0.0};
+    uint64_t n[2] = {0, 0};
+    for (auto& t : c->timed) {
+        float e = 0.0f;
+        cudaEventElapsedTime(&e, t.a, t.b);
+        ms[t.kind] += e;
+        n[t.kind] += 1;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    c->timed.clear();
+    if (trace_ms) *trace_ms = ms[0];
+    if (trace_n) *trace_n = n[0];
+    if (reduce_ms) *reduce_ms = ms[1];
+    if (reduce_n) *reduce_n = n[1];
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_launch_count(const oxpt_ctx* c, uint64_t* out) {
+    if (!c || !out) return OXPT_E_INVALID;
+    *out = c->launches;
+    return OXPT_OK;
+}
+
+}  // extern "C"
