@@ -174,6 +174,11 @@ oxpt_status oxpt_resolve(oxpt_ctx* ctx, const oxpt_resolve_params* params, int h
  * count). Blocking. */
 oxpt_status oxpt_read_accum(oxpt_ctx* ctx, float* host_out);
 
+/* The accumulator itself as a device image (RGBA32F, read-write), for
+ * gathering the row tiles of a frame split across GPUs with a collective
+ * that writes into it. No counterpart in the reference (single device). */
+oxpt_status oxpt_accum_view(oxpt_ctx* ctx, oxpt_devimage* out);
+
 #ifdef __cplusplus
 }
 #endif

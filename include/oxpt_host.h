@@ -216,6 +216,10 @@ void oxpt_tracer_size(const oxpt_tracer* t, uint32_t* w, uint32_t* h);
 oxpt_status oxpt_tracer_sync(oxpt_tracer* t, const oxpt_scene* scene,
                              const oxpt_render_options* opts, int* did_reset);
 oxpt_status oxpt_tracer_refine(oxpt_tracer* t, uint32_t samples);
+/* refine() restricted to rows [y0, y0 + rows): the per-GPU share of a
+ * frame split by row tiles across GPUs (sample indices and the samples()
+ * count advance exactly as for refine). */
+oxpt_status oxpt_tracer_refine_rows(oxpt_tracer* t, uint32_t samples, uint32_t y0, uint32_t rows);
 oxpt_status oxpt_tracer_finish(oxpt_tracer* t);
 /* w*h*4 bytes (RGBA8, sRGB-encoded). */
 oxpt_status oxpt_tracer_image(oxpt_tracer* t, uint8_t* out);

@@ -110,6 +110,7 @@ _SIGS = {
     "oxpt_finish": (cint, [vp]),
     "oxpt_resolve": (cint, [vp, C.POINTER(ResolveParams), cint, vp, C.POINTER(DevImage)]),
     "oxpt_read_accum": (cint, [vp, vp]),
+    "oxpt_accum_view": (cint, [vp, C.POINTER(DevImage)]),
     # oxpt_diag.h
     "oxpt_diag_sobol": (cint, [vp, vp, u32, sz, vp, vp, vp, vp, vp]),
     "oxpt_diag_trace_rays": (cint, [vp, sz, vp, u32, vp, vp, vp, vp]),
@@ -153,6 +154,7 @@ _SIGS = {
     "oxpt_tracer_size": (None, [vp, C.POINTER(u32), C.POINTER(u32)]),
     "oxpt_tracer_sync": (cint, [vp, vp, C.POINTER(RenderOptions), C.POINTER(cint)]),
     "oxpt_tracer_refine": (cint, [vp, u32]),
+    "oxpt_tracer_refine_rows": (cint, [vp, u32, u32, u32]),
     "oxpt_tracer_finish": (cint, [vp]),
     "oxpt_tracer_image": (cint, [vp, vp]),
     "oxpt_tracer_hdr": (cint, [vp, vp]),

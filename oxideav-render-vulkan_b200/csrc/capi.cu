@@ -424,6 +424,17 @@ oxpt_status oxpt_read_accum(oxpt_ctx* c, float* out) {
     return OXPT_OK;
 }
 
+oxpt_status oxpt_accum_view(oxpt_ctx* c, oxpt_devimage* out) {
+    if (!c || !out) return fail(c, OXPT_E_INVALID, "null output");
+    if (!c->accum) return fail(c, OXPT_E_INVALID, "no accumulator");
+    out->data = c->accum;
+    out->width = c->w;
+    out->height = c->h;
+    out->pitch_bytes = c->w * 16u;
+    out->format = OXPT_FORMAT_RGBA32F;
+    return OXPT_OK;
+}
+
 // ---------------------------------------------------------------------
 // Diagnostics (oxpt_diag.h).
 // ---------------------------------------------------------------------

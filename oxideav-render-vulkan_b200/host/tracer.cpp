@@ -144,13 +144,19 @@ struct oxpt_tracer {
         return OXPT_OK;
     }
 
-    oxpt_status refine(uint32_t n) {
+    oxpt_status refine(uint32_t n) { return refine_rows(n, 0, h); }
+
+    oxpt_status refine_rows(uint32_t n, uint32_t y0, uint32_t rows) {
         if (!scene || n == 0) return OXPT_OK;
+        if (y0 > h || rows > h - y0) return fail(OXPT_E_INVALID, "row range outside the image");
         n = std::min(n, 0xffffffffu - samples);
         oxpt_status st = ensure_binding();
         if (st) return st;
-        st = check(oxpt_refine(ctx, samples, n));
-        if (st) return st;
+        if (rows > 0) {
+            oxpt_frame f{samples, n, y0, rows};
+            st = check(oxpt_dispatch(ctx, &f));
+            if (st) return st;
+        }
         samples += n;
         return OXPT_OK;
     }
@@ -231,6 +237,9 @@ oxpt_status oxpt_tracer_sync(oxpt_tracer* t, const oxpt_scene* scene, const oxpt
 }
 
 oxpt_status oxpt_tracer_refine(oxpt_tracer* t, uint32_t n) { return t->refine(n); }
+oxpt_status oxpt_tracer_refine_rows(oxpt_tracer* t, uint32_t n, uint32_t y0, uint32_t rows) {
+    return t->refine_rows(n, y0, rows);
+}
 oxpt_status oxpt_tracer_finish(oxpt_tracer* t) { return t->check(oxpt_finish(t->ctx)); }
 oxpt_status oxpt_tracer_image(oxpt_tracer* t, uint8_t* out) { return t->resolve(false, out, nullptr); }
 oxpt_status oxpt_tracer_hdr(oxpt_tracer* t, float* out) { return t->resolve(true, out, nullptr); }

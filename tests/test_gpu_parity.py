@@ -137,10 +137,8 @@ def test_closest_hit_ids_on_a_million_rays(pkg, oracle, which):
         assert np.array_equal(bary[same].view(np.uint32), obary[same].view(np.uint32))
 
 
-def _accum_parity(pkg, oracle, scene, opts, spp, env=None, env_gpu=None, splits=(None,)):
+def _accum_parity(pkg, oracle, scene, opts, spp, env_gpu=None):
     t = _tracer(pkg, scene, opts, env_gpu)
-    for s in splits:
-        pass
     t.refine(spp)
     t.finish()
     gpu = t.read_accum()
@@ -203,10 +201,10 @@ def test_images_vs_libm_oracle_psnr_at_least_60db(pkg, oracle):
 def test_traversal_counters_match_oracle(pkg, oracle):
     opts = _opts(pkg, 48, 32, 4)
     t = _tracer(pkg, scenes.materials_scene(pkg), opts)
+    p = t.prepared()  # binds tables and params on the context
     out = (C.c_uint64 * 8)()
     st = pkg._native.lib().oxpt_diag_refine_counted(t.ctx, 0, 4, out)
     assert st == 0
-    p = t.prepared()
     cpu, cnt = oracle.render(p, 4)
     assert list(out) == [int(c) for c in cnt]
     assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
