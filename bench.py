@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="auto", choices=["auto", "mega", "wave"],
+                    help="execution plan; auto = the library default")
+    ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
     return ap.parse_args()
 
 
@@ -149,10 +152,10 @@ def cpu_baseline(pkg, oracle, prep, a, budget_s: float):
     frame at the same spp, sized to about `budget_s` of CPU work."""
     threads = os.cpu_count() or 1
     h, w = a.height, a.width
-    probe_rows = 2
+    probe_rows = min(h, max(16, 2 * threads))
     acc = np.zeros((h, w, 4), np.float32)
     t0 = time.perf_counter()
-    oracle.dispatch(prep, prep.params, (0, 1, h // 2, probe_rows), acc, threads)
+    oracle.dispatch(prep, prep.params, (0, 1, (h - probe_rows) // 2, probe_rows), acc, threads)
     per_path = (time.perf_counter() - t0) / (probe_rows * w)
     rows = int(max(1, min(h, budget_s / max(per_path * w * a.spp, 1e-9))))
     spp = a.spp
@@ -236,6 +239,11 @@ def main():
     assert L.oxpt_set_stream(pt.ctx, C.c_void_p(stream.cuda_stream)) == 0
     pt.set_environment(env)
     pt.sync(scene, opts)
+    if a.mode != "auto" or a.slots:
+        kw = {"wave_slots": a.slots} if a.slots else {}
+        if a.mode != "auto":
+            kw["mode"] = 0 if a.mode == "mega" else 1
+        pt.set_tuning(**kw)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp).
@@ -323,7 +331,8 @@ def main():
                              "algorithmic_bytes_per_path": bytes_per_path, "launch_ms": launch_ms,
                              "launches": int(tn.value), "reduce_ms_total": rms.value},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(n1.value - n0.value),
-                "clocks": clk.summary(), "rays_per_path": rays_per_path}
+                "clocks": clk.summary(), "rays_per_path": rays_per_path,
+                "plan": {"mode": ["megakernel", "wavefront"][pt.tuning().mode], "wave_slots": pt.tuning().wave_slots}}
         print(json.dumps(line), flush=True)
     del pt
     if world > 1:

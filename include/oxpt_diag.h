@@ -65,10 +65,38 @@ oxpt_status oxpt_diag_timing(oxpt_ctx* ctx, double* trace_ms, uint64_t* trace_la
                              double* reduce_ms, uint64_t* reduce_launches);
 
 /* Launch-shape override for tuning: threads per block and resident blocks
- * per SM of the trace kernel (0 = library default), and the largest number
- * of paths one launch may take. */
+ * per SM of the megakernel (0 = library default), and the largest number
+ * of paths one launch may take (both execution modes). */
 oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t blocks_per_sm,
                                  uint64_t max_paths_per_launch);
+
+/*
+ * Execution plan of a context, chosen by the autotuner (tuner.py) or left
+ * at the defaults. Every plan produces bit-identical accumulators; only
+ * speed differs.
+ *   mode           OXPT_MODE_MEGAKERNEL: one persistent kernel runs whole
+ *                  paths; OXPT_MODE_WAVEFRONT: path state in HBM, one
+ *                  shading launch and two traversal launches per bounce.
+ *   threads, blocks_per_sm, max_paths   megakernel launch shape.
+ *   wave_slots     paths in flight (wavefront); wave_items its paths per
+ *                  launch; check_every its bounces between completion
+ *                  checks.
+ */
+enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1 };
+typedef struct oxpt_tuning {
+    uint32_t mode;
+    uint32_t threads;
+    uint32_t blocks_per_sm;
+    uint32_t wave_slots;
+    uint64_t max_paths;
+    uint64_t wave_items;
+    uint32_t check_every;
+    uint32_t reserved;
+} oxpt_tuning;
+oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
+oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);
+/* Wavefront bounces (logic + extend + shadow launches) run so far. */
+oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* ctx, uint64_t* out);
 
 /* Number of trace / reduce / resolve kernels launched by this context. */
 oxpt_status oxpt_diag_launch_count(const oxpt_ctx* ctx, uint64_t* out);

@@ -88,6 +88,13 @@ class PreparedView(C.Structure):
                 ("params", Params), ("bvh_depth", u32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("mode", u32), ("threads", u32), ("blocks_per_sm", u32), ("wave_slots", u32),
+                ("max_paths", u64), ("wave_items", u64), ("check_every", u32), ("reserved", u32)]
+
+
+MODE_MEGAKERNEL, MODE_WAVEFRONT = 0, 1
+
 assert C.sizeof(Params) == 176
 assert C.sizeof(ResolveParams) == 48
 
@@ -119,6 +126,9 @@ _SIGS = {
     "oxpt_diag_set_launch": (cint, [vp, u32, u32, u64]),
     "oxpt_diag_launch_count": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_set_timing": (cint, [vp, cint]),
+    "oxpt_set_tuning": (cint, [vp, C.POINTER(Tuning)]),
+    "oxpt_get_tuning": (cint, [vp, C.POINTER(Tuning)]),
+    "oxpt_diag_wave_iterations": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_timing": (cint, [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(u64)]),
     # oxpt_host.h
     "oxpt_material_default": (None, [C.POINTER(Material)]),

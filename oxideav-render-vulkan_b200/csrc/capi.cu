@@ -19,6 +19,7 @@
 #include "../../include/oxpt.h"
 #include "../../include/oxpt_diag.h"
 #include "kernels.cuh"
+#include "wavefront.cuh"
 
 struct oxpt_ctx {
     int device = 0;
@@ -61,6 +62,16 @@ struct oxpt_ctx {
         int kind;
     };
     std::vector<Timed> timed;
+    // execution mode: megakernel or wavefront, and the wavefront's buffers
+    uint32_t mode = OXPT_MODE_WAVEFRONT;
+    uint32_t wave_slots = 1u << 20;
+    uint64_t wave_items = 1ull << 24;
+    uint32_t check_every = 4;
+    void* wave_mem = nullptr;
+    size_t wave_bytes = 0;
+    uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
+    uint32_t* wave_host = nullptr;  // pinned: [0..2] counters snapshot
+    uint64_t wave_iterations = 0;
 };
 
 namespace {
@@ -144,13 +155,117 @@ uint32_t trace_grid(oxpt_ctx* c, uint64_t total, bool count) {
     return (uint32_t)std::max<uint64_t>(1, std::min(blocks, need));
 }
 
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Carve the wavefront's path state and queues out of one allocation.
+oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveState* st, oxd::WaveQueues* q,
+                        uint32_t** ctr, unsigned long long** work) {
+    size_t P = slots, PJ = (size_t)slots * jobs;
+    size_t sizes[] = {P * 8, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 4, P * 4,
+                      PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64};
+    size_t total = 0;
+    for (size_t s : sizes) total += align256(s);
+    if (slots > c->wave_cap_slots || jobs > c->wave_cap_jobs || total > c->wave_bytes) {
+        if (c->wave_mem) cudaFree(c->wave_mem);
+        c->wave_mem = nullptr;
+        c->wave_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->wave_mem, total);
+        if (e != cudaSuccess) {
+            c->wave_mem = nullptr;
+            c->wave_cap_slots = c->wave_cap_jobs = 0;
+            return cuda_fail(c, e, "wavefront path state");
+        }
+        c->wave_bytes = total;
+        c->wave_cap_slots = slots;
+        c->wave_cap_jobs = jobs;
+    }
+    char* p = (char*)c->wave_mem;
+    void* ptr[17];
+    for (int k = 0; k < 17; k++) {
+        ptr[k] = p;
+        p += align256(sizes[k]);
+    }
+    st->item = (unsigned long long*)ptr[0];
+    st->seed = (uint4*)ptr[1];
+    st->beta = (float4*)ptr[2];
+    st->rad = (float4*)ptr[3];
+    st->dir = (float4*)ptr[4];
+    st->org = (float4*)ptr[5];
+    st->prev = (float4*)ptr[6];
+    st->sigma = (float4*)ptr[7];
+    st->hit = (uint4*)ptr[8];
+    st->hmeta = (uint32_t*)ptr[9];
+    st->nee_n = (uint32_t*)ptr[10];
+    st->pend = (float4*)ptr[11];
+    q->ext = (uint32_t*)ptr[12];
+    q->sh_o = (float4*)ptr[13];
+    q->sh_d = (float4*)ptr[14];
+    q->sh_m = (uint4*)ptr[15];
+    *ctr = (uint32_t*)ptr[16];
+    *work = (unsigned long long*)((char*)ptr[16] + 32);
+    if (!c->wave_host) {
+        cudaError_t e = cudaMallocHost((void**)&c->wave_host, 64);
+        if (e != cudaSuccess) {
+            c->wave_host = nullptr;
+            return cuda_fail(c, e, "pinned counters");
+        }
+    }
+    return OXPT_OK;
+}
+
+// One sub-frame through the wavefront: iterate logic / extend / shadow
+// until every slot is empty, then reduce in sample order.
+oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
+    uint32_t J = c->params.cfg[2] + 1u;
+    uint64_t total = ta.total;
+    uint32_t P = (uint32_t)std::min<uint64_t>(total, c->wave_slots);
+    oxd::WaveArgs wa;
+    oxpt_status s = ensure_wave(c, P, J, &wa.st, &wa.q, &wa.ctr, &wa.work);
+    if (s) return s;
+    wa.s = ta.s;
+    wa.slots = P;
+    wa.jobs = J;
+    wa.first = ta.first;
+    wa.y0 = ta.y0;
+    wa.npix = ta.npix;
+    wa.total = total;
+    wa.out = ta.out;
+    wa.counters = ta.counters;
+    wa.err = ta.err;
+    CK(c, cudaMemsetAsync(wa.st.rad, 0, (size_t)P * 16, c->stream), "wave init");
+    CK(c, cudaMemsetAsync(wa.st.nee_n, 0, (size_t)P * 4, c->stream), "wave init");
+    CK(c, cudaMemsetAsync(wa.ctr, 0, 64, c->stream), "wave init");
+    static int tb = 0;
+    if (!tb) tb = std::max(1, oxd::wave_traverse_blocks_per_sm());
+    uint32_t tblocks = (uint32_t)c->sms * (uint32_t)tb;
+    uint64_t per_slot = total / P + 1;
+    uint64_t bounces = std::min<uint64_t>(c->params.dims[3], 1u << 20);
+    uint64_t cap = 4 * (bounces + 2) * per_slot + 1024;
+    for (uint64_t it = 0;; it++) {
+        if (it > cap) return fail(c, OXPT_E_TIMEOUT, "wavefront did not drain within its iteration bound");
+        CK(c, cudaMemsetAsync(wa.ctr, 0, 16, c->stream), "queue reset");
+        CK(c, oxd::launch_wave_logic(wa, count, c->stream), "wave logic");
+        CK(c, oxd::launch_wave_extend(wa, count, tblocks, c->stream), "wave extend");
+        CK(c, oxd::launch_wave_shadow(wa, count, tblocks, c->stream), "wave shadow");
+        c->launches += 3;
+        c->wave_iterations++;
+        if ((it + 1) % c->check_every == 0) {
+            CK(c, cudaMemcpyAsync(c->wave_host, wa.ctr, 16, cudaMemcpyDeviceToHost, c->stream), "queue readback");
+            CK(c, cudaStreamSynchronize(c->stream), "queue readback");
+            if (c->wave_host[2] == 0) break;
+        }
+    }
+    return OXPT_OK;
+}
+
 // One dispatch = frame {first, count, y0, rows}, split into launches of at
-// most max_paths paths; each launch traces into `out` and reduces in
-// sample order.
+// most max_paths paths (megakernel) or wave_items (wavefront); each launch
+// traces into `out` and reduces in sample order.
 oxpt_status run_frame(oxpt_ctx* c, const oxpt_frame& f, bool count) {
     if (f.count == 0 || f.rows == 0) return OXPT_OK;
     if (f.y0 >= c->h || f.rows > c->h - f.y0) return fail(c, OXPT_E_INVALID, "frame rows outside the image");
-    uint64_t cap = std::max<uint64_t>(c->max_paths, c->w);
+    bool wave = c->mode == OXPT_MODE_WAVEFRONT;
+    uint64_t cap = std::max<uint64_t>(wave ? c->wave_items : c->max_paths, c->w);
     uint32_t rows_per = f.rows, per = f.count;
     uint64_t row_paths = (uint64_t)c->w * f.rows;
     if (row_paths > cap) {
@@ -184,7 +299,14 @@ oxpt_status run_frame(oxpt_ctx* c, const oxpt_frame& f, bool count) {
                 CK(c, cudaEventCreate(&tr.b), "event");
                 CK(c, cudaEventRecord(tt.a, c->stream), "event record");
             }
-            CK(c, oxd::launch_trace(ta, count, trace_grid(c, ta.total, count), c->threads, c->stream), "trace launch");
+            if (wave) {
+                oxpt_status ws = run_wave(c, ta, count);
+                if (ws) return ws;
+            } else {
+                CK(c, oxd::launch_trace(ta, count, trace_grid(c, ta.total, count), c->threads, c->stream),
+                   "trace launch");
+                c->launches += 1;
+            }
             if (c->timing) {
                 CK(c, cudaEventRecord(tt.b, c->stream), "event record");
                 CK(c, cudaEventRecord(tr.a, c->stream), "event record");
@@ -196,7 +318,7 @@ oxpt_status run_frame(oxpt_ctx* c, const oxpt_frame& f, bool count) {
                 c->timed.push_back(tt);
                 c->timed.push_back(tr);
             }
-            c->launches += 2;
+            c->launches += 1;
         }
     }
     return OXPT_OK;
@@ -245,9 +367,11 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
     }
-    void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err, c->dev_counters};
+    void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
+                    c->dev_counters, c->wave_mem};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (c->wave_host) cudaFreeHost(c->wave_host);
     if (c->own) cudaStreamDestroy(c->own);
     (void)cudaGetLastError();
     delete c;
@@ -540,6 +664,42 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* c, uint32_t threads, uint32_t blocks_
     c->threads = threads ? threads : oxd::TRACE_THREADS;
     c->blocks_per_sm = blocks_per_sm;
     c->max_paths = max_paths ? max_paths : (1ull << 22);
+    c->wave_items = max_paths ? max_paths : (1ull << 24);
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
+    if (!c || !t) return OXPT_E_INVALID;
+    if (t->mode > OXPT_MODE_WAVEFRONT) return fail(c, OXPT_E_INVALID, "unknown execution mode");
+    if (t->threads && (t->threads % 32 != 0 || t->threads > oxd::TRACE_THREADS))
+        return fail(c, OXPT_E_INVALID, "threads must be a multiple of 32 and at most the kernel's block bound");
+    if (t->wave_slots > (1u << 26)) return fail(c, OXPT_E_LIMIT, "at most 2^26 wavefront slots");
+    c->mode = t->mode;
+    c->threads = t->threads ? t->threads : oxd::TRACE_THREADS;
+    c->blocks_per_sm = t->blocks_per_sm;
+    c->wave_slots = t->wave_slots ? t->wave_slots : (1u << 20);
+    c->max_paths = t->max_paths ? t->max_paths : (1ull << 22);
+    c->wave_items = t->wave_items ? t->wave_items : (1ull << 24);
+    c->check_every = t->check_every ? t->check_every : 4u;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
+    if (!c || !t) return OXPT_E_INVALID;
+    std::memset(t, 0, sizeof(*t));
+    t->mode = c->mode;
+    t->threads = c->threads;
+    t->blocks_per_sm = c->blocks_per_sm;
+    t->wave_slots = c->wave_slots;
+    t->max_paths = c->max_paths;
+    t->wave_items = c->wave_items;
+    t->check_every = c->check_every;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* c, uint64_t* out) {
+    if (!c || !out) return OXPT_E_INVALID;
+    *out = c->wave_iterations;
     return OXPT_OK;
 }
 

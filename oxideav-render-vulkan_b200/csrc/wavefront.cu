@@ -1,0 +1,271 @@
+// Wavefront path tracing for sm_100a (Laine, Karras & Aila 2013,
+// "Megakernels considered harmful").
+//
+// The megakernel (trace.cu) interleaves traversal, texture filtering,
+// the layered BSDF and light sampling in one divergent loop: its code does
+// not fit the instruction cache and a warp's lanes sit at different stages.
+// Here a path is a slot of SoA state in HBM and every bounce is three
+// launches:
+//   wave_logic   one thread per slot: adds the previous vertex's visible NEE
+//                contributions in job order, processes the continuation
+//                ray's hit (emission, material, BSDF), evaluates every NEE
+//                job of the new vertex at once (their shadow rays go to a
+//                queue), samples the BSDF and queues the next continuation
+//                ray; finished slots take the next (pixel, sample) item from
+//                a global counter (path regeneration);
+//   wave_extend  closest-hit traversal of the queued continuation rays;
+//   wave_shadow  any-hit traversal of the queued shadow rays.
+// The traversal kernels hold nothing but the ray and the stack, so they run
+// at high occupancy with coherent code. Each path's radiance receives the
+// same contributions in the same order as in the megakernel (emission, the
+// unoccluded NEE terms in job order, the next ray's findings), so results
+// are bit-identical; finished paths land in the per-launch result buffer
+// that reduce_frame adds to the accumulator in sample order.
+#include <cooperative_groups.h>
+
+#include "kernels.cuh"
+#include "path.cuh"
+#include "shade.cuh"
+#include "traverse.cuh"
+#include "wavefront.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace oxd {
+
+enum : uint32_t { ST_EMPTY = 0, ST_TRACING = 1, ST_ENDING = 2 };
+
+// Warp-aggregated append: one atomic per converged group.
+__device__ __forceinline__ uint32_t append(uint32_t* ctr) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+__device__ __forceinline__ unsigned long long fetch_item(unsigned long long* ctr) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, (unsigned long long)g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
+__device__ __forceinline__ void load_core(const WaveArgs& a, uint32_t i, PathCore* pc, Sampler* smp, uint32_t* flags) {
+    uint4 sd = a.st.seed[i];
+    float4 b = a.st.beta[i], r = a.st.rad[i], d = a.st.dir[i], pp = a.st.prev[i], sg = a.st.sigma[i];
+    smp->pixel_seed = sd.x;
+    smp->index = sd.y;
+    smp->path_seed = sd.z;
+    pc->k = sd.w;
+    pc->beta = xyz(b);
+    pc->prev_pdf = b.w;
+    pc->radiance = xyz(r);
+    *flags = __float_as_uint(r.w);
+    pc->in_medium = (*flags & 4u) != 0u;
+    pc->d = xyz(d);
+    pc->prev_pos = xyz(pp);
+    pc->sigma = xyz(sg);
+}
+
+__device__ __forceinline__ void store_core(const WaveArgs& a, uint32_t i, const PathCore& pc, const Sampler& smp,
+                                           uint32_t stage) {
+    a.st.seed[i] = make_uint4(smp.pixel_seed, smp.index, smp.path_seed, pc.k);
+    a.st.beta[i] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, pc.prev_pdf);
+    uint32_t flags = stage | (pc.in_medium ? 4u : 0u);
+    a.st.rad[i] = make_float4(pc.radiance.x, pc.radiance.y, pc.radiance.z, __uint_as_float(flags));
+    a.st.dir[i] = make_float4(pc.d.x, pc.d.y, pc.d.z, 0.0f);
+    a.st.prev[i] = make_float4(pc.prev_pos.x, pc.prev_pos.y, pc.prev_pos.z, 0.0f);
+    a.st.sigma[i] = make_float4(pc.sigma.x, pc.sigma.y, pc.sigma.z, 0.0f);
+}
+
+__device__ __forceinline__ void set_stage(const WaveArgs& a, uint32_t i, uint32_t flags_other, uint32_t stage) {
+    float4 r = a.st.rad[i];
+    r.w = __uint_as_float(stage | flags_other);
+    a.st.rad[i] = r;
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) wave_logic(const __grid_constant__ WaveArgs a) {
+    __shared__ uint32_t s_sobol[128];
+    __shared__ float s_sheen[512];
+    const Scene& s = a.s;
+    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s, s.P.offs0[0] + i);
+    for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s, s.P.offs0[1] + i);
+    __syncthreads();
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.slots) return;
+    const uint32_t J = a.jobs;
+    unsigned long long paths = 0, shaded = 0;
+
+    PathCore pc;
+    Sampler smp;
+    uint32_t flags = __float_as_uint(a.st.rad[i].w);
+    uint32_t stage = flags & 3u;
+    bool need_new = stage == ST_EMPTY;
+    if (!need_new) {
+        load_core(a, i, &pc, &smp, &flags);
+        // The previous vertex's NEE terms, in job order.
+        uint32_t n = a.st.nee_n[i];
+        for (uint32_t j = 0; j < n; j++) {
+            float4 pe = a.st.pend[(uint64_t)i * J + j];
+            if (pe.w == 2.0f) pc.radiance = pc.radiance + xyz(pe);
+        }
+        a.st.nee_n[i] = 0u;
+        bool covered = true, finished = false;
+        if (stage == ST_ENDING) {
+            finished = true;
+        } else {
+            uint4 hb = a.st.hit[i];
+            uint32_t hm = a.st.hmeta[i];
+            Hit hit;
+            hit.slot = hb.x;
+            bool got = hb.x != NONE;
+            uint32_t hmat = hm & 0x7fffffffu;
+            hit.t = __uint_as_float(hb.y);
+            float u = __uint_as_float(hb.z), v = __uint_as_float(hb.w);
+            hit.b = mk(1.0f - u - v, u, v);
+            hit.front = (hm >> 31) != 0u;
+            Vertex vx;
+            int outcome = on_path_hit<COUNT>(s, s_sheen, s_sobol, smp, pc, got, hit, hmat, &vx, &shaded);
+            if (outcome != PATH_VERTEX) {
+                finished = true;
+                covered = outcome != PATH_UNCOVERED;
+            } else {
+                uint32_t armed = 0;
+                for (uint32_t j = 0; j < J; j++) {
+                    ShadowRay sr;
+                    float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (nee_job(s, s_sheen, pc, vx, j, &sr)) {
+                        pe = make_float4(sr.pending.x, sr.pending.y, sr.pending.z, 1.0f);
+                        uint32_t q = append(&a.ctr[1]);
+                        a.q.sh_o[q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+                        a.q.sh_d[q] = make_float4(sr.d.x, sr.d.y, sr.d.z, __uint_as_float(sr.skip));
+                        a.q.sh_m[q] = make_uint4(i, j, sr.rid, smp.path_seed);
+                        armed = j + 1;
+                    }
+                    a.st.pend[(uint64_t)i * J + j] = pe;
+                }
+                a.st.nee_n[i] = armed;
+                f3 o;
+                if (continue_path(s, s_sheen, s_sobol, smp, pc, vx, &o)) {
+                    store_core(a, i, pc, smp, ST_TRACING);
+                    a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
+                    a.q.ext[append(&a.ctr[0])] = i;
+                } else if (armed) {
+                    store_core(a, i, pc, smp, ST_ENDING);
+                } else {
+                    finished = true;
+                }
+            }
+        }
+        if (finished) {
+            a.out[a.st.item[i]] = path_result(pc, covered);
+            need_new = true;
+        }
+    }
+    if (need_new) {
+        unsigned long long item = fetch_item(a.work);
+        if (item < a.total) {
+            uint32_t it = (uint32_t)(item / a.npix);
+            uint32_t q = (uint32_t)(item - (unsigned long long)it * a.npix);
+            uint32_t yy = q / s.P.dims[0];
+            f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], a.y0 + yy, a.first + it, &smp, &pc);
+            a.st.item[i] = item;
+            store_core(a, i, pc, smp, ST_TRACING);
+            a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
+            a.q.ext[append(&a.ctr[0])] = i;
+            paths = 1;
+        } else {
+            if (stage != ST_EMPTY) set_stage(a, i, 0u, ST_EMPTY);
+            stage = ST_EMPTY;
+            if (COUNT) {
+                if (shaded) atomicAdd(a.counters + C_SHADED, shaded);
+            }
+            return;
+        }
+    }
+    append(&a.ctr[2]);  // one more slot still active
+    if (COUNT) {
+        if (paths) atomicAdd(a.counters + C_PATHS, paths);
+        if (shaded) atomicAdd(a.counters + C_SHADED, shaded);
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_extend(const __grid_constant__ WaveArgs a) {
+    Cnt cnt;
+    if (COUNT)
+        for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        uint32_t i = a.q.ext[q];
+        float4 o = a.st.org[i], d = a.st.dir[i];
+        uint4 sd = a.st.seed[i];
+        Sampler smp{sd.x, sd.y, sd.z};
+        uint32_t k = sd.w;
+        Hit h;
+        uint32_t m = 0u;
+        bump<COUNT>(cnt, C_PATH_RAYS);
+        bool got = traverse<COUNT>(a.s, make_ray(xyz(o), xyz(d)), INF, smp, k << 16u, k == 0u, false, NONE, &h, &m,
+                                   cnt, a.err);
+        if (got) {
+            f3 b = h.b;
+            a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(b.y), __float_as_uint(b.z));
+            a.st.hmeta[i] = m | (h.front ? 0x80000000u : 0u);
+        } else {
+            a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+        }
+    }
+    if (COUNT)
+        for (int c = 0; c < C_N; c++)
+            if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_shadow(const __grid_constant__ WaveArgs a) {
+    Cnt cnt;
+    if (COUNT)
+        for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[1]);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
+        uint4 m = a.q.sh_m[q];
+        Sampler smp{0u, 0u, m.w};
+        Hit h;
+        uint32_t mat = 0u;
+        bump<COUNT>(cnt, C_SHADOW_RAYS);
+        bool got = traverse<COUNT>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, true, __float_as_uint(d.w),
+                                   &h, &mat, cnt, a.err);
+        if (!got) a.st.pend[(uint64_t)m.x * a.jobs + m.y].w = 2.0f;
+    }
+    if (COUNT)
+        for (int c = 0; c < C_N; c++)
+            if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
+}
+
+cudaError_t launch_wave_logic(const WaveArgs& a, bool count, cudaStream_t st) {
+    uint32_t blocks = (a.slots + 127u) / 128u;
+    if (count) wave_logic<true><<<blocks, 128, 0, st>>>(a);
+    else wave_logic<false><<<blocks, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wave_extend(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st) {
+    if (count) wave_extend<true><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
+    else wave_extend<false><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st) {
+    if (count) wave_shadow<true><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
+    else wave_shadow<false><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+int wave_traverse_blocks_per_sm() {
+    int a = 0, b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, wave_extend<false>, WAVE_TRAVERSE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wave_shadow<false>, WAVE_TRAVERSE_THREADS, 0);
+    return a < b ? a : b;
+}
+
+}  // namespace oxd

@@ -1,0 +1,56 @@
+// Wavefront path-state layout and launch entry points (see wavefront.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device.cuh"
+
+namespace oxd {
+
+constexpr uint32_t WAVE_TRAVERSE_THREADS = 128;
+
+// Path slots, structure-of-arrays in HBM (16-byte records: one vector load
+// per field, coalesced across consecutive slots).
+struct WaveState {
+    unsigned long long* item;  // work item of the slot
+    uint4* seed;               // pixel seed, sample index, path seed, bounce k
+    float4* beta;              // beta.xyz, previous BSDF pdf
+    float4* rad;               // radiance.xyz, flags (stage | in_medium << 2)
+    float4* dir;               // continuation direction
+    float4* org;               // continuation origin
+    float4* prev;              // previous vertex position
+    float4* sigma;             // medium extinction
+    uint4* hit;                // slot (0xffffffff = miss), t, u, v
+    uint32_t* hmeta;           // material | front << 31
+    uint32_t* nee_n;           // NEE jobs of the last vertex to add (0..J)
+    float4* pend;              // slots x J: contribution.xyz, 0 none / 1 queued / 2 visible
+};
+
+struct WaveQueues {
+    uint32_t* ext;  // slot ids with a continuation ray
+    float4* sh_o;   // shadow ray origin, t_max
+    float4* sh_d;   // shadow ray direction, skip id bits
+    uint4* sh_m;    // slot, job, ray id, path seed
+};
+
+struct WaveArgs {
+    Scene s;
+    WaveState st;
+    WaveQueues q;
+    uint32_t slots, jobs;
+    uint32_t first, y0, npix;
+    unsigned long long total;   // items of this launch (npix x samples)
+    unsigned long long* work;   // next item
+    uint32_t* ctr;              // [0] continuation rays, [1] shadow rays, [2] active slots
+    float4* out;
+    unsigned long long* counters;
+    uint32_t* err;
+};
+
+cudaError_t launch_wave_logic(const WaveArgs& a, bool count, cudaStream_t st);
+cudaError_t launch_wave_extend(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st);
+cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st);
+int wave_traverse_blocks_per_sm();
+
+}  // namespace oxd

@@ -302,6 +302,21 @@ class GpuPathTracer:
     def ctx(self):
         return N.lib().oxpt_tracer_ctx(self._h)
 
+    def tuning(self) -> N.Tuning:
+        t = N.Tuning()
+        N.lib().oxpt_get_tuning(self.ctx, C.byref(t))
+        return t
+
+    def set_tuning(self, **kw):
+        """Change the execution plan (mode, launch shape); results are
+        bit-identical under every plan."""
+        t = self.tuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        st = N.lib().oxpt_set_tuning(self.ctx, C.byref(t))
+        if st != N.OK:
+            _raise(st, N.lib().oxpt_last_error(self.ctx).decode())
+
     def adapter_summary(self) -> str:
         buf = C.create_string_buffer(256)
         N.lib().oxpt_device_summary(self.ctx, buf, 256)

@@ -198,9 +198,32 @@ def test_images_vs_libm_oracle_psnr_at_least_60db(pkg, oracle):
     assert psnr >= 60.0, psnr
 
 
-def test_traversal_counters_match_oracle(pkg, oracle):
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("which", ["materials", "layered", "alpha"])
+def test_both_execution_modes_bit_exact(pkg, oracle, mode, which):
+    """Megakernel and wavefront plans give the oracle's accumulator, also
+    with few wavefront slots (path regeneration) and split launches."""
+    if which == "materials":
+        scene, env = scenes.materials_scene(pkg), None
+    elif which == "alpha":
+        scene, env = scenes.alpha_scene(pkg), None
+    else:
+        scene = pkg.Scene.icosphere(freq=16, seed=2, n_materials=12, n_textures=3, tex_size=64, n_punctual=3,
+                                    n_emissive=16, material_mix=1)
+        env = pkg.EnvironmentMap.sky(64, 32)
+    t = _tracer(pkg, scene, _opts(pkg, 40, 28, 6, bounces=10), env)
+    t.set_tuning(mode=mode, wave_slots=333, wave_items=2000, max_paths=2000, check_every=3)
+    t.refine(6)
+    gpu = t.read_accum()
+    cpu, _ = oracle.render(t.prepared(), 6)
+    assert np.array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_traversal_counters_match_oracle(pkg, oracle, mode):
     opts = _opts(pkg, 48, 32, 4)
     t = _tracer(pkg, scenes.materials_scene(pkg), opts)
+    t.set_tuning(mode=mode)
     p = t.prepared()  # binds tables and params on the context
     out = (C.c_uint64 * 8)()
     st = pkg._native.lib().oxpt_diag_refine_counted(t.ctx, 0, 4, out)
