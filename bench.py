@@ -246,12 +246,24 @@ def main():
         pt.set_tuning(**kw)
     prep = pt.prepared()
 
-    # Algorithmic bytes per path from the counting build (untimed, 1 spp).
+    # Algorithmic bytes per path from the counting build (untimed, 1 spp):
+    # traversal kernels 32 B per AABB and 48 B per triangle tested, shading
+    # 192 B of attributes + 544 B of material record per shaded hit.
     cnt = (C.c_uint64 * 8)()
     assert L.oxpt_diag_refine_counted(pt.ctx, 1 << 20, 1, cnt) == 0
     c = [int(x) for x in cnt]
-    bytes_per_path = (BYTES_AABB * c[3] + BYTES_TRI * c[5] + (BYTES_ATTR + BYTES_MAT) * c[6]) / max(c[0], 1)
-    rays_per_path = (c[1] + c[2]) / max(c[0], 1)
+    split = (C.c_uint64 * 16)()
+    L.oxpt_diag_counters_split(pt.ctx, split)
+    h0, h1 = [int(x) for x in split[:8]], [int(x) for x in split[8:]]
+    npaths = max(c[0], 1)
+    bytes_per_path = (BYTES_AABB * c[3] + BYTES_TRI * c[5] + (BYTES_ATTR + BYTES_MAT) * c[6]) / npaths
+    kernel_bytes = {  # algorithmic bytes per camera path, per kernel
+        "trace_paths": bytes_per_path,
+        "wave_logic": (BYTES_ATTR + BYTES_MAT) * c[6] / npaths,
+        "wave_extend": (BYTES_AABB * h0[3] + BYTES_TRI * h0[5]) / npaths,
+        "wave_shadow": (BYTES_AABB * h1[3] + BYTES_TRI * h1[5]) / npaths,
+    }
+    rays_per_path = (c[1] + c[2]) / npaths
 
     def step():
         pt.reset()
@@ -290,16 +302,33 @@ def main():
     paths_step = a.width * a.height * a.spp
     value = world * a.steps * paths_step / t_max / 1e6
 
-    # Roofline of the trace kernel.
+    # Roofline of the dominant kernel: its algorithmic bytes over the timed
+    # region / its summed CUDA-event time (kernel launches on the tracer's
+    # stream), against the measured HBM copy bandwidth.
     peak, peak_kind = measured_peak()
-    launch_ms = tms.value / max(tn.value, 1)
-    paths_per_launch = paths_step * a.steps / max(tn.value, 1)
-    achieved = bytes_per_path * paths_per_launch / (launch_ms / 1e3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "trace_paths_traffic.json"
+    kms, kn = (C.c_double * 8)(), (C.c_uint64 * 8)()
+    L.oxpt_diag_timing_kinds(pt.ctx, kms, kn)
+    wave = pt.tuning().mode == 1
+    paths_timed = paths_step * a.steps
+    kinds = ((2, "wave_logic"), (3, "wave_extend"), (4, "wave_shadow")) if wave else ((0, "trace_paths"),)
+    traffic_db = {}
+    tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
-        td = json.loads(tf.read_text())
-        traffic = td.get("bytes_per_path", 0) * paths_per_launch if td.get("bytes_per_path") else None
+        traffic_db = json.loads(tf.read_text())
+    kernels = {}
+    for k, name in kinds:
+        if not kn[k]:
+            continue
+        b = kernel_bytes[name] * paths_timed
+        per_launch = b / kn[k]
+        tr = traffic_db.get(name, {}).get("dram_bytes_per_path")
+        kernels[name] = {"ms_total": kms[k], "launches": int(kn[k]), "launch_ms": kms[k] / kn[k],
+                         "algorithmic_bytes_per_launch": per_launch,
+                         "achieved_gbs": b / (kms[k] / 1e3) / 1e9 if kms[k] else None,
+                         "traffic_bytes_per_launch": tr * paths_timed / kn[k] if tr else None}
+    dom = max(kernels, key=lambda n: kernels[n]["ms_total"])
+    kd = kernels[dom]
+    achieved = kd["achieved_gbs"]
 
     # End to end through the C ABI with host buffers.
     e2e = None
@@ -326,10 +355,12 @@ def main():
                 "config": config(a, world),
                 "mrays_per_s": value * rays_per_path,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic,
-                             "kernel": "trace_paths", "peak_kind": peak_kind,
-                             "algorithmic_bytes_per_path": bytes_per_path, "launch_ms": launch_ms,
-                             "launches": int(tn.value), "reduce_ms_total": rms.value},
+                             "frac": achieved / peak, "traffic": kd["traffic_bytes_per_launch"],
+                             "kernel": dom, "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_launch": kd["algorithmic_bytes_per_launch"],
+                             "launch_ms": kd["launch_ms"], "launches": kd["launches"],
+                             "algorithmic_bytes_per_path": bytes_per_path, "kernels": kernels,
+                             "trace_phase_ms": tms.value, "reduce_ms_total": rms.value},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(n1.value - n0.value),
                 "clocks": clk.summary(), "rays_per_path": rays_per_path,
                 "plan": {"mode": ["megakernel", "wavefront"][pt.tuning().mode], "wave_slots": pt.tuning().wave_slots}}

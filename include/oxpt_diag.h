@@ -63,6 +63,16 @@ oxpt_status oxpt_diag_refine_counted(oxpt_ctx* ctx, uint32_t first_sample, uint3
 oxpt_status oxpt_diag_set_timing(oxpt_ctx* ctx, int enabled);
 oxpt_status oxpt_diag_timing(oxpt_ctx* ctx, double* trace_ms, uint64_t* trace_launches,
                              double* reduce_ms, uint64_t* reduce_launches);
+/* The per-kind figures of the last oxpt_diag_timing call: kind 0 the trace
+ * phase of each launch (the megakernel, or a whole wavefront run), 1 the
+ * ordered reduce, 2 wavefront logic, 3 wavefront extension traversal, 4
+ * wavefront shadow traversal. */
+oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* ctx, double ms[8], uint64_t n[8]);
+/* The last oxpt_diag_refine_counted totals split by ray kind: out[0..7] for
+ * continuation rays and shading (wavefront logic + extension), out[8..15]
+ * for shadow rays (wavefront shadow kernel); the megakernel reports all in
+ * the first half. */
+oxpt_status oxpt_diag_counters_split(const oxpt_ctx* ctx, uint64_t out[16]);
 
 /* Launch-shape override for tuning: threads per block and resident blocks
  * per SM of the megakernel (0 = library default), and the largest number

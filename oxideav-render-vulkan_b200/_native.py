@@ -129,6 +129,8 @@ _SIGS = {
     "oxpt_set_tuning": (cint, [vp, C.POINTER(Tuning)]),
     "oxpt_get_tuning": (cint, [vp, C.POINTER(Tuning)]),
     "oxpt_diag_wave_iterations": (cint, [vp, C.POINTER(u64)]),
+    "oxpt_diag_timing_kinds": (cint, [vp, vp, vp]),
+    "oxpt_diag_counters_split": (cint, [vp, vp]),
     "oxpt_diag_timing": (cint, [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(u64)]),
     # oxpt_host.h
     "oxpt_material_default": (None, [C.POINTER(Material)]),

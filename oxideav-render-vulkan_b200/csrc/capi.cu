@@ -62,6 +62,9 @@ struct oxpt_ctx {
         int kind;
     };
     std::vector<Timed> timed;
+    double kind_ms[8] = {0}, last_ms[8] = {0};
+    uint64_t kind_n[8] = {0}, last_n[8] = {0};
+    uint64_t split_counts[2 * oxd::C_N] = {0};
     // execution mode: megakernel or wavefront, and the wavefront's buffers
     uint32_t mode = OXPT_MODE_WAVEFRONT;
     uint32_t wave_slots = 1u << 20;
@@ -241,12 +244,28 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     uint64_t per_slot = total / P + 1;
     uint64_t bounces = std::min<uint64_t>(c->params.dims[3], 1u << 20);
     uint64_t cap = 4 * (bounces + 2) * per_slot + 1024;
+    oxd::WaveArgs wsh = wa;  // shadow rays count into the second counter half
+    if (wsh.counters) wsh.counters += oxd::C_N;
+    auto timed = [&](int kind, auto&& launch) -> cudaError_t {
+        oxpt_ctx::Timed t{nullptr, nullptr, kind};
+        if (c->timing) {
+            cudaEventCreate(&t.a);
+            cudaEventCreate(&t.b);
+            cudaEventRecord(t.a, c->stream);
+        }
+        cudaError_t e = launch();
+        if (c->timing) {
+            cudaEventRecord(t.b, c->stream);
+            c->timed.push_back(t);
+        }
+        return e;
+    };
     for (uint64_t it = 0;; it++) {
         if (it > cap) return fail(c, OXPT_E_TIMEOUT, "wavefront did not drain within its iteration bound");
         CK(c, cudaMemsetAsync(wa.ctr, 0, 16, c->stream), "queue reset");
-        CK(c, oxd::launch_wave_logic(wa, count, c->stream), "wave logic");
-        CK(c, oxd::launch_wave_extend(wa, count, tblocks, c->stream), "wave extend");
-        CK(c, oxd::launch_wave_shadow(wa, count, tblocks, c->stream), "wave shadow");
+        CK(c, timed(2, [&] { return oxd::launch_wave_logic(wa, count, c->stream); }), "wave logic");
+        CK(c, timed(3, [&] { return oxd::launch_wave_extend(wa, count, tblocks, c->stream); }), "wave extend");
+        CK(c, timed(4, [&] { return oxd::launch_wave_shadow(wsh, count, tblocks, c->stream); }), "wave shadow");
         c->launches += 3;
         c->wave_iterations++;
         if ((it + 1) % c->check_every == 0) {
@@ -347,7 +366,7 @@ oxpt_status oxpt_create(int device, oxpt_ctx** out) {
     c->sms = prop.multiProcessorCount;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc((void**)&c->dev_err, sizeof(uint32_t)) != cudaSuccess ||
-        cudaMalloc((void**)&c->dev_counters, sizeof(unsigned long long) * oxd::C_N) != cudaSuccess ||
+        cudaMalloc((void**)&c->dev_counters, sizeof(unsigned long long) * 2 * oxd::C_N) != cudaSuccess ||
         cudaMemset(c->dev_err, 0, sizeof(uint32_t)) != cudaSuccess) {
         (void)cudaGetLastError();
         oxpt_destroy(c);
@@ -647,14 +666,21 @@ oxpt_status oxpt_diag_refine_counted(oxpt_ctx* c, uint32_t first, uint32_t count
     oxpt_status s = ready(c);
     if (s) return s;
     if ((s = set_device(c))) return s;
-    CK(c, cudaMemsetAsync(c->dev_counters, 0, sizeof(unsigned long long) * oxd::C_N, c->stream), "counter clear");
+    CK(c, cudaMemsetAsync(c->dev_counters, 0, sizeof(unsigned long long) * 2 * oxd::C_N, c->stream), "counter clear");
     oxpt_frame f{first, count, 0, c->h};
     if ((s = run_frame(c, f, true))) return s;
-    unsigned long long host[oxd::C_N];
+    unsigned long long host[2 * oxd::C_N];
     CK(c, cudaMemcpyAsync(host, c->dev_counters, sizeof(host), cudaMemcpyDeviceToHost, c->stream), "counters");
     CK(c, cudaStreamSynchronize(c->stream), "counters");
-    for (int k = 0; k < 8; k++) out[k] = k < oxd::C_N ? host[k] : 0;
+    for (int k = 0; k < 2 * oxd::C_N; k++) c->split_counts[k] = host[k];
+    for (int k = 0; k < 8; k++) out[k] = k < oxd::C_N ? host[k] + host[oxd::C_N + k] : 0;
     return oxpt_finish(c);
+}
+
+oxpt_status oxpt_diag_counters_split(const oxpt_ctx* c, uint64_t out[16]) {
+    if (!c || !out) return OXPT_E_INVALID;
+    for (int k = 0; k < 16; k++) out[k] = k < 2 * oxd::C_N ? c->split_counts[k] : 0;
+    return OXPT_OK;
 }
 
 oxpt_status oxpt_diag_set_launch(oxpt_ctx* c, uint32_t threads, uint32_t blocks_per_sm, uint64_t max_paths) {
@@ -714,21 +740,34 @@ oxpt_status oxpt_diag_timing(oxpt_ctx* c, double* trace_ms, uint64_t* trace_n, d
     oxpt_status s = set_device(c);
     if (s) return s;
     CK(c, cudaStreamSynchronize(c->stream), "timing sync");
-    double ms[2] = {0.0, 0.0};
-    uint64_t n[2] = {0, 0};
     for (auto& t : c->timed) {
         float e = 0.0f;
         cudaEventElapsedTime(&e, t.a, t.b);
-        ms[t.kind] += e;
-        n[t.kind] += 1;
+        c->kind_ms[t.kind] += e;
+        c->kind_n[t.kind] += 1;
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
     }
     c->timed.clear();
-    if (trace_ms) *trace_ms = ms[0];
-    if (trace_n) *trace_n = n[0];
-    if (reduce_ms) *reduce_ms = ms[1];
-    if (reduce_n) *reduce_n = n[1];
+    if (trace_ms) *trace_ms = c->kind_ms[0];
+    if (trace_n) *trace_n = c->kind_n[0];
+    if (reduce_ms) *reduce_ms = c->kind_ms[1];
+    if (reduce_n) *reduce_n = c->kind_n[1];
+    std::memcpy(c->last_ms, c->kind_ms, sizeof(c->last_ms));
+    std::memcpy(c->last_n, c->kind_n, sizeof(c->last_n));
+    for (int k = 0; k < 8; k++) {
+        c->kind_ms[k] = 0.0;
+        c->kind_n[k] = 0;
+    }
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* c, double ms[8], uint64_t n[8]) {
+    if (!c || !ms || !n) return OXPT_E_INVALID;
+    for (int k = 0; k < 8; k++) {
+        ms[k] = c->last_ms[k];
+        n[k] = c->last_n[k];
+    }
     return OXPT_OK;
 }
 
