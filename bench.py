@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--mode", default="auto", choices=["auto", "mega", "wave"],
                     help="execution plan; auto = the library default")
     ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     return ap.parse_args()
 
 
@@ -239,11 +240,15 @@ def main():
     assert L.oxpt_set_stream(pt.ctx, C.c_void_p(stream.cuda_stream)) == 0
     pt.set_environment(env)
     pt.sync(scene, opts)
+    tune_log = []
     if a.mode != "auto" or a.slots:
         kw = {"wave_slots": a.slots} if a.slots else {}
         if a.mode != "auto":
             kw["mode"] = 0 if a.mode == "mega" else 1
         pt.set_tuning(**kw)
+    elif not a.no_tune:
+        from oxideav_render_vulkan_b200 import tuner
+        tuner.tune(pt, spp=1, repeats=1, log=tune_log)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):
@@ -363,11 +368,17 @@ def main():
                              "trace_phase_ms": tms.value, "reduce_ms_total": rms.value},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(n1.value - n0.value),
                 "clocks": clk.summary(), "rays_per_path": rays_per_path,
-                "plan": {"mode": ["megakernel", "wavefront"][pt.tuning().mode], "wave_slots": pt.tuning().wave_slots}}
+                "plan": plan_of(pt), "tuner_trials": len(tune_log)}
         print(json.dumps(line), flush=True)
     del pt
     if world > 1:
         dist.destroy_process_group()
+
+
+def plan_of(pt):
+    t = pt.tuning()
+    return {"mode": ["megakernel", "wavefront"][t.mode], "wave_slots": t.wave_slots,
+            "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack}
 
 
 def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank):

@@ -91,6 +91,11 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *   wave_slots     paths in flight (wavefront); wave_items its paths per
  *                  launch; check_every its bounces between completion
  *                  checks.
+ *   shade_variant  wavefront logic kernel compiled for 2 / 3 / 4 resident
+ *                  blocks per SM (0 / 1 / 2): registers against occupancy.
+ *   trace_variant  wavefront traversal kernels for 6 / 8 / 10 blocks.
+ *   stack          traversal stack entries: 32 or 64; 0 = 32 when the BVH
+ *                  is at most 32 levels deep, else 64 (exact either way).
  */
 enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1 };
 typedef struct oxpt_tuning {
@@ -101,7 +106,9 @@ typedef struct oxpt_tuning {
     uint64_t max_paths;
     uint64_t wave_items;
     uint32_t check_every;
-    uint32_t reserved;
+    uint32_t shade_variant;
+    uint32_t trace_variant;
+    uint32_t stack;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);

@@ -70,6 +70,8 @@ struct oxpt_ctx {
     uint32_t wave_slots = 1u << 20;
     uint64_t wave_items = 1ull << 24;
     uint32_t check_every = 4;
+    uint32_t shade_variant = 1, trace_variant = 1, stack = 0;
+    uint32_t bvh_depth = 0;
     void* wave_mem = nullptr;
     size_t wave_bytes = 0;
     uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
@@ -160,6 +162,30 @@ uint32_t trace_grid(oxpt_ctx* c, uint64_t total, bool count) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Levels of the BVH (root = 1), walking the node words on the host; a
+// malformed tree (child index out of range or a cycle) reports 65 so that
+// the reference's 64-entry stack is used.
+uint32_t bvh_depth_of(const uint32_t* geom, uint32_t nodes) {
+    if (nodes == 0) return 0;
+    std::vector<std::pair<uint32_t, uint32_t>> st;
+    st.push_back({0u, 1u});
+    uint32_t depth = 0;
+    uint64_t visits = 0;
+    while (!st.empty()) {
+        auto [n, d] = st.back();
+        st.pop_back();
+        if (++visits > (uint64_t)nodes || d > 64) return 65;
+        depth = std::max(depth, d);
+        uint32_t first = geom[(size_t)n * 8 + 3], count = geom[(size_t)n * 8 + 7];
+        if (count == 0) {
+            if ((uint64_t)first + 1 >= nodes) return 65;
+            st.push_back({first, d + 1});
+            st.push_back({first + 1, d + 1});
+        }
+    }
+    return depth;
+}
+
 // Carve the wavefront's path state and queues out of one allocation.
 oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveState* st, oxd::WaveQueues* q,
                         uint32_t** ctr, unsigned long long** work) {
@@ -238,9 +264,8 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     CK(c, cudaMemsetAsync(wa.st.rad, 0, (size_t)P * 16, c->stream), "wave init");
     CK(c, cudaMemsetAsync(wa.st.nee_n, 0, (size_t)P * 4, c->stream), "wave init");
     CK(c, cudaMemsetAsync(wa.ctr, 0, 64, c->stream), "wave init");
-    static int tb = 0;
-    if (!tb) tb = std::max(1, oxd::wave_traverse_blocks_per_sm());
-    uint32_t tblocks = (uint32_t)c->sms * (uint32_t)tb;
+    // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
+    int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
     uint64_t per_slot = total / P + 1;
     uint64_t bounces = std::min<uint64_t>(c->params.dims[3], 1u << 20);
     uint64_t cap = 4 * (bounces + 2) * per_slot + 1024;
@@ -263,9 +288,14 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     for (uint64_t it = 0;; it++) {
         if (it > cap) return fail(c, OXPT_E_TIMEOUT, "wavefront did not drain within its iteration bound");
         CK(c, cudaMemsetAsync(wa.ctr, 0, 16, c->stream), "queue reset");
-        CK(c, timed(2, [&] { return oxd::launch_wave_logic(wa, count, c->stream); }), "wave logic");
-        CK(c, timed(3, [&] { return oxd::launch_wave_extend(wa, count, tblocks, c->stream); }), "wave extend");
-        CK(c, timed(4, [&] { return oxd::launch_wave_shadow(wsh, count, tblocks, c->stream); }), "wave shadow");
+        CK(c, timed(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, c->stream); }),
+           "wave logic");
+        CK(c, timed(3, [&] {
+               return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, sd, c->sms, c->stream);
+           }), "wave extend");
+        CK(c, timed(4, [&] {
+               return oxd::launch_wave_shadow(wsh, count, (int)c->trace_variant, sd, c->sms, c->stream);
+           }), "wave shadow");
         c->launches += 3;
         c->wave_iterations++;
         if ((it + 1) % c->check_every == 0) {
@@ -442,6 +472,8 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     c->side = d->atlas_side;
     c->layers = d->atlas_layers;
     c->node_count = d->node_count;
+    c->bvh_depth = bvh_depth_of(d->geom, d->node_count);
+    if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
     c->has_scene = true;
     return OXPT_OK;
 }
@@ -707,6 +739,12 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     c->max_paths = t->max_paths ? t->max_paths : (1ull << 22);
     c->wave_items = t->wave_items ? t->wave_items : (1ull << 24);
     c->check_every = t->check_every ? t->check_every : 4u;
+    if (t->shade_variant > 2 || t->trace_variant > 2) return fail(c, OXPT_E_INVALID, "variants are 0, 1 or 2");
+    if (t->stack && t->stack != 32 && t->stack != 64) return fail(c, OXPT_E_INVALID, "stack is 0, 32 or 64");
+    if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
+    c->shade_variant = t->shade_variant;
+    c->trace_variant = t->trace_variant;
+    c->stack = t->stack;
     return OXPT_OK;
 }
 
@@ -720,6 +758,9 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->max_paths = c->max_paths;
     t->wave_items = c->wave_items;
     t->check_every = c->check_every;
+    t->shade_variant = c->shade_variant;
+    t->trace_variant = c->trace_variant;
+    t->stack = c->stack;
     return OXPT_OK;
 }
 

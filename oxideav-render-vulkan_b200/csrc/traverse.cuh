@@ -36,7 +36,10 @@ __device__ __forceinline__ bool accept(const Scene& s, uint32_t slot, uint32_t m
 
 // Closest-hit (any = false) or any-hit (any = true) query. Returns whether
 // something was hit; *best holds the hit and *best_mat its material.
-template <bool COUNT>
+// SD is the stack depth: the reference's 64 (an overflow drops the far
+// child, pathtrace.wgsl:700-704), or any depth at least the BVH's, which
+// never overflows and so gives the same walk with less local memory.
+template <bool COUNT, int SD = STACK>
 __device__ bool traverse(const Scene& s, const Ray& r, float t_max, const Sampler& smp, uint32_t ray_id,
                          bool primary, bool any, uint32_t skip, Hit* best, uint32_t* best_mat, Cnt& cnt,
                          uint32_t* err) {
@@ -47,8 +50,8 @@ __device__ bool traverse(const Scene& s, const Ray& r, float t_max, const Sample
     bump<COUNT>(cnt, C_BOXES);
     if (slab(r, rlo, rhi, t_max) < 0.0f) return false;
     uint32_t cur_first = __float_as_uint(rlo.w), cur_count = __float_as_uint(rhi.w);
-    uint2 st_fc[STACK];
-    float st_t[STACK];
+    uint2 st_fc[SD];
+    float st_t[SD];
     uint32_t sp = 0u;
     // A tree visits each node at most once; anything longer is a malformed
     // BVH, reported through the error word instead of looping.
@@ -98,7 +101,7 @@ __device__ bool traverse(const Scene& s, const Ray& r, float t_max, const Sample
                                     : make_uint2(__float_as_uint(alo.w), __float_as_uint(ahi.w));
                 uint2 farfc = swap ? make_uint2(__float_as_uint(alo.w), __float_as_uint(ahi.w))
                                    : make_uint2(__float_as_uint(blo.w), __float_as_uint(bhi.w));
-                if (sp < (uint32_t)STACK) {
+                if (sp < (uint32_t)SD) {
                     st_fc[sp] = farfc;
                     st_t[sp] = swap ? tl : tr;
                     sp++;

@@ -83,8 +83,8 @@ __device__ __forceinline__ void set_stage(const WaveArgs& a, uint32_t i, uint32_
     a.st.rad[i] = r;
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(128) wave_logic(const __grid_constant__ WaveArgs a) {
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ WaveArgs a) {
     __shared__ uint32_t s_sobol[128];
     __shared__ float s_sheen[512];
     const Scene& s = a.s;
@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(128) wave_logic(const __grid_constant__ WaveAr
     }
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_extend(const __grid_constant__ WaveArgs a) {
+template <bool COUNT, int MINB, int SD>
+__global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_extend(const __gri
         Hit h;
         uint32_t m = 0u;
         bump<COUNT>(cnt, C_PATH_RAYS);
-        bool got = traverse<COUNT>(a.s, make_ray(xyz(o), xyz(d)), INF, smp, k << 16u, k == 0u, false, NONE, &h, &m,
+        bool got = traverse<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), INF, smp, k << 16u, k == 0u, false, NONE, &h, &m,
                                    cnt, a.err);
         if (got) {
             f3 b = h.b;
@@ -220,8 +220,8 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_extend(const __gri
             if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_shadow(const __grid_constant__ WaveArgs a) {
+template <bool COUNT, int MINB, int SD>
+__global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_shadow(const __gri
         Hit h;
         uint32_t mat = 0u;
         bump<COUNT>(cnt, C_SHADOW_RAYS);
-        bool got = traverse<COUNT>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, true, __float_as_uint(d.w),
+        bool got = traverse<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, true, __float_as_uint(d.w),
                                    &h, &mat, cnt, a.err);
         if (!got) a.st.pend[(uint64_t)m.x * a.jobs + m.y].w = 2.0f;
     }
@@ -242,30 +242,64 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS) wave_shadow(const __gri
             if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
 }
 
-cudaError_t launch_wave_logic(const WaveArgs& a, bool count, cudaStream_t st) {
-    uint32_t blocks = (a.slots + 127u) / 128u;
-    if (count) wave_logic<true><<<blocks, 128, 0, st>>>(a);
-    else wave_logic<false><<<blocks, 128, 0, st>>>(a);
+// Compiled variants: logic kernel occupancy targets 2 / 3 / 4 resident
+// blocks per SM, traversal kernels 6 / 8 / 10 blocks with a 32- or 64-deep
+// stack. The tuner picks one; all give the same results.
+template <bool C>
+static cudaError_t logic_v(const WaveArgs& a, int v, unsigned blocks, cudaStream_t st) {
+    switch (v) {
+        case 0: wave_logic<C, 2><<<blocks, 128, 0, st>>>(a); break;
+        case 1: wave_logic<C, 3><<<blocks, 128, 0, st>>>(a); break;
+        default: wave_logic<C, 4><<<blocks, 128, 0, st>>>(a); break;
+    }
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave_extend(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st) {
-    if (count) wave_extend<true><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
-    else wave_extend<false><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
-    return cudaGetLastError();
+template <bool C, bool EXT, int SD>
+static void* trav_fn(int v) {
+    if (EXT) {
+        if (v == 0) return (void*)wave_extend<C, 6, SD>;
+        if (v == 1) return (void*)wave_extend<C, 8, SD>;
+        return (void*)wave_extend<C, 10, SD>;
+    }
+    if (v == 0) return (void*)wave_shadow<C, 6, SD>;
+    if (v == 1) return (void*)wave_shadow<C, 8, SD>;
+    return (void*)wave_shadow<C, 10, SD>;
 }
 
-cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st) {
-    if (count) wave_shadow<true><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
-    else wave_shadow<false><<<blocks, WAVE_TRAVERSE_THREADS, 0, st>>>(a);
-    return cudaGetLastError();
+static void* trav_kernel(bool count, bool ext, int v, int sd) {
+    if (count) {
+        if (ext) return sd <= 32 ? trav_fn<true, true, 32>(v) : trav_fn<true, true, 64>(v);
+        return sd <= 32 ? trav_fn<true, false, 32>(v) : trav_fn<true, false, 64>(v);
+    }
+    if (ext) return sd <= 32 ? trav_fn<false, true, 32>(v) : trav_fn<false, true, 64>(v);
+    return sd <= 32 ? trav_fn<false, false, 32>(v) : trav_fn<false, false, 64>(v);
 }
 
-int wave_traverse_blocks_per_sm() {
-    int a = 0, b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, wave_extend<false>, WAVE_TRAVERSE_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wave_shadow<false>, WAVE_TRAVERSE_THREADS, 0);
-    return a < b ? a : b;
+cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st) {
+    unsigned blocks = (a.slots + 127u) / 128u;
+    variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
+    return count ? logic_v<true>(a, variant, blocks, st) : logic_v<false>(a, variant, blocks, st);
+}
+
+static cudaError_t launch_trav(const WaveArgs& a, bool count, bool ext, int variant, int sd, int sms,
+                               cudaStream_t st) {
+    variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
+    void* fn = trav_kernel(count, ext, variant, sd);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, WAVE_TRAVERSE_THREADS, 0);
+    unsigned blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+    WaveArgs copy = a;
+    void* args[] = {&copy};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(WAVE_TRAVERSE_THREADS), args, 0, st);
+}
+
+cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
+    return launch_trav(a, count, true, variant, stack, sms, st);
+}
+
+cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
+    return launch_trav(a, count, false, variant, stack, sms, st);
 }
 
 }  // namespace oxd

@@ -48,9 +48,10 @@ struct WaveArgs {
     uint32_t* err;
 };
 
-cudaError_t launch_wave_logic(const WaveArgs& a, bool count, cudaStream_t st);
-cudaError_t launch_wave_extend(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st);
-cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, uint32_t blocks, cudaStream_t st);
-int wave_traverse_blocks_per_sm();
+// `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3
+// / 4 blocks per SM; traversal 6 / 8 / 10); `stack`: 32 or 64 entries.
+cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st);
+cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
+cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
 
 }  // namespace oxd

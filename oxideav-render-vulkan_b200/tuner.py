@@ -1,0 +1,119 @@
+"""Autotuner for the tracer's execution plan.
+
+Chooses, per scene and resolution, between the megakernel and the
+wavefront, and within the wavefront the shading kernel's register budget
+(shade_variant), the traversal kernels' occupancy target (trace_variant),
+the traversal stack depth and the number of paths in flight (wave_slots).
+Every plan yields bit-identical accumulators, so the tuner only measures
+time: each candidate runs a short refine at sample indices far from any
+real render's, timed with CUDA events on the tracer's stream, and the
+accumulator is reset afterwards. The search is coordinate descent (one knob
+at a time, keeping the best), which needs ~10 short runs instead of the full
+product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import time
+from dataclasses import asdict, dataclass
+from typing import Callable, Dict, List, Optional
+
+from . import _native as N
+
+TUNE_FIRST_SAMPLE = 1 << 30  # sample indices the tuner uses (not rendered by users)
+
+
+@dataclass
+class Plan:
+    mode: int = N.MODE_WAVEFRONT
+    shade_variant: int = 1
+    trace_variant: int = 1
+    stack: int = 0
+    wave_slots: int = 1 << 20
+
+    def key(self):
+        return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots)
+
+
+SPACE = {
+    "mode": [N.MODE_WAVEFRONT, N.MODE_MEGAKERNEL],
+    "shade_variant": [0, 1, 2],
+    "trace_variant": [0, 1, 2],
+    "stack": [0, 64],
+    "wave_slots": [1 << 19, 1 << 20, 1 << 21],
+}
+WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots")
+
+
+def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] = None,
+                       space: Dict[str, List[int]] = SPACE, log: Optional[list] = None) -> Plan:
+    """Minimise `measure` (seconds) one knob at a time."""
+    best = start or Plan()
+    cache = {}
+
+    def cost(p: Plan) -> float:
+        k = p.key()
+        if k not in cache:
+            cache[k] = measure(p)
+            if log is not None:
+                log.append({"plan": asdict(p), "seconds": cache[k]})
+        return cache[k]
+
+    best_cost = cost(best)
+    for knob, values in space.items():
+        if knob in WAVE_ONLY and best.mode != N.MODE_WAVEFRONT:
+            continue
+        for v in values:
+            if getattr(best, knob) == v:
+                continue
+            cand = Plan(**{**asdict(best), knob: v})
+            c = cost(cand)
+            if c < best_cost:
+                best, best_cost = cand, c
+    return best
+
+
+def apply(tracer, plan: Plan):
+    tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
+                      stack=plan.stack, wave_slots=plan.wave_slots)
+
+
+def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:
+    """Tune `tracer` (already synced to its scene and options) in place and
+    return the chosen plan. Leaves the accumulation reset."""
+    L = N.lib()
+    ctx = tracer.ctx
+    tracer.prepared()  # binds tables and params
+
+    def measure(p: Plan) -> float:
+        apply(tracer, p)
+        best = float("inf")
+        for r in range(repeats + 1):
+            L.oxpt_diag_set_timing(ctx, 1)
+            L.oxpt_diag_timing(ctx, None, None, None, None)
+            t0 = time.perf_counter()
+            st = L.oxpt_refine(ctx, TUNE_FIRST_SAMPLE + 97 * r, spp)
+            if st != N.OK:
+                raise RuntimeError(L.oxpt_last_error(ctx).decode())
+            ms = C.c_double()
+            L.oxpt_diag_timing(ctx, C.byref(ms), None, None, None)
+            L.oxpt_diag_set_timing(ctx, 0)
+            if r > 0 or repeats == 0:  # the first run warms caches and buffers
+                best = min(best, ms.value / 1e3 if ms.value > 0 else time.perf_counter() - t0)
+        return best
+
+    plan = coordinate_descent(measure, log=log)
+    apply(tracer, plan)
+    tracer.reset()
+    return plan
+
+
+def describe(plan: Plan) -> dict:
+    d = asdict(plan)
+    d["mode"] = "wavefront" if plan.mode == N.MODE_WAVEFRONT else "megakernel"
+    return d
+
+
+def dumps(plan: Plan) -> str:
+    return json.dumps(describe(plan))
