@@ -65,7 +65,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     cu, cpp, headers = _sources()
     BUILD.mkdir(parents=True, exist_ok=True)
     nv = nvcc()
-    inc = ["-I", str(ROOT / "include")]
+    inc = ["-I", str(ROOT / "include")] + os.environ.get("OXPT_NVCC_DEFINES", "").split()
     jobs_list = []
     objs = []
     for src in cu:

@@ -16,6 +16,16 @@
 #include "../../include/oxpt.h"
 #include "fmath.h"
 
+// Large shading functions (texture filtering, material, BSDF evaluation and
+// sampling, light sampling) are kept out of line when OXPT_OUTLINE_SHADING
+// is defined: a smaller hot loop against call overhead, chosen by
+// measurement.
+#if defined(OXPT_OUTLINE_SHADING)
+#define OXD_HEAVY __noinline__
+#else
+#define OXD_HEAVY
+#endif
+
 namespace oxd {
 
 constexpr float PI = 3.14159265358979f;
@@ -256,7 +266,7 @@ static __device__ float4 filter_level(const Scene& s, const Level& lv, float2 uv
     float4 t3 = fetch(s, lv, wadd(x0, 1), wadd(y0, 1), ws, wt);
     return mix4(mix4(t0, t1, fx), mix4(t2, t3, fx), fy);
 }
-static __device__ float4 sample_lod(const Scene& s, uint32_t desc, float2 uv, float lod) {
+static __device__ OXD_HEAVY float4 sample_lod(const Scene& s, uint32_t desc, float2 uv, float lod) {
     uint32_t levels = tw(s, desc), flags = tw(s, desc + 1u);
     uint32_t ws = flags & 3u, wt = (flags >> 2u) & 3u, minf = (flags >> 5u) & 7u;
     bool lin = minf == 1u || minf == 3u || minf == 5u;
@@ -309,7 +319,7 @@ static __device__ float cone_lod(const Scene& s, uint32_t o, uint32_t slot, cons
     float l = 0.5f * fm_log2(ta / pa) + fm_log2(lod.width / c);
     return finite(l) ? l : 0.0f;
 }
-static __device__ float4 slot_sample(const Scene& s, uint32_t m, uint32_t k, uint32_t slot, f3 b, const Lod& lod) {
+static __device__ OXD_HEAVY float4 slot_sample(const Scene& s, uint32_t m, uint32_t k, uint32_t slot, f3 b, const Lod& lod) {
     uint32_t o = slot_word(s, m, k);
     uint32_t uvset = tw(s, o + 1u);
     float2 a0 = vertex_uv(s, slot, uvset, 0u), a1 = vertex_uv(s, slot, uvset, 1u), a2 = vertex_uv(s, slot, uvset, 2u);

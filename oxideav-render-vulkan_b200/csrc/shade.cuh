@@ -55,7 +55,7 @@ static __device__ f3 perturb(const Scene& s, uint32_t slot, f3 b, f3 n, float4 t
 
 // material() (pathtrace.wgsl:842-902). Slots are sampled in order; an
 // absent slot is white. `m` is the hit's material index.
-static __device__ Mat material(const Scene& s, uint32_t slot, uint32_t m, f3 b, f3 sn_in, const Lod& lod, bool flip) {
+static __device__ OXD_HEAVY Mat material(const Scene& s, uint32_t slot, uint32_t m, f3 b, f3 sn_in, const Lod& lod, bool flip) {
     f3 sn = flip ? -sn_in : sn_in;
     uint32_t o = mat_off(s, m);
     float4 tex[13];
@@ -213,7 +213,7 @@ __device__ __forceinline__ f3 fresnel_d(const Bsdf& bs, float c) {
     }
     return schlick(bs.f0d, c);
 }
-static __device__ Bsdf make_bsdf(const float* lut, const Mat& m, f3 v, f3 ng_in, bool front) {
+static __device__ OXD_HEAVY Bsdf make_bsdf(const float* lut, const Mat& m, f3 v, f3 ng_in, bool front) {
     float fl = front ? 1.0f : -1.0f;
     f3 ng = ng_in * fl;
     f3 n = m.normal * fl;
@@ -287,7 +287,7 @@ struct Eval {
     f3 f;
     float pdf;
 };
-static __device__ Eval bsdf_eval(const float* lut, const Bsdf& b, f3 l) {
+static __device__ OXD_HEAVY Eval bsdf_eval(const float* lut, const Bsdf& b, f3 l) {
     f3 v = b.v, n = b.n;
     float nv = fmaxf(dot(n, v), 1.0e-4f);
     if (dot(b.ng, l) > 0.0f) {
@@ -364,7 +364,7 @@ struct BSample {
     f3 l, f;
     float pdf;
 };
-static __device__ BSample bsdf_sample(const float* lut, const Bsdf& b, float ux, float uy, float uz) {
+static __device__ OXD_HEAVY BSample bsdf_sample(const float* lut, const Bsdf& b, float ux, float uy, float uz) {
     BSample res;
     res.ok = false;
     float acc = 0.0f;
@@ -484,7 +484,7 @@ __device__ __forceinline__ float triangle_solid_angle(f3 p, f3 a0, f3 b0, f3 c0)
     float o = 2.0f * fm_atan2(num, den);
     return finite(o) ? fmaxf(o, 0.0f) : 0.0f;
 }
-static __device__ f3 sample_spherical_triangle(f3 p, f3 a0, f3 b0, f3 c0, float u0, float u1) {
+static __device__ OXD_HEAVY f3 sample_spherical_triangle(f3 p, f3 a0, f3 b0, f3 c0, float u0, float u1) {
     f3 zero = sp(0.0f);
     f3 a = nrm_any(a0 - p), b = nrm_any(b0 - p), c = nrm_any(c0 - p);
     f3 nab = nrm_any(cross(a, b)), nbc = nrm_any(cross(b, c)), nca = nrm_any(cross(c, a));
@@ -558,7 +558,7 @@ struct EnvSample {
     f3 d, le;
     float pdf;
 };
-static __device__ EnvSample env_sample(const Scene& s, float u0, float u1) {
+static __device__ OXD_HEAVY EnvSample env_sample(const Scene& s, float u0, float u1) {
     EnvSample r;
     r.ok = false;
     uint32_t w = s.P.env[0], h = s.P.env[1];
