@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", default="auto", choices=["auto", "mega", "wave"],
+    ap.add_argument("--mode", default="auto", choices=["auto", "mega", "wave", "split"],
                     help="execution plan; auto = the library default")
     ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
@@ -244,7 +244,7 @@ def main():
     if a.mode != "auto" or a.slots:
         kw = {"wave_slots": a.slots} if a.slots else {}
         if a.mode != "auto":
-            kw["mode"] = 0 if a.mode == "mega" else 1
+            kw["mode"] = {"mega": 0, "wave": 1, "split": 2}[a.mode]
         pt.set_tuning(**kw)
     elif not a.no_tune:
         from oxideav_render_vulkan_b200 import tuner
@@ -267,6 +267,9 @@ def main():
         "wave_logic": (BYTES_ATTR + BYTES_MAT) * c[6] / npaths,
         "wave_extend": (BYTES_AABB * h0[3] + BYTES_TRI * h0[5]) / npaths,
         "wave_shadow": (BYTES_AABB * h1[3] + BYTES_TRI * h1[5]) / npaths,
+        "split_logic": 0.0,
+        "split_shade": (BYTES_ATTR + BYTES_MAT) * c[6] / npaths,
+        "split_nee": 0.0,
     }
     rays_per_path = (c[1] + c[2]) / npaths
 
@@ -315,7 +318,10 @@ def main():
     L.oxpt_diag_timing_kinds(pt.ctx, kms, kn)
     wave = pt.tuning().mode == 1
     paths_timed = paths_step * a.steps
-    kinds = ((2, "wave_logic"), (3, "wave_extend"), (4, "wave_shadow")) if wave else ((0, "trace_paths"),)
+    mode = pt.tuning().mode
+    kinds = {0: ((0, "trace_paths"),), 1: ((2, "wave_logic"), (3, "wave_extend"), (4, "wave_shadow")),
+             2: ((2, "split_logic"), (5, "split_shade"), (6, "split_nee"), (3, "wave_extend"),
+                 (4, "wave_shadow"))}[mode]
     traffic_db = {}
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -377,8 +383,9 @@ def main():
 
 def plan_of(pt):
     t = pt.tuning()
-    return {"mode": ["megakernel", "wavefront"][t.mode], "wave_slots": t.wave_slots,
-            "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack}
+    return {"mode": ["megakernel", "wavefront", "wavefront-split"][t.mode], "wave_slots": t.wave_slots,
+            "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack,
+            "nee_variant": t.nee_variant}
 
 
 def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank):

@@ -66,7 +66,8 @@ oxpt_status oxpt_diag_timing(oxpt_ctx* ctx, double* trace_ms, uint64_t* trace_la
 /* The per-kind figures of the last oxpt_diag_timing call: kind 0 the trace
  * phase of each launch (the megakernel, or a whole wavefront run), 1 the
  * ordered reduce, 2 wavefront logic, 3 wavefront extension traversal, 4
- * wavefront shadow traversal. */
+ * wavefront shadow traversal, 5 split-wavefront shading, 6 split-wavefront
+ * NEE. */
 oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* ctx, double ms[8], uint64_t n[8]);
 /* The last oxpt_diag_refine_counted totals split by ray kind: out[0..7] for
  * continuation rays and shading (wavefront logic + extension), out[8..15]
@@ -94,10 +95,15 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *   shade_variant  wavefront logic kernel compiled for 2 / 3 / 4 resident
  *                  blocks per SM (0 / 1 / 2): registers against occupancy.
  *   trace_variant  wavefront traversal kernels for 6 / 8 / 10 blocks.
+ *   nee_variant    split wavefront NEE kernel for 4 / 5 / 6 blocks.
+ *   OXPT_MODE_WAVEFRONT_SPLIT: the wavefront with the shading of a bounce
+ *                  in three kernels (path logic, surface shading, one thread
+ *                  per NEE job); shade_variant then applies to the shading
+ *                  kernel.
  *   stack          traversal stack entries: 32 or 64; 0 = 32 when the BVH
  *                  is at most 32 levels deep, else 64 (exact either way).
  */
-enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1 };
+enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1, OXPT_MODE_WAVEFRONT_SPLIT = 2 };
 typedef struct oxpt_tuning {
     uint32_t mode;
     uint32_t threads;
@@ -109,6 +115,8 @@ typedef struct oxpt_tuning {
     uint32_t shade_variant;
     uint32_t trace_variant;
     uint32_t stack;
+    uint32_t nee_variant;
+    uint32_t reserved;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);

@@ -70,7 +70,7 @@ struct oxpt_ctx {
     uint32_t wave_slots = 1u << 20;
     uint64_t wave_items = 1ull << 24;
     uint32_t check_every = 4;
-    uint32_t shade_variant = 1, trace_variant = 1, stack = 0;
+    uint32_t shade_variant = 1, trace_variant = 1, nee_variant = 1, stack = 0;
     uint32_t bvh_depth = 0;
     void* wave_mem = nullptr;
     size_t wave_bytes = 0;
@@ -190,8 +190,11 @@ uint32_t bvh_depth_of(const uint32_t* geom, uint32_t nodes) {
 oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveState* st, oxd::WaveQueues* q,
                         uint32_t** ctr, unsigned long long** work) {
     size_t P = slots, PJ = (size_t)slots * jobs;
+    bool split = c->mode == OXPT_MODE_WAVEFRONT_SPLIT;
     size_t sizes[] = {P * 8, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 4, P * 4,
-                      PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64};
+                      PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64,
+                      split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0};
+    constexpr int NB = 20;
     size_t total = 0;
     for (size_t s : sizes) total += align256(s);
     if (slots > c->wave_cap_slots || jobs > c->wave_cap_jobs || total > c->wave_bytes) {
@@ -209,11 +212,14 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
         c->wave_cap_jobs = jobs;
     }
     char* p = (char*)c->wave_mem;
-    void* ptr[17];
-    for (int k = 0; k < 17; k++) {
+    void* ptr[NB];
+    for (int k = 0; k < NB; k++) {
         ptr[k] = p;
         p += align256(sizes[k]);
     }
+    q->shade = split ? (uint32_t*)ptr[17] : nullptr;
+    q->vslot = split ? (uint32_t*)ptr[18] : nullptr;
+    q->vrec = split ? (float4*)ptr[19] : nullptr;
     st->item = (unsigned long long*)ptr[0];
     st->seed = (uint4*)ptr[1];
     st->beta = (float4*)ptr[2];
@@ -253,6 +259,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     if (s) return s;
     wa.s = ta.s;
     wa.slots = P;
+    wa.vcap = P;
     wa.jobs = J;
     wa.first = ta.first;
     wa.y0 = ta.y0;
@@ -287,9 +294,19 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     };
     for (uint64_t it = 0;; it++) {
         if (it > cap) return fail(c, OXPT_E_TIMEOUT, "wavefront did not drain within its iteration bound");
-        CK(c, cudaMemsetAsync(wa.ctr, 0, 16, c->stream), "queue reset");
-        CK(c, timed(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, c->stream); }),
-           "wave logic");
+        CK(c, cudaMemsetAsync(wa.ctr, 0, 32, c->stream), "queue reset");
+        if (c->mode == OXPT_MODE_WAVEFRONT_SPLIT) {
+            CK(c, timed(2, [&] { return oxd::launch_split_logic(wa, count, c->stream); }), "split logic");
+            CK(c, timed(5, [&] {
+                   return oxd::launch_split_shade(wa, count, (int)c->shade_variant, c->sms, c->stream);
+               }), "split shade");
+            CK(c, timed(6, [&] { return oxd::launch_split_nee(wa, count, (int)c->nee_variant, c->sms, c->stream); }),
+               "split nee");
+            c->launches += 2;
+        } else {
+            CK(c, timed(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, c->stream); }),
+               "wave logic");
+        }
         CK(c, timed(3, [&] {
                return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, sd, c->sms, c->stream);
            }), "wave extend");
@@ -313,7 +330,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
 oxpt_status run_frame(oxpt_ctx* c, const oxpt_frame& f, bool count) {
     if (f.count == 0 || f.rows == 0) return OXPT_OK;
     if (f.y0 >= c->h || f.rows > c->h - f.y0) return fail(c, OXPT_E_INVALID, "frame rows outside the image");
-    bool wave = c->mode == OXPT_MODE_WAVEFRONT;
+    bool wave = c->mode != OXPT_MODE_MEGAKERNEL;
     uint64_t cap = std::max<uint64_t>(wave ? c->wave_items : c->max_paths, c->w);
     uint32_t rows_per = f.rows, per = f.count;
     uint64_t row_paths = (uint64_t)c->w * f.rows;
@@ -728,7 +745,7 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* c, uint32_t threads, uint32_t blocks_
 
 oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     if (!c || !t) return OXPT_E_INVALID;
-    if (t->mode > OXPT_MODE_WAVEFRONT) return fail(c, OXPT_E_INVALID, "unknown execution mode");
+    if (t->mode > OXPT_MODE_WAVEFRONT_SPLIT) return fail(c, OXPT_E_INVALID, "unknown execution mode");
     if (t->threads && (t->threads % 32 != 0 || t->threads > oxd::TRACE_THREADS))
         return fail(c, OXPT_E_INVALID, "threads must be a multiple of 32 and at most the kernel's block bound");
     if (t->wave_slots > (1u << 26)) return fail(c, OXPT_E_LIMIT, "at most 2^26 wavefront slots");
@@ -739,11 +756,13 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     c->max_paths = t->max_paths ? t->max_paths : (1ull << 22);
     c->wave_items = t->wave_items ? t->wave_items : (1ull << 24);
     c->check_every = t->check_every ? t->check_every : 4u;
-    if (t->shade_variant > 2 || t->trace_variant > 2) return fail(c, OXPT_E_INVALID, "variants are 0, 1 or 2");
+    if (t->shade_variant > 2 || t->trace_variant > 2 || t->nee_variant > 2)
+        return fail(c, OXPT_E_INVALID, "variants are 0, 1 or 2");
     if (t->stack && t->stack != 32 && t->stack != 64) return fail(c, OXPT_E_INVALID, "stack is 0, 32 or 64");
     if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
     c->shade_variant = t->shade_variant;
     c->trace_variant = t->trace_variant;
+    c->nee_variant = t->nee_variant;
     c->stack = t->stack;
     return OXPT_OK;
 }
@@ -760,6 +779,7 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->check_every = c->check_every;
     t->shade_variant = c->shade_variant;
     t->trace_variant = c->trace_variant;
+    t->nee_variant = c->nee_variant;
     t->stack = c->stack;
     return OXPT_OK;
 }

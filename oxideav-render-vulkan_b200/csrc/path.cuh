@@ -74,14 +74,12 @@ __device__ __forceinline__ f3 start_path(const Scene& s, const uint32_t* sobol, 
     return o;
 }
 
-enum HitOutcome { PATH_DONE = 0, PATH_UNCOVERED = 1, PATH_VERTEX = 2 };
+enum HitOutcome { PATH_DONE = 0, PATH_UNCOVERED = 1, PATH_VERTEX = 2, PATH_SURFACE = 3 };
 
-// The PATH branch after a continuation ray (pathtrace.wgsl:1773-1861).
-// PATH_VERTEX: *v holds the vertex and NEE / BSDF sampling follow.
-template <bool COUNT>
-__device__ __forceinline__ int on_path_hit(const Scene& s, const float* sheen, const uint32_t* sobol,
-                                           const Sampler& smp, PathCore& pc, bool got, const Hit& hit,
-                                           uint32_t hmat, Vertex* v, unsigned long long* shaded) {
+// The start of the PATH branch (pathtrace.wgsl:1773-1798): medium
+// attenuation, then a miss (environment / ambient with MIS). PATH_SURFACE:
+// a surface was hit and shade_hit follows.
+__device__ __forceinline__ int after_ray(const Scene& s, PathCore& pc, bool got, const Hit& hit) {
     const uint32_t strategy = s.P.cfg[1];
     if (pc.in_medium) {
         if (!got) return PATH_DONE;
@@ -101,6 +99,17 @@ __device__ __forceinline__ int on_path_hit(const Scene& s, const float* sheen, c
         if (w > 0.0f) pc.radiance = pc.radiance + clamp_c(s, pc.beta * le * w);
         return PATH_DONE;
     }
+    return PATH_SURFACE;
+}
+
+// The rest of the PATH branch at a surface hit (pathtrace.wgsl:1799-1861):
+// emission with MIS, unlit, the bounce limit and the vertex's BSDF.
+// PATH_VERTEX: *v holds the vertex and NEE / BSDF sampling follow.
+template <bool COUNT>
+__device__ __forceinline__ int shade_hit(const Scene& s, const float* sheen, const uint32_t* sobol,
+                                         const Sampler& smp, PathCore& pc, const Hit& hit, uint32_t hmat,
+                                         Vertex* v, unsigned long long* shaded) {
+    const uint32_t strategy = s.P.cfg[1];
     if (COUNT) *shaded += 1;
     Surface surf = surface(s, hit.slot, hit.b);
     uint32_t mflags = mat_flags(s, hmat);
@@ -148,6 +157,16 @@ __device__ __forceinline__ int on_path_hit(const Scene& s, const float* sheen, c
     v->front = hit.front;
     v->pl_u = pattern(sobol, smp, 2u + 2u * pc.k);
     return PATH_VERTEX;
+}
+
+// The whole PATH branch after a continuation ray.
+template <bool COUNT>
+__device__ __forceinline__ int on_path_hit(const Scene& s, const float* sheen, const uint32_t* sobol,
+                                           const Sampler& smp, PathCore& pc, bool got, const Hit& hit,
+                                           uint32_t hmat, Vertex* v, unsigned long long* shaded) {
+    int r = after_ray(s, pc, got, hit);
+    if (r != PATH_SURFACE) return r;
+    return shade_hit<COUNT>(s, sheen, sobol, smp, pc, hit, hmat, v, shaded);
 }
 
 // NEE job `job` of vertex v (pathtrace.wgsl:1863-1993). True when it arms

@@ -1,0 +1,304 @@
+// Split wavefront: the shading work of a bounce in three small kernels.
+//
+// The single wavefront logic kernel (wavefront.cu) carries texture
+// filtering, the layered BSDF, light sampling and path bookkeeping in one
+// body whose code does not fit the instruction cache. Here a bounce is
+//   split_logic  one thread per slot: adds the previous vertex's visible NEE
+//                terms in job order, attenuates in a medium, handles misses
+//                (environment / ambient), finalises finished paths and
+//                regenerates their slots; surface hits go to a shade queue;
+//   split_shade  one thread per queued hit: emission, material, BSDF of the
+//                vertex (written to a vertex record for split_nee), BSDF
+//                sampling and roulette; queues the continuation ray;
+//   split_nee    one thread per (vertex, NEE job), job-major so that a warp
+//                evaluates the same light for 32 vertices;
+// followed by the same extension and shadow traversal kernels. Every path
+// still receives its contributions in the reference's order: the vertex's
+// NEE terms are added by the next split_logic before anything the next
+// continuation ray finds.
+#include <cooperative_groups.h>
+
+#include "kernels.cuh"
+#include "path.cuh"
+#include "shade.cuh"
+#include "traverse.cuh"
+#include "wavefront.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace oxd {
+
+namespace {
+
+enum : uint32_t { ST_EMPTY = 0, ST_TRACING = 1, ST_ENDING = 2 };
+
+__device__ __forceinline__ uint32_t append1(uint32_t* ctr) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+__device__ __forceinline__ unsigned long long fetch1(unsigned long long* ctr) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, (unsigned long long)g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
+__device__ __forceinline__ void load_state(const WaveArgs& a, uint32_t i, PathCore* pc, Sampler* smp) {
+    uint4 sd = a.st.seed[i];
+    float4 b = a.st.beta[i], r = a.st.rad[i], d = a.st.dir[i], pp = a.st.prev[i], sg = a.st.sigma[i];
+    smp->pixel_seed = sd.x;
+    smp->index = sd.y;
+    smp->path_seed = sd.z;
+    pc->k = sd.w;
+    pc->beta = xyz(b);
+    pc->prev_pdf = b.w;
+    pc->radiance = xyz(r);
+    pc->in_medium = (__float_as_uint(r.w) & 4u) != 0u;
+    pc->d = xyz(d);
+    pc->prev_pos = xyz(pp);
+    pc->sigma = xyz(sg);
+}
+
+__device__ __forceinline__ void save_state(const WaveArgs& a, uint32_t i, const PathCore& pc, const Sampler& smp,
+                                           uint32_t stage) {
+    a.st.seed[i] = make_uint4(smp.pixel_seed, smp.index, smp.path_seed, pc.k);
+    a.st.beta[i] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, pc.prev_pdf);
+    a.st.rad[i] = make_float4(pc.radiance.x, pc.radiance.y, pc.radiance.z,
+                              __uint_as_float(stage | (pc.in_medium ? 4u : 0u)));
+    a.st.dir[i] = make_float4(pc.d.x, pc.d.y, pc.d.z, 0.0f);
+    a.st.prev[i] = make_float4(pc.prev_pos.x, pc.prev_pos.y, pc.prev_pos.z, 0.0f);
+    a.st.sigma[i] = make_float4(pc.sigma.x, pc.sigma.y, pc.sigma.z, 0.0f);
+}
+
+__device__ __forceinline__ Hit load_hit(const WaveArgs& a, uint32_t i, uint32_t* hmat) {
+    uint4 hb = a.st.hit[i];
+    uint32_t hm = a.st.hmeta[i];
+    Hit h;
+    h.slot = hb.x;
+    h.t = __uint_as_float(hb.y);
+    float u = __uint_as_float(hb.z), v = __uint_as_float(hb.w);
+    h.b = mk(1.0f - u - v, u, v);
+    h.front = (hm >> 31) != 0u;
+    *hmat = hm & 0x7fffffffu;
+    return h;
+}
+
+// Vertex record, 13 float4 fields stored field-major (a warp's loads of one
+// field are contiguous).
+constexpr uint32_t VREC = 13;
+
+__device__ __forceinline__ void put_vertex(const WaveArgs& a, uint32_t v, const Vertex& x, const PathCore& pc,
+                                           uint32_t path_seed) {
+    const uint32_t P = a.vcap;
+    const Bsdf& b = x.bsdf;
+    float4* r = a.q.vrec;
+    r[0 * P + v] = make_float4(b.v.x, b.v.y, b.v.z, b.metallic);
+    r[1 * P + v] = make_float4(b.n.x, b.n.y, b.n.z, b.alpha);
+    r[2 * P + v] = make_float4(b.ng.x, b.ng.y, b.ng.z, b.specular);
+    r[3 * P + v] = make_float4(b.ncc.x, b.ncc.y, b.ncc.z, b.transmission);
+    r[4 * P + v] = make_float4(b.base.x, b.base.y, b.base.z, b.clearcoat);
+    r[5 * P + v] = make_float4(b.f0d.x, b.f0d.y, b.f0d.z, b.cc_alpha);
+    r[6 * P + v] = make_float4(b.sheen.x, b.sheen.y, b.sheen.z, b.sheen_rough);
+    r[7 * P + v] = make_float4(b.eta_i, b.eta_t, b.sheen_alpha, b.w_cc);
+    r[8 * P + v] = make_float4(b.p0, b.p1, b.p2, b.p3);
+    r[9 * P + v] = make_float4(b.p4, __uint_as_float(b.thin ? 1u : 0u), __uint_as_float(pc.k), __uint_as_float(path_seed));
+    r[10 * P + v] = make_float4(x.p.x, x.p.y, x.p.z, 0.0f);
+    r[11 * P + v] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, 0.0f);
+    r[12 * P + v] = x.pl_u;
+}
+
+__device__ __forceinline__ void get_vertex(const WaveArgs& a, uint32_t v, Vertex* x, PathCore* pc,
+                                           uint32_t* path_seed) {
+    const uint32_t P = a.vcap;
+    const float4* r = a.q.vrec;
+    Bsdf& b = x->bsdf;
+    float4 f;
+    f = r[0 * P + v]; b.v = xyz(f); b.metallic = f.w;
+    f = r[1 * P + v]; b.n = xyz(f); b.alpha = f.w;
+    f = r[2 * P + v]; b.ng = xyz(f); b.specular = f.w;
+    f = r[3 * P + v]; b.ncc = xyz(f); b.transmission = f.w;
+    f = r[4 * P + v]; b.base = xyz(f); b.clearcoat = f.w;
+    f = r[5 * P + v]; b.f0d = xyz(f); b.cc_alpha = f.w;
+    f = r[6 * P + v]; b.sheen = xyz(f); b.sheen_rough = f.w;
+    f = r[7 * P + v]; b.eta_i = f.x; b.eta_t = f.y; b.sheen_alpha = f.z; b.w_cc = f.w;
+    f = r[8 * P + v]; b.p0 = f.x; b.p1 = f.y; b.p2 = f.z; b.p3 = f.w;
+    f = r[9 * P + v];
+    b.p4 = f.x;
+    b.thin = __float_as_uint(f.y) != 0u;
+    pc->k = __float_as_uint(f.z);
+    *path_seed = __float_as_uint(f.w);
+    f = r[10 * P + v]; x->p = xyz(f);
+    f = r[11 * P + v]; pc->beta = xyz(f);
+    x->pl_u = r[12 * P + v];
+    x->ng = b.ng;
+}
+
+}  // namespace
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ WaveArgs a) {
+    __shared__ uint32_t s_sobol[128];
+    const Scene& s = a.s;
+    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s, s.P.offs0[0] + i);
+    __syncthreads();
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.slots) return;
+    const uint32_t J = a.jobs;
+    PathCore pc;
+    Sampler smp;
+    uint32_t stage = __float_as_uint(a.st.rad[i].w) & 3u;
+    bool need_new = stage == ST_EMPTY;
+    if (!need_new) {
+        load_state(a, i, &pc, &smp);
+        uint32_t n = a.st.nee_n[i];
+        for (uint32_t j = 0; j < n; j++) {
+            float4 pe = a.st.pend[(uint64_t)i * J + j];
+            if (pe.w == 2.0f) pc.radiance = pc.radiance + xyz(pe);
+        }
+        if (n) a.st.nee_n[i] = 0u;
+        int r = PATH_DONE;
+        if (stage == ST_TRACING) {
+            uint32_t hmat;
+            Hit hit = load_hit(a, i, &hmat);
+            r = after_ray(s, pc, hit.slot != NONE, hit);
+        }
+        if (r == PATH_SURFACE) {
+            save_state(a, i, pc, smp, ST_TRACING);
+            a.q.shade[append1(&a.ctr[3])] = i;
+            append1(&a.ctr[2]);
+            return;
+        }
+        a.out[a.st.item[i]] = path_result(pc, r != PATH_UNCOVERED);
+        need_new = true;
+    }
+    unsigned long long item = fetch1(a.work);
+    if (item < a.total) {
+        uint32_t it = (uint32_t)(item / a.npix);
+        uint32_t q = (uint32_t)(item - (unsigned long long)it * a.npix);
+        uint32_t yy = q / s.P.dims[0];
+        f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], a.y0 + yy, a.first + it, &smp, &pc);
+        a.st.item[i] = item;
+        save_state(a, i, pc, smp, ST_TRACING);
+        a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
+        a.q.ext[append1(&a.ctr[0])] = i;
+        append1(&a.ctr[2]);
+        if (COUNT) atomicAdd(a.counters + C_PATHS, 1ull);
+    } else if (stage != ST_EMPTY) {
+        float4 r = a.st.rad[i];
+        r.w = __uint_as_float(ST_EMPTY);
+        a.st.rad[i] = r;
+    }
+}
+
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__ WaveArgs a) {
+    __shared__ uint32_t s_sobol[128];
+    __shared__ float s_sheen[512];
+    const Scene& s = a.s;
+    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s, s.P.offs0[0] + i);
+    for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s, s.P.offs0[1] + i);
+    __syncthreads();
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[3]);
+    unsigned long long shaded = 0;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        uint32_t i = a.q.shade[q];
+        PathCore pc;
+        Sampler smp;
+        load_state(a, i, &pc, &smp);
+        uint32_t hmat;
+        Hit hit = load_hit(a, i, &hmat);
+        Vertex vx;
+        int r = shade_hit<COUNT>(s, s_sheen, s_sobol, smp, pc, hit, hmat, &vx, &shaded);
+        if (r != PATH_VERTEX) {
+            save_state(a, i, pc, smp, ST_ENDING);
+            continue;
+        }
+        uint32_t v = append1(&a.ctr[4]);
+        put_vertex(a, v, vx, pc, smp.path_seed);
+        a.q.vslot[v] = i;
+        a.st.nee_n[i] = a.jobs;
+        f3 o;
+        if (continue_path(s, s_sheen, s_sobol, smp, pc, vx, &o)) {
+            save_state(a, i, pc, smp, ST_TRACING);
+            a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
+            a.q.ext[append1(&a.ctr[0])] = i;
+        } else {
+            save_state(a, i, pc, smp, ST_ENDING);
+        }
+    }
+    if (COUNT && shaded) atomicAdd(a.counters + C_SHADED, shaded);
+}
+
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(128, MINB) split_nee(const __grid_constant__ WaveArgs a) {
+    __shared__ float s_sheen[512];
+    const Scene& s = a.s;
+    for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s, s.P.offs0[1] + i);
+    __syncthreads();
+    const uint32_t nv = *((volatile uint32_t*)&a.ctr[4]);
+    const uint64_t total = (uint64_t)nv * a.jobs;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t j = (uint32_t)(t / nv);
+        uint32_t v = (uint32_t)(t - (uint64_t)j * nv);
+        uint32_t slot = a.q.vslot[v];
+        Vertex vx;
+        PathCore pc;
+        uint32_t path_seed;
+        get_vertex(a, v, &vx, &pc, &path_seed);
+        ShadowRay sr;
+        float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (nee_job(s, s_sheen, pc, vx, j, &sr)) {
+            pe = make_float4(sr.pending.x, sr.pending.y, sr.pending.z, 1.0f);
+            uint32_t q = append1(&a.ctr[1]);
+            a.q.sh_o[q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+            a.q.sh_d[q] = make_float4(sr.d.x, sr.d.y, sr.d.z, __uint_as_float(sr.skip));
+            a.q.sh_m[q] = make_uint4(slot, j, sr.rid, path_seed);
+        }
+        a.st.pend[(uint64_t)slot * a.jobs + j] = pe;
+    }
+}
+
+// Variants: shade kernel for 2 / 3 / 4 resident blocks per SM; the NEE
+// kernel for 4 / 5 / 6.
+template <bool C>
+static void* shade_fn(int v) {
+    if (v == 0) return (void*)split_shade<C, 2>;
+    if (v == 1) return (void*)split_shade<C, 3>;
+    return (void*)split_shade<C, 4>;
+}
+template <bool C>
+static void* nee_fn(int v) {
+    if (v == 0) return (void*)split_nee<C, 4>;
+    if (v == 1) return (void*)split_nee<C, 5>;
+    return (void*)split_nee<C, 6>;
+}
+
+static cudaError_t persistent(void* fn, const WaveArgs& a, int sms, cudaStream_t st) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0);
+    WaveArgs copy = a;
+    void* args[] = {&copy};
+    return cudaLaunchKernel(fn, dim3((unsigned)(sms * (per_sm > 0 ? per_sm : 1))), dim3(128), args, 0, st);
+}
+
+cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st) {
+    unsigned blocks = (a.slots + 127u) / 128u;
+    if (count) split_logic<true><<<blocks, 128, 0, st>>>(a);
+    else split_logic<false><<<blocks, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_shade(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st) {
+    variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
+    return persistent(count ? shade_fn<true>(variant) : shade_fn<false>(variant), a, sms, st);
+}
+
+cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st) {
+    variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
+    return persistent(count ? nee_fn<true>(variant) : nee_fn<false>(variant), a, sms, st);
+}
+
+}  // namespace oxd

@@ -32,17 +32,22 @@ struct WaveQueues {
     float4* sh_o;   // shadow ray origin, t_max
     float4* sh_d;   // shadow ray direction, skip id bits
     uint4* sh_m;    // slot, job, ray id, path seed
+    // split wavefront (wave_split.cu)
+    uint32_t* shade;  // slot ids with a surface hit to shade
+    uint32_t* vslot;  // vertex record -> slot
+    float4* vrec;     // vertex records, 13 float4 fields, field-major
 };
 
 struct WaveArgs {
     Scene s;
     WaveState st;
     WaveQueues q;
-    uint32_t slots, jobs;
+    uint32_t slots, jobs, vcap;
     uint32_t first, y0, npix;
     unsigned long long total;   // items of this launch (npix x samples)
     unsigned long long* work;   // next item
-    uint32_t* ctr;              // [0] continuation rays, [1] shadow rays, [2] active slots
+    uint32_t* ctr;              // [0] continuation rays, [1] shadow rays, [2] active slots,
+                                // [3] hits to shade, [4] vertex records
     float4* out;
     unsigned long long* counters;
     uint32_t* err;
@@ -53,5 +58,10 @@ struct WaveArgs {
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st);
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
 cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
+// Split wavefront (wave_split.cu); shade variants 2 / 3 / 4 blocks per SM,
+// NEE variants 4 / 5 / 6.
+cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st);
+cudaError_t launch_split_shade(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st);
+cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st);
 
 }  // namespace oxd

@@ -31,19 +31,22 @@ class Plan:
     trace_variant: int = 1
     stack: int = 0
     wave_slots: int = 1 << 20
+    nee_variant: int = 0
 
     def key(self):
-        return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots)
+        return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant)
 
 
 SPACE = {
-    "mode": [N.MODE_WAVEFRONT, N.MODE_MEGAKERNEL],
+    "mode": [N.MODE_WAVEFRONT, N.MODE_WAVEFRONT_SPLIT, N.MODE_MEGAKERNEL],
     "shade_variant": [0, 1, 2],
     "trace_variant": [0, 1, 2],
     "stack": [0, 64],
     "wave_slots": [1 << 19, 1 << 20, 1 << 21],
+    "nee_variant": [0, 1, 2],
 }
-WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots")
+WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant")
+SPLIT_ONLY = ("nee_variant",)
 
 
 def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] = None,
@@ -62,7 +65,9 @@ def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] =
 
     best_cost = cost(best)
     for knob, values in space.items():
-        if knob in WAVE_ONLY and best.mode != N.MODE_WAVEFRONT:
+        if knob in WAVE_ONLY and best.mode == N.MODE_MEGAKERNEL:
+            continue
+        if knob in SPLIT_ONLY and best.mode != N.MODE_WAVEFRONT_SPLIT:
             continue
         for v in values:
             if getattr(best, knob) == v:
@@ -76,7 +81,7 @@ def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] =
 
 def apply(tracer, plan: Plan):
     tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
-                      stack=plan.stack, wave_slots=plan.wave_slots)
+                      stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant)
 
 
 def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:
@@ -111,7 +116,8 @@ def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> 
 
 def describe(plan: Plan) -> dict:
     d = asdict(plan)
-    d["mode"] = "wavefront" if plan.mode == N.MODE_WAVEFRONT else "megakernel"
+    d["mode"] = {N.MODE_WAVEFRONT: "wavefront", N.MODE_WAVEFRONT_SPLIT: "wavefront-split"}.get(plan.mode,
+                                                                                           "megakernel")
     return d
 
 

@@ -198,7 +198,7 @@ def test_images_vs_libm_oracle_psnr_at_least_60db(pkg, oracle):
     assert psnr >= 60.0, psnr
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("which", ["materials", "layered", "alpha"])
 def test_both_execution_modes_bit_exact(pkg, oracle, mode, which):
     """Megakernel and wavefront plans give the oracle's accumulator, also
@@ -219,7 +219,7 @@ def test_both_execution_modes_bit_exact(pkg, oracle, mode, which):
     assert np.array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 def test_traversal_counters_match_oracle(pkg, oracle, mode):
     opts = _opts(pkg, 48, 32, 4)
     t = _tracer(pkg, scenes.materials_scene(pkg), opts)

@@ -42,7 +42,7 @@ def test_megakernel_skips_wavefront_knobs(pkg):
 
     best = tuner.coordinate_descent(cost)
     assert best.mode == N.MODE_MEGAKERNEL
-    assert len(seen) == 2
+    assert len(seen) == 3
 
 
 @pytest.mark.gpu
