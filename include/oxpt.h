@@ -179,6 +179,49 @@ oxpt_status oxpt_read_accum(oxpt_ctx* ctx, float* host_out);
  * that writes into it. No counterpart in the reference (single device). */
 oxpt_status oxpt_accum_view(oxpt_ctx* ctx, oxpt_devimage* out);
 
+/*
+ * Allocation-free dispatch. This entry point has no counterpart in the
+ * reference.
+ *
+ * For callers that may not let a library allocate or free device memory:
+ * an application that owns all device memory through its own allocator and
+ * hands each component the buffers it may use, or one that cannot afford
+ * the device synchronisation that cudaMalloc / cudaFree can cause in the
+ * middle of a frame. Everything here is the caller's: the scene buffers
+ * (device pointers, in the layouts of oxpt_scene_desc / oxpt_set_tables),
+ * the Params, and the accumulator (device pointer, w*h*4 floats, updated in
+ * place exactly as oxpt_dispatch updates the context's accumulator, so the
+ * results are bit-identical). No context is needed and nothing is
+ * allocated: the per-path scratch of the dispatch lives in a fixed array
+ * of OXPT_NOALLOC_MAX_PATHS x 16 bytes (4 MiB) that every GPU loading the
+ * library holds until the process exits; larger frames run as several
+ * launches over it. An image row wider than OXPT_NOALLOC_MAX_PATHS pixels
+ * is rejected with OXPT_E_LIMIT.
+ *
+ * The first call on a device looks up the array's device address with
+ * that device current (so make that first call before any stream capture).
+ * Launches go to `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) and the call returns without waiting. All calls share the one
+ * array, which keeps the previous call's contents: calls whose work
+ * overlaps on the GPU (different streams, or different host threads on the
+ * same device) race on it and must be ordered by the caller. A malformed
+ * BVH is cut short on the device, not reported.
+ */
+#define OXPT_NOALLOC_MAX_PATHS (1u << 18)
+typedef struct oxpt_device_scene {
+    const void* geom;    /* device: node + triangle words */
+    size_t geom_words;
+    const void* attrs;   /* device: 48 floats per slot */
+    size_t attr_floats;
+    const void* tables;  /* device: scene tables + environment words */
+    size_t table_words;
+    const void* atlas;   /* device: RGBA16F layers */
+    uint32_t atlas_side;
+    uint32_t atlas_layers;
+} oxpt_device_scene;
+oxpt_status oxpt_dispatch_noalloc(const oxpt_device_scene* scene, const oxpt_params* params,
+                                  const oxpt_frame* frame, float* accum, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,14 @@ class SceneDesc(C.Structure):
                 ("node_count", u32), ("slot_count", u32)]
 
 
+class DeviceScene(C.Structure):
+    _fields_ = [("geom", vp), ("geom_words", sz), ("attrs", vp), ("attr_floats", sz), ("tables", vp),
+                ("table_words", sz), ("atlas", vp), ("atlas_side", u32), ("atlas_layers", u32)]
+
+
+NOALLOC_MAX_PATHS = 1 << 18
+
+
 class DevImage(C.Structure):
     _fields_ = [("data", vp), ("width", u32), ("height", u32), ("pitch_bytes", u32), ("format", u32)]
 
@@ -119,6 +127,7 @@ _SIGS = {
     "oxpt_resolve": (cint, [vp, C.POINTER(ResolveParams), cint, vp, C.POINTER(DevImage)]),
     "oxpt_read_accum": (cint, [vp, vp]),
     "oxpt_accum_view": (cint, [vp, C.POINTER(DevImage)]),
+    "oxpt_dispatch_noalloc": (cint, [C.c_void_p, C.POINTER(Params), C.POINTER(Frame), vp, vp]),
     # oxpt_diag.h
     "oxpt_diag_sobol": (cint, [vp, vp, u32, sz, vp, vp, vp, vp, vp]),
     "oxpt_diag_trace_rays": (cint, [vp, sz, vp, u32, vp, vp, vp, vp]),
