@@ -67,6 +67,8 @@ def parse():
                     help="execution plan; auto = the library default")
     ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
+                    help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
     return ap.parse_args()
 
 
@@ -245,6 +247,8 @@ def main():
         kw = {"wave_slots": a.slots} if a.slots else {}
         if a.mode != "auto":
             kw["mode"] = {"mega": 0, "wave": 1, "split": 2}[a.mode]
+        if a.shadow_walk != "auto":
+            kw["shadow_walk"] = {"four": 0, "binary": 1}[a.shadow_walk]
         pt.set_tuning(**kw)
     elif not a.no_tune:
         from oxideav_render_vulkan_b200 import tuner
@@ -316,7 +320,6 @@ def main():
     peak, peak_kind = measured_peak()
     kms, kn = (C.c_double * 8)(), (C.c_uint64 * 8)()
     L.oxpt_diag_timing_kinds(pt.ctx, kms, kn)
-    wave = pt.tuning().mode == 1
     paths_timed = paths_step * a.steps
     mode = pt.tuning().mode
     kinds = {0: ((0, "trace_paths"),), 1: ((2, "wave_logic"), (3, "wave_extend"), (4, "wave_shadow")),

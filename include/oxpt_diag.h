@@ -31,7 +31,9 @@ oxpt_status oxpt_diag_sobol(oxpt_ctx* ctx, const uint32_t* sobol_dirs, uint32_t 
  * BVH ray queries on the uploaded scene and tables (traverse,
  * pathtrace.wgsl:646-735). rays[8i..8i+7] = o.xyz, t_max, d.xyz, skip
  * (global triangle id bits, 0xffffffff = none). flags bit 0 = any-hit,
- * bit 1 = primary (back-face culling of single-sided materials).
+ * bit 1 = primary (back-face culling of single-sided materials), bit 2 =
+ * any-hit rays walk the four-wide tree (OXPT_E_INVALID when none was
+ * built; which occluder is reported may differ, occlusion may not).
  * Outputs per ray: slot (0xffffffff = miss), global id, t, barycentrics
  * (3 floats). Any output pointer may be NULL.
  */
@@ -102,6 +104,9 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *                  kernel.
  *   stack          traversal stack entries: 32 or 64; 0 = 32 when the BVH
  *                  is at most 32 levels deep, else 64 (exact either way).
+ *   shadow_walk    wavefront shadow rays: 0 = the four-wide tree built on
+ *                  upload when the scene allows it (same occlusion), 1 =
+ *                  the binary ordered walk.
  */
 enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1, OXPT_MODE_WAVEFRONT_SPLIT = 2 };
 typedef struct oxpt_tuning {
@@ -116,10 +121,22 @@ typedef struct oxpt_tuning {
     uint32_t trace_variant;
     uint32_t stack;
     uint32_t nee_variant;
-    uint32_t reserved;
+    uint32_t shadow_walk;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);
+/* The four-wide any-hit tree of the uploaded scene: out[0] 1 when built
+ * (0: the scene keeps the binary walk for every ray), out[1] its nodes,
+ * out[2] its root reference, out[3] the stack entries its walk needs. */
+oxpt_status oxpt_diag_bvh4(const oxpt_ctx* ctx, uint32_t out[4]);
+/* Host-side collapse of binary node words (node i at words 8i..8i+7) into
+ * the four-wide layout: 32 words per node, written to `out` when it has
+ * room for them (`cap` words); *words = the words needed, *root = the root
+ * reference, *stack_need as above. OXPT_E_INVALID when the tree cannot be
+ * collapsed exactly (malformed, a child box outside its parent's, a leaf of
+ * more than 16 triangles). Needs no GPU. */
+oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint32_t* out, size_t cap,
+                                 size_t* words, uint32_t* root, uint32_t* stack_need);
 /* Wavefront bounces (logic + extend + shadow launches) run so far. */
 oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* ctx, uint64_t* out);
 

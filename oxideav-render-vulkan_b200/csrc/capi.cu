@@ -20,6 +20,7 @@
 #include "../../include/oxpt_diag.h"
 #include "kernels.cuh"
 #include "wavefront.cuh"
+#include "../host/bvh4.hpp"
 
 struct oxpt_ctx {
     int device = 0;
@@ -72,6 +73,11 @@ struct oxpt_ctx {
     uint32_t check_every = 4;
     uint32_t shade_variant = 1, trace_variant = 1, nee_variant = 1, stack = 0;
     uint32_t bvh_depth = 0;
+    // four-wide any-hit tree (host/bvh4.cpp), built on upload when exact
+    float4* bvh4 = nullptr;
+    bool bvh4_built = false;
+    uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
+    uint32_t shadow_walk = 0;
     void* wave_mem = nullptr;
     size_t wave_bytes = 0;
     uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
@@ -113,6 +119,13 @@ oxpt_status realloc_dev(oxpt_ctx* c, T** p, size_t bytes, const char* what) {
     return OXPT_OK;
 }
 
+// The four-wide tree answers any-hit queries exactly when it was built from
+// the whole tree the params name and the binary walk it replaces never
+// overflows its 64-entry stack (at most 64 levels).
+bool bvh4_usable(const oxpt_ctx* c) {
+    return c->bvh4_built && c->params.env[3] == c->node_count && c->bvh_depth <= 64 && c->bvh4_need <= 64;
+}
+
 oxd::Scene scene_view(const oxpt_ctx* c) {
     oxd::Scene s;
     s.geom = c->geom;
@@ -125,6 +138,11 @@ oxd::Scene scene_view(const oxpt_ctx* c) {
     s.side = c->side;
     s.layers = c->layers;
     s.P = c->params;
+    if (bvh4_usable(c)) {
+        s.bvh4 = c->bvh4;
+        s.bvh4_root = c->bvh4_root;
+        s.bvh4_nodes = c->bvh4_nodes;
+    }
     return s;
 }
 
@@ -273,6 +291,8 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     CK(c, cudaMemsetAsync(wa.ctr, 0, 64, c->stream), "wave init");
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
+    bool four = c->shadow_walk == 0 && bvh4_usable(c);
+    int sd4 = c->bvh4_need <= 32 ? 32 : 64;
     uint64_t per_slot = total / P + 1;
     uint64_t bounces = std::min<uint64_t>(c->params.dims[3], 1u << 20);
     uint64_t cap = 4 * (bounces + 2) * per_slot + 1024;
@@ -311,7 +331,8 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
                return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, sd, c->sms, c->stream);
            }), "wave extend");
         CK(c, timed(4, [&] {
-               return oxd::launch_wave_shadow(wsh, count, (int)c->trace_variant, sd, c->sms, c->stream);
+               return oxd::launch_wave_shadow(wsh, count, four, (int)c->trace_variant, four ? sd4 : sd, c->sms,
+                                              c->stream);
            }), "wave shadow");
         c->launches += 3;
         c->wave_iterations++;
@@ -434,7 +455,7 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
         cudaEventDestroy(t.b);
     }
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
-                    c->dev_counters, c->wave_mem};
+                    c->dev_counters, c->wave_mem, c->bvh4};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->wave_host) cudaFreeHost(c->wave_host);
@@ -460,6 +481,27 @@ oxpt_status oxpt_device_summary(const oxpt_ctx* c, char* buf, size_t len) {
     if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return OXPT_E_CUDA;
     std::snprintf(buf, len, "%s (sm_%d%d, %d SMs, %zu MiB)", prop.name, prop.major, prop.minor,
                   prop.multiProcessorCount, (size_t)(prop.totalGlobalMem >> 20));
+    return OXPT_OK;
+}
+
+// Collapse the uploaded binary tree into the four-wide any-hit tree; a
+// tree that does not collapse exactly keeps the binary walk.
+static oxpt_status upload_bvh4(oxpt_ctx* c, const oxpt_scene_desc* d) {
+    c->bvh4_built = false;
+    std::vector<uint32_t> words;
+    uint32_t root = 0xffffffffu;
+    if (!oxpt::build_bvh4(d->geom, d->node_count, &words, &root)) return realloc_dev(c, &c->bvh4, 0, "bvh4");
+    oxpt_status s = realloc_dev(c, &c->bvh4, words.size() * 4, "four-wide tree");
+    if (s) return s;
+    if (!words.empty()) {
+        CK(c, cudaMemcpyAsync(c->bvh4, words.data(), words.size() * 4, cudaMemcpyHostToDevice, c->stream),
+           "four-wide tree upload");
+        CK(c, cudaStreamSynchronize(c->stream), "four-wide tree upload");
+    }
+    c->bvh4_nodes = (uint32_t)(words.size() / oxpt::BVH4_NODE_WORDS);
+    c->bvh4_root = root;
+    c->bvh4_need = oxpt::bvh4_stack_need(words, root);
+    c->bvh4_built = true;
     return OXPT_OK;
 }
 
@@ -491,6 +533,7 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     c->node_count = d->node_count;
     c->bvh_depth = bvh_depth_of(d->geom, d->node_count);
     if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
+    if ((s = upload_bvh4(c, d))) return s;
     c->has_scene = true;
     return OXPT_OK;
 }
@@ -658,6 +701,7 @@ oxpt_status oxpt_diag_trace_rays(oxpt_ctx* c, size_t n, const float* rays, uint3
                                  uint32_t* gid, float* t, float* bary) {
     if (!c || (n && !rays)) return fail(c, OXPT_E_INVALID, "null argument");
     if (!c->has_scene || !c->has_tables || !c->has_params) return fail(c, OXPT_E_INVALID, "scene, tables and params must be set first");
+    if ((flags & 4u) && !bvh4_usable(c)) return fail(c, OXPT_E_INVALID, "no four-wide tree for this scene");
     if (n == 0) return OXPT_OK;
     oxpt_status s = set_device(c);
     if (s) return s;
@@ -760,6 +804,8 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
         return fail(c, OXPT_E_INVALID, "variants are 0, 1 or 2");
     if (t->stack && t->stack != 32 && t->stack != 64) return fail(c, OXPT_E_INVALID, "stack is 0, 32 or 64");
     if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
+    if (t->shadow_walk > 1) return fail(c, OXPT_E_INVALID, "shadow_walk is 0 or 1");
+    c->shadow_walk = t->shadow_walk;
     c->shade_variant = t->shade_variant;
     c->trace_variant = t->trace_variant;
     c->nee_variant = t->nee_variant;
@@ -781,6 +827,29 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->trace_variant = c->trace_variant;
     t->nee_variant = c->nee_variant;
     t->stack = c->stack;
+    t->shadow_walk = c->shadow_walk;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_bvh4(const oxpt_ctx* c, uint32_t out[4]) {
+    if (!c || !out) return OXPT_E_INVALID;
+    out[0] = bvh4_usable(c) ? 1u : 0u;
+    out[1] = c->bvh4_nodes;
+    out[2] = c->bvh4_root;
+    out[3] = c->bvh4_need;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint32_t* out, size_t cap, size_t* words,
+                                 uint32_t* root, uint32_t* stack_need) {
+    if ((node_count && !geom) || !words || !root || !stack_need) return OXPT_E_INVALID;
+    std::vector<uint32_t> w;
+    uint32_t r = 0xffffffffu;
+    if (!oxpt::build_bvh4(geom, node_count, &w, &r)) return OXPT_E_INVALID;
+    *words = w.size();
+    *root = r;
+    *stack_need = oxpt::bvh4_stack_need(w, r);
+    if (out && cap >= w.size()) std::memcpy(out, w.data(), w.size() * 4);
     return OXPT_OK;
 }
 

@@ -108,6 +108,9 @@ struct Scene {
     const uint2* atlas;  // RGBA16F texels
     uint32_t side, layers;
     oxpt_params P;
+    // Four-wide tree for any-hit queries (8 float4 per node), or null.
+    const float4* bvh4 = nullptr;
+    uint32_t bvh4_root = 0xffffffffu, bvh4_nodes = 0u;
 };
 
 __device__ __forceinline__ uint32_t tw(const Scene& s, uint32_t i) {
@@ -372,15 +375,20 @@ __device__ __forceinline__ Ray make_ray(f3 o, f3 d) {
     return r;
 }
 // Robust slab test (Williams et al. 2005, Ize 2013 far scaling).
-__device__ __forceinline__ float slab(const Ray& r, float4 lo, float4 hi, float t_max) {
-    float t0x = (lo.x - r.o.x) * r.inv.x, t1x = (hi.x - r.o.x) * r.inv.x;
-    float t0y = (lo.y - r.o.y) * r.inv.y, t1y = (hi.y - r.o.y) * r.inv.y;
-    float t0z = (lo.z - r.o.z) * r.inv.z, t1z = (hi.z - r.o.z) * r.inv.z;
+// Returns the entry distance, or -1 when the box is missed.
+__device__ __forceinline__ float slab6(const Ray& r, float lox, float loy, float loz, float hix, float hiy, float hiz,
+                                       float t_max) {
+    float t0x = (lox - r.o.x) * r.inv.x, t1x = (hix - r.o.x) * r.inv.x;
+    float t0y = (loy - r.o.y) * r.inv.y, t1y = (hiy - r.o.y) * r.inv.y;
+    float t0z = (loz - r.o.z) * r.inv.z, t1z = (hiz - r.o.z) * r.inv.z;
     float tnx = fminf(t0x, t1x), tny = fminf(t0y, t1y), tnz = fminf(t0z, t1z);
     float tfx = fmaxf(t0x, t1x), tfy = fmaxf(t0y, t1y), tfz = fmaxf(t0z, t1z);
     float t0 = fmaxf(fmaxf(0.0f, tnx), fmaxf(tny, tnz));
     float t1 = fminf(t_max, fminf(tfx, fminf(tfy, tfz)) * 1.0000004f);
     return t0 <= t1 ? t0 : -1.0f;
+}
+__device__ __forceinline__ float slab(const Ray& r, float4 lo, float4 hi, float t_max) {
+    return slab6(r, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, t_max);
 }
 
 struct Hit {

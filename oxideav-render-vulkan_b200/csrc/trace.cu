@@ -142,9 +142,13 @@ __global__ void __launch_bounds__(128) trace_rays(const __grid_constant__ RayArg
         Sampler smp{0u, 0u, 0u};
         Hit h;
         uint32_t m = 0;
-        bool got = traverse<COUNT>(a.s, make_ray(mk(r[0], r[1], r[2]), mk(r[4], r[5], r[6])), r[3], smp, 0u,
-                                   (a.flags & 2u) != 0u, (a.flags & 1u) != 0u, __float_as_uint(r[7]), &h, &m, cnt,
-                                   a.err);
+        Ray ray = make_ray(mk(r[0], r[1], r[2]), mk(r[4], r[5], r[6]));
+        bool primary = (a.flags & 2u) != 0u;
+        bool got = (a.flags & 5u) == 5u
+                       ? occluded4<COUNT, STACK>(a.s, ray, r[3], smp, 0u, primary, __float_as_uint(r[7]), &h, &m, cnt,
+                                                 a.err)
+                       : traverse<COUNT>(a.s, ray, r[3], smp, 0u, primary, (a.flags & 1u) != 0u,
+                                         __float_as_uint(r[7]), &h, &m, cnt, a.err);
         if (a.slot) a.slot[i] = got ? h.slot : NONE;
         if (a.gid) a.gid[i] = got ? tri_word(a.s, h.slot, 0u) : NONE;
         if (a.t) a.t[i] = got ? h.t : 0.0f;

@@ -135,4 +135,97 @@ __device__ bool traverse(const Scene& s, const Ray& r, float t_max, const Sample
     return hit_any;
 }
 
+// Any-hit query over the four-wide tree built on upload (host/bvh4.cpp):
+// 128-byte nodes holding four child boxes as x/y/z planes and four child
+// references, one node per cache line. Whether a ray is occluded does not
+// depend on the order its candidate triangles are tested in (acceptance is
+// a function of the ray and the triangle alone), and with every child box
+// inside its parent's the slab test passes a leaf's box only if it passes
+// all its ancestors', so this walk tests exactly the leaves the binary walk
+// reaches and returns the same answer with half the dependent fetches.
+// The nearest passing child is taken next and the others pushed without
+// their distances (order only changes how early an occluder is found). SD
+// is at least the tree's stack need, checked on upload; *hit is the
+// accepted triangle.
+template <bool COUNT, int SD>
+__device__ bool occluded4(const Scene& s, const Ray& r, float t_max, const Sampler& smp, uint32_t ray_id,
+                          bool primary, uint32_t skip, Hit* hit, uint32_t* hit_mat, Cnt& cnt, uint32_t* err) {
+    hit->slot = NONE;
+    if (!r.valid || s.bvh4_root == NONE) return false;
+    uint32_t stack[SD];
+    uint32_t sp = 0u, cur = s.bvh4_root;
+    uint32_t guard = 4u * s.bvh4_nodes + 8u;
+    for (;;) {
+        if (guard-- == 0u) {
+            atomicOr(err, 1u);
+            return false;
+        }
+        if (cur & 0x80000000u) {
+            bump<COUNT>(cnt, C_LEAVES);
+            uint32_t first = cur & 0x07ffffffu, end = first + ((cur >> 27) & 15u) + 1u;
+            if ((uint64_t)end > s.slot_count) {
+                atomicOr(err, 2u);
+                return false;
+            }
+            for (uint32_t slot = first; slot < end; slot++) {
+                bump<COUNT>(cnt, C_TRIS);
+                uint64_t tb = tri_base(s, slot);
+                float4 q0 = geomv(s, tb), q1 = geomv(s, tb + 1), q2 = geomv(s, tb + 2);
+                Hit h;
+                if (!intersect(r, q0, q1, q2, t_max, &h)) continue;
+                uint32_t gid = __float_as_uint(q0.w);
+                if (gid == skip) continue;
+                uint32_t m = __float_as_uint(q2.w);
+                if (!accept(s, slot, m, gid, h, smp, ray_id, primary)) continue;
+                h.slot = slot;
+                *hit = h;
+                *hit_mat = m;
+                return true;
+            }
+        } else {
+            if (cur >= s.bvh4_nodes) {
+                atomicOr(err, 1u);
+                return false;
+            }
+            bump<COUNT>(cnt, C_BOXES, 4);
+            const float4* nd = s.bvh4 + (uint64_t)cur * 8u;
+            float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+            float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+            uint4 rf = __ldg(reinterpret_cast<const uint4*>(nd) + 6);
+            uint32_t ref[4] = {rf.x, rf.y, rf.z, rf.w};
+            float t[4];
+            t[0] = rf.x == NONE ? -1.0f : slab6(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, t_max);
+            t[1] = rf.y == NONE ? -1.0f : slab6(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, t_max);
+            t[2] = rf.z == NONE ? -1.0f : slab6(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, t_max);
+            t[3] = rf.w == NONE ? -1.0f : slab6(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, t_max);
+            int best = -1;
+            float bt = 0.0f;
+            uint32_t bref = NONE;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (t[k] >= 0.0f && (best < 0 || t[k] < bt)) {
+                    best = k;
+                    bt = t[k];
+                    bref = ref[k];
+                }
+            if (best >= 0) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (k == best || !(t[k] >= 0.0f)) continue;
+                    if (sp >= (uint32_t)SD) {  // excluded on upload
+                        atomicOr(err, 4u);
+                        return false;
+                    }
+                    stack[sp++] = ref[k];
+                }
+                cur = bref;
+                continue;
+            }
+        }
+        if (sp == 0u) return false;
+        bump<COUNT>(cnt, C_POPS);
+        cur = stack[--sp];
+    }
+}
+
 }  // namespace oxd

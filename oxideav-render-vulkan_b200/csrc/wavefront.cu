@@ -220,7 +220,8 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const
             if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
 }
 
-template <bool COUNT, int MINB, int SD>
+// FOUR: walk the four-wide tree (same occlusion as the binary walk).
+template <bool COUNT, int MINB, int SD, bool FOUR>
 __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
@@ -233,8 +234,10 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
         Hit h;
         uint32_t mat = 0u;
         bump<COUNT>(cnt, C_SHADOW_RAYS);
-        bool got = traverse<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, true, __float_as_uint(d.w),
-                                   &h, &mat, cnt, a.err);
+        bool got = FOUR ? occluded4<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, __float_as_uint(d.w),
+                                               &h, &mat, cnt, a.err)
+                        : traverse<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, true,
+                                              __float_as_uint(d.w), &h, &mat, cnt, a.err);
         if (!got) a.st.pend[(uint64_t)m.x * a.jobs + m.y].w = 2.0f;
     }
     if (COUNT)
@@ -255,25 +258,29 @@ static cudaError_t logic_v(const WaveArgs& a, int v, unsigned blocks, cudaStream
     return cudaGetLastError();
 }
 
-template <bool C, bool EXT, int SD>
-static void* trav_fn(int v) {
-    if (EXT) {
-        if (v == 0) return (void*)wave_extend<C, 6, SD>;
-        if (v == 1) return (void*)wave_extend<C, 8, SD>;
-        return (void*)wave_extend<C, 10, SD>;
-    }
-    if (v == 0) return (void*)wave_shadow<C, 6, SD>;
-    if (v == 1) return (void*)wave_shadow<C, 8, SD>;
-    return (void*)wave_shadow<C, 10, SD>;
+template <bool C, int SD>
+static void* ext_fn(int v) {
+    if (v == 0) return (void*)wave_extend<C, 6, SD>;
+    if (v == 1) return (void*)wave_extend<C, 8, SD>;
+    return (void*)wave_extend<C, 10, SD>;
 }
 
-static void* trav_kernel(bool count, bool ext, int v, int sd) {
-    if (count) {
-        if (ext) return sd <= 32 ? trav_fn<true, true, 32>(v) : trav_fn<true, true, 64>(v);
-        return sd <= 32 ? trav_fn<true, false, 32>(v) : trav_fn<true, false, 64>(v);
-    }
-    if (ext) return sd <= 32 ? trav_fn<false, true, 32>(v) : trav_fn<false, true, 64>(v);
-    return sd <= 32 ? trav_fn<false, false, 32>(v) : trav_fn<false, false, 64>(v);
+template <bool C, int SD, bool FOUR>
+static void* shadow_fn(int v) {
+    if (v == 0) return (void*)wave_shadow<C, 6, SD, FOUR>;
+    if (v == 1) return (void*)wave_shadow<C, 8, SD, FOUR>;
+    return (void*)wave_shadow<C, 10, SD, FOUR>;
+}
+
+template <bool C>
+static void* trav_kernel_c(bool ext, bool four, int v, int sd) {
+    if (ext) return sd <= 32 ? ext_fn<C, 32>(v) : ext_fn<C, 64>(v);
+    if (four) return sd <= 32 ? shadow_fn<C, 32, true>(v) : shadow_fn<C, 64, true>(v);
+    return sd <= 32 ? shadow_fn<C, 32, false>(v) : shadow_fn<C, 64, false>(v);
+}
+
+static void* trav_kernel(bool count, bool ext, bool four, int v, int sd) {
+    return count ? trav_kernel_c<true>(ext, four, v, sd) : trav_kernel_c<false>(ext, four, v, sd);
 }
 
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st) {
@@ -282,10 +289,10 @@ cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaSt
     return count ? logic_v<true>(a, variant, blocks, st) : logic_v<false>(a, variant, blocks, st);
 }
 
-static cudaError_t launch_trav(const WaveArgs& a, bool count, bool ext, int variant, int sd, int sms,
+static cudaError_t launch_trav(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
                                cudaStream_t st) {
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
-    void* fn = trav_kernel(count, ext, variant, sd);
+    void* fn = trav_kernel(count, ext, four, variant, sd);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, WAVE_TRAVERSE_THREADS, 0);
     unsigned blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
@@ -295,11 +302,12 @@ static cudaError_t launch_trav(const WaveArgs& a, bool count, bool ext, int vari
 }
 
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
-    return launch_trav(a, count, true, variant, stack, sms, st);
+    return launch_trav(a, count, true, false, variant, stack, sms, st);
 }
 
-cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
-    return launch_trav(a, count, false, variant, stack, sms, st);
+cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, bool four, int variant, int stack, int sms,
+                               cudaStream_t st) {
+    return launch_trav(a, count, false, four, variant, stack, sms, st);
 }
 
 }  // namespace oxd

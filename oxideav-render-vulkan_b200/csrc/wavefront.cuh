@@ -57,7 +57,10 @@ struct WaveArgs {
 // / 4 blocks per SM; traversal 6 / 8 / 10); `stack`: 32 or 64 entries.
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st);
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
-cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
+// four: any-hit walk over the four-wide tree (Scene::bvh4) instead of the
+// binary one; stack: 32 or 64 entries, enough for the tree walked.
+cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, bool four, int variant, int stack, int sms,
+                               cudaStream_t st);
 // Split wavefront (wave_split.cu); shade variants 2 / 3 / 4 blocks per SM,
 // NEE variants 4 / 5 / 6.
 cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st);

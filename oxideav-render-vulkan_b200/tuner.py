@@ -3,7 +3,8 @@
 Chooses, per scene and resolution, between the megakernel and the
 wavefront, and within the wavefront the shading kernel's register budget
 (shade_variant), the traversal kernels' occupancy target (trace_variant),
-the traversal stack depth and the number of paths in flight (wave_slots).
+the traversal stack depth, the number of paths in flight (wave_slots) and
+the shadow rays' tree (the four-wide any-hit tree or the binary walk).
 Every plan yields bit-identical accumulators, so the tuner only measures
 time: each candidate runs a short refine at sample indices far from any
 real render's, timed with CUDA events on the tracer's stream, and the
@@ -32,9 +33,11 @@ class Plan:
     stack: int = 0
     wave_slots: int = 1 << 20
     nee_variant: int = 0
+    shadow_walk: int = 0
 
     def key(self):
-        return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant)
+        return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant,
+                self.shadow_walk)
 
 
 SPACE = {
@@ -44,8 +47,9 @@ SPACE = {
     "stack": [0, 64],
     "wave_slots": [1 << 19, 1 << 20, 1 << 21],
     "nee_variant": [0, 1, 2],
+    "shadow_walk": [0, 1],
 }
-WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant")
+WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk")
 SPLIT_ONLY = ("nee_variant",)
 
 
@@ -81,7 +85,8 @@ def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] =
 
 def apply(tracer, plan: Plan):
     tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
-                      stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant)
+                      stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant,
+                      shadow_walk=plan.shadow_walk)
 
 
 def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:

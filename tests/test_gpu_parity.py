@@ -95,7 +95,7 @@ def _random_rays(rng, n, lo, hi):
     return rays
 
 
-@pytest.mark.parametrize("which", ["icosphere", "boxes", "cornell"])
+@pytest.mark.parametrize("which", ["icosphere", "boxes", "cornell", "alpha"])
 def test_closest_hit_ids_on_a_million_rays(pkg, oracle, which):
     if which == "icosphere":
         scene = pkg.Scene.icosphere(freq=64, seed=3, n_textures=0, n_punctual=0, n_emissive=16)
@@ -103,6 +103,9 @@ def test_closest_hit_ids_on_a_million_rays(pkg, oracle, which):
     elif which == "boxes":
         scene = pkg.Scene.box_field(2000, seed=4, material_mix=0)
         lo, hi = -8.0, 8.0
+    elif which == "alpha":
+        scene = scenes.alpha_scene(pkg)
+        lo, hi = -1.5, 1.5
     else:
         scene = pkg.Scene.cornell()
         lo, hi = 0.01, 0.99
@@ -112,8 +115,12 @@ def test_closest_hit_ids_on_a_million_rays(pkg, oracle, which):
     rng = np.random.default_rng(11)
     n = 1_000_000
     rays = _random_rays(rng, n, lo, hi)
+    rays[: n // 4, 3] = rng.uniform(0.0, 2.0 * (hi - lo), n // 4).astype(np.float32)  # finite t_max
     L = pkg._native.lib()
-    for flags in (0, 1, 2):
+    info = (C.c_uint32 * 4)()
+    assert L.oxpt_diag_bvh4(t.ctx, info) == 0 and info[0] == 1
+    # bit 2: any-hit rays walk the four-wide tree; occlusion must not change
+    for flags in (0, 1, 2, 3, 5, 7):
         slot = np.empty(n, np.uint32)
         gid = np.empty(n, np.uint32)
         tt = np.empty(n, np.float32)
@@ -121,7 +128,7 @@ def test_closest_hit_ids_on_a_million_rays(pkg, oracle, which):
         st = L.oxpt_diag_trace_rays(t.ctx, n, rays.ctypes.data, flags, slot.ctypes.data, gid.ctypes.data,
                                     tt.ctypes.data, bary.ctypes.data)
         assert st == 0
-        oslot, ogid, ot, obary, _ = oracle.trace_rays(p, rays, flags)
+        oslot, ogid, ot, obary, _ = oracle.trace_rays(p, rays, flags & 3)
         if flags & 1:
             assert np.array_equal(slot == 0xFFFFFFFF, oslot == 0xFFFFFFFF)
             continue
@@ -223,7 +230,7 @@ def test_both_execution_modes_bit_exact(pkg, oracle, mode, which):
 def test_traversal_counters_match_oracle(pkg, oracle, mode):
     opts = _opts(pkg, 48, 32, 4)
     t = _tracer(pkg, scenes.materials_scene(pkg), opts)
-    t.set_tuning(mode=mode)
+    t.set_tuning(mode=mode, shadow_walk=1)  # the reference's binary walk for every ray
     p = t.prepared()  # binds tables and params on the context
     out = (C.c_uint64 * 8)()
     st = pkg._native.lib().oxpt_diag_refine_counted(t.ctx, 0, 4, out)
@@ -231,6 +238,36 @@ def test_traversal_counters_match_oracle(pkg, oracle, mode):
     cpu, cnt = oracle.render(p, 4)
     assert list(out) == [int(c) for c in cnt]
     assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("which", ["materials", "alpha"])
+def test_four_wide_shadow_walk_matches_the_binary_walk(pkg, oracle, mode, which):
+    """Shadow rays through the four-wide tree: the accumulator is the
+    oracle's bit for bit, the continuation rays' counters are the binary
+    run's, and as many shadow rays are traced."""
+    scene = scenes.materials_scene(pkg) if which == "materials" else scenes.alpha_scene(pkg)
+    opts = _opts(pkg, 48, 32, 4)
+    L = pkg._native.lib()
+    runs = []
+    for walk in (1, 0):
+        t = _tracer(pkg, scene, opts)
+        t.set_tuning(mode=mode, shadow_walk=walk)
+        p = t.prepared()
+        out = (C.c_uint64 * 8)()
+        assert L.oxpt_diag_refine_counted(t.ctx, 0, 4, out) == 0
+        split = (C.c_uint64 * 16)()
+        assert L.oxpt_diag_counters_split(t.ctx, split) == 0
+        runs.append((list(out), list(split), t.read_accum()))
+    info = (C.c_uint32 * 4)()
+    assert L.oxpt_diag_bvh4(t.ctx, info) == 0 and info[0] == 1 and 1 <= info[3] <= 64
+    (tot_b, split_b, acc_b), (tot_f, split_f, acc_f) = runs
+    cpu, cnt = oracle.render(p, 4)
+    assert tot_b == [int(c) for c in cnt]
+    assert np.array_equal(acc_f.view(np.uint32), cpu.view(np.uint32))
+    assert np.array_equal(acc_b.view(np.uint32), cpu.view(np.uint32))
+    assert split_f[:8] == split_b[:8]
+    assert split_f[8 + 2] == split_b[8 + 2] > 0  # shadow rays
 
 
 def test_full_size_scene_rows_bit_exact(pkg, oracle):
