@@ -220,6 +220,14 @@ oxpt_status oxpt_tracer_refine(oxpt_tracer* t, uint32_t samples);
  * frame split by row tiles across GPUs (sample indices and the samples()
  * count advance exactly as for refine). */
 oxpt_status oxpt_tracer_refine_rows(oxpt_tracer* t, uint32_t samples, uint32_t y0, uint32_t rows);
+/* refine() of several tracers at once: tracer k gets samples[k] more
+ * samples over all its rows, traced as one wavefront by `exec`
+ * (oxpt_refine_batch; NULL = the first tracer's context). Each tracer's
+ * accumulation ends bit-identical to its own refine(samples[k]). On error
+ * no tracer's sample count advances; the message is the executor's
+ * oxpt_last_error. */
+oxpt_status oxpt_tracers_refine_batch(oxpt_tracer* const* tracers, uint32_t count, const uint32_t* samples,
+                                      oxpt_ctx* exec);
 oxpt_status oxpt_tracer_finish(oxpt_tracer* t);
 /* w*h*4 bytes (RGBA8, sRGB-encoded). */
 oxpt_status oxpt_tracer_image(oxpt_tracer* t, uint8_t* out);

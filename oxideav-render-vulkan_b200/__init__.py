@@ -7,6 +7,6 @@ The package directory name contains hyphens, so it is loaded by path (see
 from .pathtracer import (  # noqa: F401
     PATHTRACE_BACKEND_NAME, BackendError, DeviceImage, EnvironmentMap, Error, GpuMode, GpuPathTracer,
     GpuRenderer, InvalidOptionsError, LightStrategy, PathTraceOptions, Prepared, RenderOptions,
-    RenderRegistry, Scene, ToneMap, material, prepare, register_into,
+    RenderRegistry, Scene, ToneMap, material, prepare, refine_batch, register_into,
 )
 from . import _native  # noqa: F401

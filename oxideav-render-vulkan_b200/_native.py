@@ -1,4 +1,4 @@
-"""ctypes bindings of liboxpt.so (include/oxpt.h, oxpt_host.h, oxpt_diag.h).
+"""ctypes bindings of liboxpt.so (include/oxpt.h, oxpt_batch.h, oxpt_host.h, oxpt_diag.h).
 
 The library is built in-tree by ``build.py``. Loading fails loudly when it
 is missing: there is no CPU fallback on this path.
@@ -44,6 +44,10 @@ class DeviceScene(C.Structure):
 
 
 NOALLOC_MAX_PATHS = 1 << 18
+
+
+class BatchFrame(C.Structure):
+    _fields_ = [("ctx", vp), ("first", u32), ("count", u32), ("y0", u32), ("rows", u32)]
 
 
 class DevImage(C.Structure):
@@ -128,6 +132,9 @@ _SIGS = {
     "oxpt_read_accum": (cint, [vp, vp]),
     "oxpt_accum_view": (cint, [vp, C.POINTER(DevImage)]),
     "oxpt_dispatch_noalloc": (cint, [C.c_void_p, C.POINTER(Params), C.POINTER(Frame), vp, vp]),
+    # oxpt_batch.h
+    "oxpt_refine_batch": (cint, [vp, C.POINTER(BatchFrame), u32]),
+    "oxpt_diag_batch_plan": (cint, [vp, u32, u64, vp, sz, C.POINTER(sz)]),
     # oxpt_diag.h
     "oxpt_diag_sobol": (cint, [vp, vp, u32, sz, vp, vp, vp, vp, vp]),
     "oxpt_diag_trace_rays": (cint, [vp, sz, vp, u32, vp, vp, vp, vp]),
@@ -179,6 +186,7 @@ _SIGS = {
     "oxpt_tracer_sync": (cint, [vp, vp, C.POINTER(RenderOptions), C.POINTER(cint)]),
     "oxpt_tracer_refine": (cint, [vp, u32]),
     "oxpt_tracer_refine_rows": (cint, [vp, u32, u32, u32]),
+    "oxpt_tracers_refine_batch": (cint, [C.POINTER(vp), u32, C.POINTER(u32), vp]),
     "oxpt_tracer_finish": (cint, [vp]),
     "oxpt_tracer_image": (cint, [vp, vp]),
     "oxpt_tracer_hdr": (cint, [vp, vp]),

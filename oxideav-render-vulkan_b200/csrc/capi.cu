@@ -17,9 +17,11 @@
 #include <vector>
 
 #include "../../include/oxpt.h"
+#include "../../include/oxpt_batch.h"
 #include "../../include/oxpt_diag.h"
 #include "kernels.cuh"
 #include "wavefront.cuh"
+#include "../host/batch.hpp"
 #include "../host/bvh4.hpp"
 
 struct oxpt_ctx {
@@ -83,6 +85,10 @@ struct oxpt_ctx {
     uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
     uint32_t* wave_host = nullptr;  // pinned: [0..2] counters snapshot
     uint64_t wave_iterations = 0;
+    // batched refinement as an executor: frame records of every round
+    oxd::BatchFrame* batch_dev = nullptr;
+    size_t batch_cap = 0;
+    cudaEvent_t batch_done = nullptr;
 };
 
 namespace {
@@ -142,6 +148,7 @@ oxd::Scene scene_view(const oxpt_ctx* c) {
         s.bvh4 = c->bvh4;
         s.bvh4_root = c->bvh4_root;
         s.bvh4_nodes = c->bvh4_nodes;
+        s.bvh4_ok = 1u;
     }
     return s;
 }
@@ -211,8 +218,8 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     bool split = c->mode == OXPT_MODE_WAVEFRONT_SPLIT;
     size_t sizes[] = {P * 8, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 4, P * 4,
                       PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64,
-                      split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0};
-    constexpr int NB = 20;
+                      split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0, P * 4};
+    constexpr int NB = 21;
     size_t total = 0;
     for (size_t s : sizes) total += align256(s);
     if (slots > c->wave_cap_slots || jobs > c->wave_cap_jobs || total > c->wave_bytes) {
@@ -250,6 +257,7 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     st->hmeta = (uint32_t*)ptr[9];
     st->nee_n = (uint32_t*)ptr[10];
     st->pend = (float4*)ptr[11];
+    st->frame = (uint32_t*)ptr[20];
     q->ext = (uint32_t*)ptr[12];
     q->sh_o = (float4*)ptr[13];
     q->sh_d = (float4*)ptr[14];
@@ -268,6 +276,9 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
 
 // One sub-frame through the wavefront: iterate logic / extend / shadow
 // until every slot is empty, then reduce in sample order.
+oxpt_status wave_loop(oxpt_ctx* c, const oxd::WaveArgs& wa, bool count, bool four, int sd, int sd4,
+                      uint32_t max_bounces);
+
 oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     uint32_t J = c->params.cfg[2] + 1u;
     uint64_t total = ta.total;
@@ -286,15 +297,26 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     wa.out = ta.out;
     wa.counters = ta.counters;
     wa.err = ta.err;
-    CK(c, cudaMemsetAsync(wa.st.rad, 0, (size_t)P * 16, c->stream), "wave init");
-    CK(c, cudaMemsetAsync(wa.st.nee_n, 0, (size_t)P * 4, c->stream), "wave init");
-    CK(c, cudaMemsetAsync(wa.ctr, 0, 64, c->stream), "wave init");
+    wa.frames = nullptr;
+    wa.nframes = 0;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
     bool four = c->shadow_walk == 0 && bvh4_usable(c);
     int sd4 = c->bvh4_need <= 32 ? 32 : 64;
-    uint64_t per_slot = total / P + 1;
-    uint64_t bounces = std::min<uint64_t>(c->params.dims[3], 1u << 20);
+    return wave_loop(c, wa, count, four, sd, sd4, c->params.dims[3]);
+}
+
+// Iterates the wavefront's kernels over `wa` until every slot is empty.
+// The bound on iterations (four times the bounces of every path a slot can
+// take, plus slack) turns a wavefront that does not drain into an error.
+oxpt_status wave_loop(oxpt_ctx* c, const oxd::WaveArgs& wa, bool count, bool four, int sd, int sd4,
+                      uint32_t max_bounces) {
+    const uint32_t P = wa.slots;
+    CK(c, cudaMemsetAsync(wa.st.rad, 0, (size_t)P * 16, c->stream), "wave init");
+    CK(c, cudaMemsetAsync(wa.st.nee_n, 0, (size_t)P * 4, c->stream), "wave init");
+    CK(c, cudaMemsetAsync(wa.ctr, 0, 64, c->stream), "wave init");
+    uint64_t per_slot = wa.total / P + 1;
+    uint64_t bounces = std::min<uint64_t>(max_bounces, 1u << 20);
     uint64_t cap = 4 * (bounces + 2) * per_slot + 1024;
     oxd::WaveArgs wsh = wa;  // shadow rays count into the second counter half
     if (wsh.counters) wsh.counters += oxd::C_N;
@@ -455,7 +477,8 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
         cudaEventDestroy(t.b);
     }
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
-                    c->dev_counters, c->wave_mem, c->bvh4};
+                    c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev};
+    if (c->batch_done) cudaEventDestroy(c->batch_done);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->wave_host) cudaFreeHost(c->wave_host);
@@ -904,6 +927,157 @@ oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* c, double ms[8], uint64_t n[8
 oxpt_status oxpt_diag_launch_count(const oxpt_ctx* c, uint64_t* out) {
     if (!c || !out) return OXPT_E_INVALID;
     *out = c->launches;
+    return OXPT_OK;
+}
+
+// ---------------------------------------------------------------------
+// Batched refinement (oxpt_batch.h).
+// ---------------------------------------------------------------------
+
+oxpt_status oxpt_diag_batch_plan(const uint32_t* frames, uint32_t count, uint64_t cap, uint64_t* out,
+                                 size_t capacity, size_t* pieces) {
+    if ((count && !frames) || !pieces || cap == 0) return OXPT_E_INVALID;
+    std::vector<oxpt::BatchInput> in(count);
+    for (uint32_t k = 0; k < count; k++) {
+        const uint32_t* f = frames + 5 * (size_t)k;
+        if (f[0] > cap) return OXPT_E_INVALID;
+        in[k] = {f[0], f[1], f[2], f[3], f[4]};
+    }
+    auto rounds = oxpt::plan_batch(in, cap);
+    size_t n = 0;
+    for (size_t r = 0; r < rounds.size(); r++)
+        for (const oxpt::BatchPiece& pc : rounds[r]) {
+            if (out && n < capacity) {
+                uint64_t* o = out + 7 * n;
+                o[0] = r;
+                o[1] = pc.frame;
+                o[2] = pc.first;
+                o[3] = pc.count;
+                o[4] = pc.y0;
+                o[5] = pc.rows;
+                o[6] = pc.base;
+            }
+            n++;
+        }
+    *pieces = n;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t n) {
+    if (!e || (n && !fr)) return fail(e, OXPT_E_INVALID, "null argument");
+    oxpt_status s = set_device(e);
+    if (s) return s;
+    // Validate every frame; the fixed tables must match the first frame's.
+    std::vector<uint32_t> ref_tables, tab(640);
+    std::vector<oxpt::BatchInput> in(n);
+    for (uint32_t k = 0; k < n; k++) {
+        oxpt_ctx* c = fr[k].ctx;
+        std::string at = "batch frame " + std::to_string(k) + ": ";
+        if (!c) return fail(e, OXPT_E_INVALID, at + "null context");
+        in[k] = {c->w, fr[k].first, fr[k].count, fr[k].y0, fr[k].rows};
+        if (fr[k].count == 0 || fr[k].rows == 0) continue;
+        if (c->device != e->device) return fail(e, OXPT_E_INVALID, at + "context on another device");
+        if ((s = ready(c))) return fail(e, s, at + c->err);
+        if (fr[k].y0 >= c->h || fr[k].rows > c->h - fr[k].y0) return fail(e, OXPT_E_INVALID, at + "rows outside the image");
+        uint64_t o0 = c->params.offs0[0], o1 = c->params.offs0[1];
+        if (o0 + 128 > c->table_words || o1 + 512 > c->table_words)
+            return fail(e, OXPT_E_INVALID, at + "tables too short for the Sobol' and sheen words");
+        if (c->stream != e->stream) CK(e, cudaStreamSynchronize(c->stream), "frame context sync");
+        CK(e, cudaMemcpy(tab.data(), c->tables + o0, 128 * 4, cudaMemcpyDeviceToHost), "table check");
+        CK(e, cudaMemcpy(tab.data() + 128, c->tables + o1, 512 * 4, cudaMemcpyDeviceToHost), "table check");
+        if (ref_tables.empty()) ref_tables = tab;
+        else if (tab != ref_tables) return fail(e, OXPT_E_INVALID, at + "Sobol' or sheen table differs from the first frame's");
+    }
+    uint64_t cap = e->wave_items;
+    for (uint32_t k = 0; k < n; k++)
+        if (fr[k].count && fr[k].rows) cap = std::max<uint64_t>(cap, fr[k].ctx->w);
+    auto rounds = oxpt::plan_batch(in, cap);
+    if (rounds.empty()) return OXPT_OK;
+    // Frame records of every round, uploaded at once.
+    std::vector<oxd::BatchFrame> recs;
+    uint32_t J = 1, max_bounces = 0;
+    int sd = e->stack == 64 ? 64 : 32;
+    for (auto& r : rounds)
+        for (const oxpt::BatchPiece& pc : r) {
+            oxpt_ctx* c = fr[pc.frame].ctx;
+            oxd::BatchFrame b{};
+            b.s = scene_view(c);
+            b.npix = c->w * pc.rows;
+            b.base = pc.base;
+            b.total = (uint64_t)b.npix * pc.count;
+            b.first = pc.first;
+            b.y0 = pc.y0;
+            recs.push_back(b);
+            J = std::max(J, c->params.cfg[2] + 1u);
+            max_bounces = std::max(max_bounces, c->params.dims[3]);
+            if (c->bvh_depth > 32) sd = 64;
+            if (e->shadow_walk == 0 && bvh4_usable(c) && c->bvh4_need > 32) sd = 64;
+        }
+    if (recs.size() > e->batch_cap) {
+        if ((s = realloc_dev(e, &e->batch_dev, recs.size() * sizeof(oxd::BatchFrame), "batch frame records"))) {
+            e->batch_cap = 0;
+            return s;
+        }
+        e->batch_cap = recs.size();
+    }
+    CK(e, cudaMemcpyAsync(e->batch_dev, recs.data(), recs.size() * sizeof(oxd::BatchFrame), cudaMemcpyHostToDevice,
+                          e->stream), "batch frame records");
+    CK(e, cudaStreamSynchronize(e->stream), "batch frame records");
+    if ((s = ensure_out(e, cap))) return s;
+    uint32_t saved_mode = e->mode;
+    if (e->mode == OXPT_MODE_MEGAKERNEL) e->mode = OXPT_MODE_WAVEFRONT_SPLIT;
+    size_t off = 0;
+    for (auto& r : rounds) {
+        uint64_t total = 0;
+        for (const oxpt::BatchPiece& pc : r) total += (uint64_t)fr[pc.frame].ctx->w * pc.rows * pc.count;
+        uint32_t P = (uint32_t)std::min<uint64_t>(total, e->wave_slots);
+        oxd::WaveArgs wa;
+        if ((s = ensure_wave(e, P, J, &wa.st, &wa.q, &wa.ctr, &wa.work))) break;
+        wa.s = recs[off].s;
+        wa.slots = P;
+        wa.vcap = P;
+        wa.jobs = J;
+        wa.first = wa.y0 = wa.npix = 0;
+        wa.total = total;
+        wa.out = e->out;
+        wa.counters = nullptr;
+        wa.err = e->dev_err;
+        wa.frames = e->batch_dev + off;
+        wa.nframes = (uint32_t)r.size();
+        oxpt_ctx::Timed tt{nullptr, nullptr, 0};
+        if (e->timing) {
+            cudaEventCreate(&tt.a);
+            cudaEventCreate(&tt.b);
+            cudaEventRecord(tt.a, e->stream);
+        }
+        if ((s = wave_loop(e, wa, false, e->shadow_walk == 0, sd, sd, max_bounces))) break;
+        if (e->timing) {
+            cudaEventRecord(tt.b, e->stream);
+            e->timed.push_back(tt);
+        }
+        for (size_t k = 0; k < r.size(); k++) {
+            const oxpt::BatchPiece& pc = r[k];
+            oxpt_ctx* c = fr[pc.frame].ctx;
+            oxd::ReduceArgs ra{c->accum, e->out + pc.base, c->w, pc.y0, c->w * pc.rows, pc.count};
+            cudaError_t ce = oxd::launch_reduce(ra, e->stream);
+            if (ce != cudaSuccess) {
+                s = cuda_fail(e, ce, "batch reduce");
+                break;
+            }
+            e->launches += 1;
+        }
+        if (s) break;
+        off += r.size();
+    }
+    e->mode = saved_mode;
+    if (s) return s;
+    // Later work on the frame contexts' own streams waits for the batch.
+    if (!e->batch_done) CK(e, cudaEventCreateWithFlags(&e->batch_done, cudaEventDisableTiming), "batch event");
+    CK(e, cudaEventRecord(e->batch_done, e->stream), "batch event");
+    for (uint32_t k = 0; k < n; k++) {
+        oxpt_ctx* c = fr[k].ctx;
+        if (c && c->stream != e->stream) CK(e, cudaStreamWaitEvent(c->stream, e->batch_done, 0), "batch event");
+    }
     return OXPT_OK;
 }
 

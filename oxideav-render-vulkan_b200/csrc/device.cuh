@@ -108,9 +108,10 @@ struct Scene {
     const uint2* atlas;  // RGBA16F texels
     uint32_t side, layers;
     oxpt_params P;
-    // Four-wide tree for any-hit queries (8 float4 per node), or null.
+    // Four-wide tree for any-hit queries (8 float4 per node), or null;
+    // bvh4_ok: 1 when it answers this scene's any-hit queries exactly.
     const float4* bvh4 = nullptr;
-    uint32_t bvh4_root = 0xffffffffu, bvh4_nodes = 0u;
+    uint32_t bvh4_root = 0xffffffffu, bvh4_nodes = 0u, bvh4_ok = 0u, pad_ = 0u;
 };
 
 __device__ __forceinline__ uint32_t tw(const Scene& s, uint32_t i) {

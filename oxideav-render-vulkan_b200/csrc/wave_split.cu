@@ -135,13 +135,39 @@ __device__ __forceinline__ void get_vertex(const WaveArgs& a, uint32_t v, Vertex
     x->ng = b.ng;
 }
 
+// Batched launches (frames of several scenes in one wavefront): the frame
+// of a launch item, and the scene of a slot.
+__device__ __forceinline__ uint32_t frame_of1(const WaveArgs& a, unsigned long long item) {
+    uint32_t lo = 0u, hi = a.nframes;
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a.frames[mid].base <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <bool BATCH>
+__device__ __forceinline__ const Scene& slot_scene(const WaveArgs& a, uint32_t i) {
+    return BATCH ? a.frames[a.st.frame[i]].s : a.s;
+}
+
+// Shared-memory tables come from the first frame in a batched launch (the
+// host checks that every scene holds the same words).
+template <bool BATCH>
+__device__ __forceinline__ const Scene& tables_of(const WaveArgs& a) {
+    return BATCH ? a.frames[0].s : a.s;
+}
+
 }  // namespace
 
-template <bool COUNT>
+template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ WaveArgs a) {
     __shared__ uint32_t s_sobol[128];
-    const Scene& s = a.s;
-    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s, s.P.offs0[0] + i);
+    {
+        const Scene& s0 = tables_of<BATCH>(a);
+        for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s0, s0.P.offs0[0] + i);
+    }
     __syncthreads();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.slots) return;
@@ -151,6 +177,7 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
     uint32_t stage = __float_as_uint(a.st.rad[i].w) & 3u;
     bool need_new = stage == ST_EMPTY;
     if (!need_new) {
+        const Scene& s = slot_scene<BATCH>(a, i);
         load_state(a, i, &pc, &smp);
         uint32_t n = a.st.nee_n[i];
         for (uint32_t j = 0; j < n; j++) {
@@ -175,11 +202,17 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
     }
     unsigned long long item = fetch1(a.work);
     if (item < a.total) {
-        uint32_t it = (uint32_t)(item / a.npix);
-        uint32_t q = (uint32_t)(item - (unsigned long long)it * a.npix);
+        uint32_t f = BATCH ? frame_of1(a, item) : 0u;
+        const Scene& s = BATCH ? a.frames[f].s : a.s;
+        unsigned long long local = BATCH ? item - a.frames[f].base : item;
+        uint32_t npix = BATCH ? a.frames[f].npix : a.npix;
+        uint32_t y0 = BATCH ? a.frames[f].y0 : a.y0, first = BATCH ? a.frames[f].first : a.first;
+        uint32_t it = (uint32_t)(local / npix);
+        uint32_t q = (uint32_t)(local - (unsigned long long)it * npix);
         uint32_t yy = q / s.P.dims[0];
-        f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], a.y0 + yy, a.first + it, &smp, &pc);
+        f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], y0 + yy, first + it, &smp, &pc);
         a.st.item[i] = item;
+        if (BATCH) a.st.frame[i] = f;
         save_state(a, i, pc, smp, ST_TRACING);
         a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
         a.q.ext[append1(&a.ctr[0])] = i;
@@ -192,18 +225,21 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
     }
 }
 
-template <bool COUNT, int MINB>
+template <bool COUNT, int MINB, bool BATCH>
 __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__ WaveArgs a) {
     __shared__ uint32_t s_sobol[128];
     __shared__ float s_sheen[512];
-    const Scene& s = a.s;
-    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s, s.P.offs0[0] + i);
-    for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s, s.P.offs0[1] + i);
+    {
+        const Scene& s0 = tables_of<BATCH>(a);
+        for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s0, s0.P.offs0[0] + i);
+        for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s0, s0.P.offs0[1] + i);
+    }
     __syncthreads();
     const uint32_t n = *((volatile uint32_t*)&a.ctr[3]);
     unsigned long long shaded = 0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         uint32_t i = a.q.shade[q];
+        const Scene& s = slot_scene<BATCH>(a, i);
         PathCore pc;
         Sampler smp;
         load_state(a, i, &pc, &smp);
@@ -218,7 +254,7 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
         uint32_t v = append1(&a.ctr[4]);
         put_vertex(a, v, vx, pc, smp.path_seed);
         a.q.vslot[v] = i;
-        a.st.nee_n[i] = a.jobs;
+        a.st.nee_n[i] = BATCH ? s.P.cfg[2] + 1u : a.jobs;
         f3 o;
         if (continue_path(s, s_sheen, s_sobol, smp, pc, vx, &o)) {
             save_state(a, i, pc, smp, ST_TRACING);
@@ -231,11 +267,13 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
     if (COUNT && shaded) atomicAdd(a.counters + C_SHADED, shaded);
 }
 
-template <bool COUNT, int MINB>
+template <bool COUNT, int MINB, bool BATCH>
 __global__ void __launch_bounds__(128, MINB) split_nee(const __grid_constant__ WaveArgs a) {
     __shared__ float s_sheen[512];
-    const Scene& s = a.s;
-    for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s, s.P.offs0[1] + i);
+    {
+        const Scene& s0 = tables_of<BATCH>(a);
+        for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s0, s0.P.offs0[1] + i);
+    }
     __syncthreads();
     const uint32_t nv = *((volatile uint32_t*)&a.ctr[4]);
     const uint64_t total = (uint64_t)nv * a.jobs;
@@ -244,6 +282,8 @@ __global__ void __launch_bounds__(128, MINB) split_nee(const __grid_constant__ W
         uint32_t j = (uint32_t)(t / nv);
         uint32_t v = (uint32_t)(t - (uint64_t)j * nv);
         uint32_t slot = a.q.vslot[v];
+        const Scene& s = slot_scene<BATCH>(a, slot);
+        if (BATCH && j > s.P.cfg[2]) continue;  // beyond this scene's NEE jobs (its nee_n stops short)
         Vertex vx;
         PathCore pc;
         uint32_t path_seed;
@@ -263,17 +303,17 @@ __global__ void __launch_bounds__(128, MINB) split_nee(const __grid_constant__ W
 
 // Variants: shade kernel for 2 / 3 / 4 resident blocks per SM; the NEE
 // kernel for 4 / 5 / 6.
-template <bool C>
+template <bool C, bool B>
 static void* shade_fn(int v) {
-    if (v == 0) return (void*)split_shade<C, 2>;
-    if (v == 1) return (void*)split_shade<C, 3>;
-    return (void*)split_shade<C, 4>;
+    if (v == 0) return (void*)split_shade<C, 2, B>;
+    if (v == 1) return (void*)split_shade<C, 3, B>;
+    return (void*)split_shade<C, 4, B>;
 }
-template <bool C>
+template <bool C, bool B>
 static void* nee_fn(int v) {
-    if (v == 0) return (void*)split_nee<C, 4>;
-    if (v == 1) return (void*)split_nee<C, 5>;
-    return (void*)split_nee<C, 6>;
+    if (v == 0) return (void*)split_nee<C, 4, B>;
+    if (v == 1) return (void*)split_nee<C, 5, B>;
+    return (void*)split_nee<C, 6, B>;
 }
 
 static cudaError_t persistent(void* fn, const WaveArgs& a, int sms, cudaStream_t st) {
@@ -284,21 +324,30 @@ static cudaError_t persistent(void* fn, const WaveArgs& a, int sms, cudaStream_t
     return cudaLaunchKernel(fn, dim3((unsigned)(sms * (per_sm > 0 ? per_sm : 1))), dim3(128), args, 0, st);
 }
 
+// Batched launches (a.nframes > 0) have no counting build.
 cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st) {
     unsigned blocks = (a.slots + 127u) / 128u;
-    if (count) split_logic<true><<<blocks, 128, 0, st>>>(a);
-    else split_logic<false><<<blocks, 128, 0, st>>>(a);
+    if (a.nframes) {
+        if (count) return cudaErrorInvalidValue;
+        split_logic<false, true><<<blocks, 128, 0, st>>>(a);
+    } else if (count) {
+        split_logic<true, false><<<blocks, 128, 0, st>>>(a);
+    } else {
+        split_logic<false, false><<<blocks, 128, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_split_shade(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st) {
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
-    return persistent(count ? shade_fn<true>(variant) : shade_fn<false>(variant), a, sms, st);
+    if (a.nframes) return count ? cudaErrorInvalidValue : persistent(shade_fn<false, true>(variant), a, sms, st);
+    return persistent(count ? shade_fn<true, false>(variant) : shade_fn<false, false>(variant), a, sms, st);
 }
 
 cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st) {
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
-    return persistent(count ? nee_fn<true>(variant) : nee_fn<false>(variant), a, sms, st);
+    if (a.nframes) return count ? cudaErrorInvalidValue : persistent(nee_fn<false, true>(variant), a, sms, st);
+    return persistent(count ? nee_fn<true, false>(variant) : nee_fn<false, false>(variant), a, sms, st);
 }
 
 }  // namespace oxd

@@ -83,13 +83,62 @@ __device__ __forceinline__ void set_stage(const WaveArgs& a, uint32_t i, uint32_
     a.st.rad[i] = r;
 }
 
-template <bool COUNT, int MINB>
+// The frame of launch item `item` in a batched launch (frames ordered by
+// base, none empty).
+__device__ __forceinline__ uint32_t frame_of(const WaveArgs& a, unsigned long long item) {
+    uint32_t lo = 0u, hi = a.nframes;
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a.frames[mid].base <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The scene of slot i: the launch's own, or in a batched launch that of the
+// frame the slot's path belongs to.
+template <bool BATCH>
+__device__ __forceinline__ const Scene& scene_of(const WaveArgs& a, uint32_t i) {
+    return BATCH ? a.frames[a.st.frame[i]].s : a.s;
+}
+
+// Starts the path of launch item `item` in slot i (camera ray queued).
+template <bool BATCH>
+__device__ __forceinline__ void start_item(const WaveArgs& a, const uint32_t* s_sobol, uint32_t i,
+                                           unsigned long long item, PathCore* pc, Sampler* smp) {
+    uint32_t f = BATCH ? frame_of(a, item) : 0u;
+    const Scene& s = BATCH ? a.frames[f].s : a.s;
+    unsigned long long local = BATCH ? item - a.frames[f].base : item;
+    uint32_t npix = BATCH ? a.frames[f].npix : a.npix;
+    uint32_t y0 = BATCH ? a.frames[f].y0 : a.y0, first = BATCH ? a.frames[f].first : a.first;
+    uint32_t it = (uint32_t)(local / npix);
+    uint32_t q = (uint32_t)(local - (unsigned long long)it * npix);
+    uint32_t yy = q / s.P.dims[0];
+    f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], y0 + yy, first + it, smp, pc);
+    a.st.item[i] = item;
+    if (BATCH) a.st.frame[i] = f;
+    store_core(a, i, *pc, *smp, ST_TRACING);
+    a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
+    a.q.ext[append(&a.ctr[0])] = i;
+}
+
+// The tables staged in shared memory (Sobol' direction numbers, sheen
+// albedo) are the same words in every scene; a batched launch checks this
+// on the host and stages the first frame's.
+template <bool BATCH>
+__device__ __forceinline__ const Scene& table_scene(const WaveArgs& a) {
+    return BATCH ? a.frames[0].s : a.s;
+}
+
+template <bool COUNT, int MINB, bool BATCH>
 __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ WaveArgs a) {
     __shared__ uint32_t s_sobol[128];
     __shared__ float s_sheen[512];
-    const Scene& s = a.s;
-    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s, s.P.offs0[0] + i);
-    for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s, s.P.offs0[1] + i);
+    {
+        const Scene& s0 = table_scene<BATCH>(a);
+        for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) s_sobol[i] = tw(s0, s0.P.offs0[0] + i);
+        for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s0, s0.P.offs0[1] + i);
+    }
     __syncthreads();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.slots) return;
@@ -102,6 +151,8 @@ __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ 
     uint32_t stage = flags & 3u;
     bool need_new = stage == ST_EMPTY;
     if (!need_new) {
+        const Scene& s = scene_of<BATCH>(a, i);
+        const uint32_t Js = BATCH ? s.P.cfg[2] + 1u : J;  // this scene's NEE jobs
         load_core(a, i, &pc, &smp, &flags);
         // The previous vertex's NEE terms, in job order.
         uint32_t n = a.st.nee_n[i];
@@ -131,7 +182,7 @@ __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ 
                 covered = outcome != PATH_UNCOVERED;
             } else {
                 uint32_t armed = 0;
-                for (uint32_t j = 0; j < J; j++) {
+                for (uint32_t j = 0; j < Js; j++) {
                     ShadowRay sr;
                     float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (nee_job(s, s_sheen, pc, vx, j, &sr)) {
@@ -165,14 +216,7 @@ __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ 
     if (need_new) {
         unsigned long long item = fetch_item(a.work);
         if (item < a.total) {
-            uint32_t it = (uint32_t)(item / a.npix);
-            uint32_t q = (uint32_t)(item - (unsigned long long)it * a.npix);
-            uint32_t yy = q / s.P.dims[0];
-            f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], a.y0 + yy, a.first + it, &smp, &pc);
-            a.st.item[i] = item;
-            store_core(a, i, pc, smp, ST_TRACING);
-            a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
-            a.q.ext[append(&a.ctr[0])] = i;
+            start_item<BATCH>(a, s_sobol, i, item, &pc, &smp);
             paths = 1;
         } else {
             if (stage != ST_EMPTY) set_stage(a, i, 0u, ST_EMPTY);
@@ -190,7 +234,7 @@ __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ 
     }
 }
 
-template <bool COUNT, int MINB, int SD>
+template <bool COUNT, int MINB, int SD, bool BATCH>
 __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
@@ -205,8 +249,8 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const
         Hit h;
         uint32_t m = 0u;
         bump<COUNT>(cnt, C_PATH_RAYS);
-        bool got = traverse<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), INF, smp, k << 16u, k == 0u, false, NONE, &h, &m,
-                                   cnt, a.err);
+        bool got = traverse<COUNT, SD>(scene_of<BATCH>(a, i), make_ray(xyz(o), xyz(d)), INF, smp, k << 16u, k == 0u,
+                                       false, NONE, &h, &m, cnt, a.err);
         if (got) {
             f3 b = h.b;
             a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(b.y), __float_as_uint(b.z));
@@ -220,8 +264,9 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const
             if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
 }
 
-// FOUR: walk the four-wide tree (same occlusion as the binary walk).
-template <bool COUNT, int MINB, int SD, bool FOUR>
+// FOUR: walk the four-wide tree (same occlusion as the binary walk); in a
+// batched launch only for the scenes that have one.
+template <bool COUNT, int MINB, int SD, bool FOUR, bool BATCH>
 __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
@@ -230,14 +275,16 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
         uint4 m = a.q.sh_m[q];
+        const Scene& s = scene_of<BATCH>(a, m.x);
         Sampler smp{0u, 0u, m.w};
         Hit h;
         uint32_t mat = 0u;
         bump<COUNT>(cnt, C_SHADOW_RAYS);
-        bool got = FOUR ? occluded4<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, __float_as_uint(d.w),
-                                               &h, &mat, cnt, a.err)
-                        : traverse<COUNT, SD>(a.s, make_ray(xyz(o), xyz(d)), o.w, smp, m.z, false, true,
-                                              __float_as_uint(d.w), &h, &mat, cnt, a.err);
+        Ray r = make_ray(xyz(o), xyz(d));
+        bool got = (FOUR && (!BATCH || s.bvh4_ok))
+                       ? occluded4<COUNT, SD>(s, r, o.w, smp, m.z, false, __float_as_uint(d.w), &h, &mat, cnt, a.err)
+                       : traverse<COUNT, SD>(s, r, o.w, smp, m.z, false, true, __float_as_uint(d.w), &h, &mat, cnt,
+                                             a.err);
         if (!got) a.st.pend[(uint64_t)m.x * a.jobs + m.y].w = 2.0f;
     }
     if (COUNT)
@@ -247,52 +294,56 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
 
 // Compiled variants: logic kernel occupancy targets 2 / 3 / 4 resident
 // blocks per SM, traversal kernels 6 / 8 / 10 blocks with a 32- or 64-deep
-// stack. The tuner picks one; all give the same results.
-template <bool C>
+// stack; batched launches have no counting build. The tuner picks one; all
+// give the same results.
+template <bool C, bool B>
 static cudaError_t logic_v(const WaveArgs& a, int v, unsigned blocks, cudaStream_t st) {
     switch (v) {
-        case 0: wave_logic<C, 2><<<blocks, 128, 0, st>>>(a); break;
-        case 1: wave_logic<C, 3><<<blocks, 128, 0, st>>>(a); break;
-        default: wave_logic<C, 4><<<blocks, 128, 0, st>>>(a); break;
+        case 0: wave_logic<C, 2, B><<<blocks, 128, 0, st>>>(a); break;
+        case 1: wave_logic<C, 3, B><<<blocks, 128, 0, st>>>(a); break;
+        default: wave_logic<C, 4, B><<<blocks, 128, 0, st>>>(a); break;
     }
     return cudaGetLastError();
 }
 
-template <bool C, int SD>
+template <bool C, int SD, bool B>
 static void* ext_fn(int v) {
-    if (v == 0) return (void*)wave_extend<C, 6, SD>;
-    if (v == 1) return (void*)wave_extend<C, 8, SD>;
-    return (void*)wave_extend<C, 10, SD>;
+    if (v == 0) return (void*)wave_extend<C, 6, SD, B>;
+    if (v == 1) return (void*)wave_extend<C, 8, SD, B>;
+    return (void*)wave_extend<C, 10, SD, B>;
 }
 
-template <bool C, int SD, bool FOUR>
+template <bool C, int SD, bool FOUR, bool B>
 static void* shadow_fn(int v) {
-    if (v == 0) return (void*)wave_shadow<C, 6, SD, FOUR>;
-    if (v == 1) return (void*)wave_shadow<C, 8, SD, FOUR>;
-    return (void*)wave_shadow<C, 10, SD, FOUR>;
+    if (v == 0) return (void*)wave_shadow<C, 6, SD, FOUR, B>;
+    if (v == 1) return (void*)wave_shadow<C, 8, SD, FOUR, B>;
+    return (void*)wave_shadow<C, 10, SD, FOUR, B>;
 }
 
-template <bool C>
+template <bool C, bool B>
 static void* trav_kernel_c(bool ext, bool four, int v, int sd) {
-    if (ext) return sd <= 32 ? ext_fn<C, 32>(v) : ext_fn<C, 64>(v);
-    if (four) return sd <= 32 ? shadow_fn<C, 32, true>(v) : shadow_fn<C, 64, true>(v);
-    return sd <= 32 ? shadow_fn<C, 32, false>(v) : shadow_fn<C, 64, false>(v);
+    if (ext) return sd <= 32 ? ext_fn<C, 32, B>(v) : ext_fn<C, 64, B>(v);
+    if (four) return sd <= 32 ? shadow_fn<C, 32, true, B>(v) : shadow_fn<C, 64, true, B>(v);
+    return sd <= 32 ? shadow_fn<C, 32, false, B>(v) : shadow_fn<C, 64, false, B>(v);
 }
 
-static void* trav_kernel(bool count, bool ext, bool four, int v, int sd) {
-    return count ? trav_kernel_c<true>(ext, four, v, sd) : trav_kernel_c<false>(ext, four, v, sd);
+static void* trav_kernel(bool count, bool batch, bool ext, bool four, int v, int sd) {
+    if (batch) return count ? nullptr : trav_kernel_c<false, true>(ext, four, v, sd);
+    return count ? trav_kernel_c<true, false>(ext, four, v, sd) : trav_kernel_c<false, false>(ext, four, v, sd);
 }
 
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st) {
     unsigned blocks = (a.slots + 127u) / 128u;
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
-    return count ? logic_v<true>(a, variant, blocks, st) : logic_v<false>(a, variant, blocks, st);
+    if (a.nframes) return count ? cudaErrorInvalidValue : logic_v<false, true>(a, variant, blocks, st);
+    return count ? logic_v<true, false>(a, variant, blocks, st) : logic_v<false, false>(a, variant, blocks, st);
 }
 
 static cudaError_t launch_trav(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
                                cudaStream_t st) {
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
-    void* fn = trav_kernel(count, ext, four, variant, sd);
+    void* fn = trav_kernel(count, a.nframes > 0, ext, four, variant, sd);
+    if (!fn) return cudaErrorInvalidValue;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, WAVE_TRAVERSE_THREADS, 0);
     unsigned blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));

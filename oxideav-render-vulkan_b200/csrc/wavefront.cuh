@@ -25,6 +25,17 @@ struct WaveState {
     uint32_t* hmeta;           // material | front << 31
     uint32_t* nee_n;           // NEE jobs of the last vertex to add (0..J)
     float4* pend;              // slots x J: contribution.xyz, 0 none / 1 queued / 2 visible
+    uint32_t* frame;           // batched launches: the slot's frame
+};
+
+// One frame of a batched launch: a scene's samples [first, first + count)
+// over npix pixels from row y0, as the launch's items [base, base + total).
+// Every path keeps its pixel, sample index and scene, so its result is the
+// one the frame's own launch gives.
+struct BatchFrame {
+    Scene s;
+    unsigned long long base, total;
+    uint32_t first, y0, npix, pad;
 };
 
 struct WaveQueues {
@@ -51,10 +62,16 @@ struct WaveArgs {
     float4* out;
     unsigned long long* counters;
     uint32_t* err;
+    // batched launches (null / 0 otherwise): frames ordered by base; `s`,
+    // first, y0 and npix are then unused, `jobs` is the largest NEE job
+    // count of the frames and out is indexed by launch item.
+    const BatchFrame* frames;
+    uint32_t nframes;
 };
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3
 // / 4 blocks per SM; traversal 6 / 8 / 10); `stack`: 32 or 64 entries.
+// With a.nframes > 0 the batched kernels run (count must then be false).
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st);
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
 // four: any-hit walk over the four-wide tree (Scene::bvh4) instead of the

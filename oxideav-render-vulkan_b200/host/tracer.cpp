@@ -10,6 +10,7 @@
 #include <optional>
 #include <string>
 
+#include "../../include/oxpt_batch.h"
 #include "model.hpp"
 
 namespace {
@@ -240,6 +241,34 @@ oxpt_status oxpt_tracer_refine(oxpt_tracer* t, uint32_t n) { return t->refine(n)
 oxpt_status oxpt_tracer_refine_rows(oxpt_tracer* t, uint32_t n, uint32_t y0, uint32_t rows) {
     return t->refine_rows(n, y0, rows);
 }
+oxpt_status oxpt_tracers_refine_batch(oxpt_tracer* const* ts, uint32_t count, const uint32_t* samples,
+                                      oxpt_ctx* exec) {
+    if (count == 0) return OXPT_OK;
+    if (!ts || !samples) return OXPT_E_INVALID;
+    std::vector<oxpt_batch_frame> frames;
+    std::vector<uint32_t> adds(count, 0);
+    for (uint32_t k = 0; k < count; k++) {
+        oxpt_tracer* t = ts[k];
+        if (!t) return OXPT_E_INVALID;
+        if (!t->scene || samples[k] == 0) continue;
+        uint32_t n = std::min(samples[k], 0xffffffffu - t->samples);
+        oxpt_status st = t->ensure_binding();
+        if (st) return st;
+        frames.push_back({t->ctx, t->samples, n, 0u, t->h});
+        adds[k] = n;
+    }
+    if (frames.empty()) return OXPT_OK;
+    oxpt_ctx* e = exec ? exec : frames[0].ctx;
+    oxpt_status st = oxpt_refine_batch(e, frames.data(), (uint32_t)frames.size());
+    if (st) {
+        for (uint32_t k = 0; k < count; k++)
+            if (adds[k]) ts[k]->err = oxpt_last_error(e);
+        return st;
+    }
+    for (uint32_t k = 0; k < count; k++) ts[k]->samples += adds[k];
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_tracer_finish(oxpt_tracer* t) { return t->check(oxpt_finish(t->ctx)); }
 oxpt_status oxpt_tracer_image(oxpt_tracer* t, uint8_t* out) { return t->resolve(false, out, nullptr); }
 oxpt_status oxpt_tracer_hdr(oxpt_tracer* t, float* out) { return t->resolve(true, out, nullptr); }

@@ -406,6 +406,27 @@ class GpuPathTracer:
         return self.hdr()
 
 
+def refine_batch(tracers, samples, executor: Optional["GpuPathTracer"] = None):
+    """refine() of several tracers traced as one wavefront (oxpt_batch.h).
+
+    `samples` is one count for all or one per tracer. Every tracer's
+    accumulation ends bit-identical to its own refine(); the executor's
+    (default: the first tracer's) stream and execution plan run the batch."""
+    tracers = list(tracers)
+    if not tracers:
+        return
+    counts = [int(samples)] * len(tracers) if np.isscalar(samples) else [int(x) for x in samples]
+    if len(counts) != len(tracers):
+        raise ValueError("one sample count per tracer")
+    hs = (C.c_void_p * len(tracers))(*[t._h for t in tracers])
+    ns = (N.u32 * len(tracers))(*counts)
+    ex = executor.ctx if executor is not None else None
+    st = N.lib().oxpt_tracers_refine_batch(hs, len(tracers), ns, ex)
+    if st != N.OK:
+        who = executor if executor is not None else tracers[0]
+        _raise(st, N.lib().oxpt_last_error(who.ctx).decode())
+
+
 class GpuMode(enum.Enum):
     """Which pipeline GpuRenderer renders with; only the path tracer exists
     here (the rasteriser is outside this build)."""
