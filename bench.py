@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
                     help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
+    ap.add_argument("--workload", default="single", choices=["single", "batch"],
+                    help="single: the large scene (headline); batch: 64 mixed scenes in batched launches")
+    ap.add_argument("--scenes", type=int, default=64, help="batch workload: number of scenes")
     return ap.parse_args()
 
 
@@ -213,10 +216,103 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+BATCH_RES = [(256, 256), (512, 512), (768, 432), (1024, 1024)]
+BATCH_SPP = [16, 64, 256]
+
+
+def batch_workload(pkg, a, seed=2):
+    """64 seeded scenes: triangle counts log-uniform in [1e3, 5e5] (displaced
+    icospheres and box fields alternating), the mixed material model (20%
+    volume transmission, 20% clearcoat, 10% sheen), resolutions from
+    {256^2, 512^2, 768x432, 1024^2} and spp from {16, 64, 256}."""
+    rng = np.random.default_rng(seed)
+    items = []
+    for k in range(a.scenes):
+        tris = float(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+        if k % 2 == 0:
+            freq = max(8, int(round(np.sqrt(tris / 20.0))))
+            scene = pkg.Scene.icosphere(freq=freq, seed=100 + k, n_materials=16, n_textures=2, tex_size=256,
+                                        n_punctual=4, n_emissive=16, material_mix=1)
+        else:
+            scene = pkg.Scene.box_field(max(1, int(tris / 12)), seed=100 + k, material_mix=1)
+        w, h = BATCH_RES[int(rng.integers(len(BATCH_RES)))]
+        spp = BATCH_SPP[int(rng.integers(len(BATCH_SPP)))]
+        items.append((scene, w, h, spp))
+    return items
+
+
+def run_batch(a):
+    """Batched launches of the 64-scene workload against the same scenes
+    refined one after another, each by its own plain refine."""
+    import torch
+    torch.cuda.set_device(0)
+    __graft_entry__.build()
+    pkg = __graft_entry__.load_package()
+    from oxideav_render_vulkan_b200 import tuner
+    items = batch_workload(pkg, a)
+    env = pkg.EnvironmentMap.sky(256, 128)
+    tracers = []
+    for scene, w, h, spp in items:
+        t = pkg.GpuPathTracer(0)
+        t.set_environment(env)
+        t.sync(scene, pkg.RenderOptions(width=w, height=h, scene_camera=0,
+                                        path_trace=pkg.PathTraceOptions(samples_per_pixel=spp, max_bounces=8)))
+        t.prepared()
+        tracers.append(t)
+    spps = [it[3] for it in items]
+    paths = sum(it[1] * it[2] * it[3] for it in items)
+    ex = pkg.GpuPathTracer(0)
+    tune_log = []
+    plan = tuner.tune_batch(tracers, ex, log=tune_log)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            for t in tracers:
+                t.reset()
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            for t in tracers:
+                t.reset()
+            for t in tracers:
+                t.finish()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record()
+            fn()
+            for t in tracers:
+                t.finish()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(max(e0.elapsed_time(e1), 1e3 * (time.perf_counter() - t0)))
+        return ms
+
+    batch_ms = timed(lambda: pkg.refine_batch(tracers, spps, executor=ex), a.steps, a.warmup)
+    accs = [t.read_accum().copy() for t in tracers[:4]]
+    serial_ms = timed(lambda: [t.refine(n) for t, n in zip(tracers, spps)], max(1, a.steps - 1), 1)
+    same = all(np.array_equal(x.view(np.uint32), t.read_accum().view(np.uint32)) for x, t in zip(accs, tracers))
+    value = paths / (statistics.median(batch_ms) / 1e3) / 1e6
+    serial = paths / (statistics.median(serial_ms) / 1e3) / 1e6
+    line = {"metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": statistics.median(batch_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched {a.scenes} scenes (triangles log-uniform 1e3..5e5, mixed materials, "
+                                   "resolutions 256^2..1024^2, spp 16/64/256)",
+                       "paths_per_step": paths, "triangles": sum(int(it[0].triangle_count()) for it in items),
+                       "timing": "host wall clock around the step (includes launch gaps), max with CUDA events"},
+            "serial_plain_value": serial, "speedup_vs_serial": value / serial,
+            "serial_matches_batch": same, "plan": tuner.describe(plan), "tuner_trials": len(tune_log)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload == "batch":
+        run_batch(a)
         return
     import torch
     import torch.distributed as dist
@@ -388,7 +484,7 @@ def plan_of(pt):
     t = pt.tuning()
     return {"mode": ["megakernel", "wavefront", "wavefront-split"][t.mode], "wave_slots": t.wave_slots,
             "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack,
-            "nee_variant": t.nee_variant}
+            "nee_variant": t.nee_variant, "shadow_walk": ["four-wide", "binary"][t.shadow_walk]}
 
 
 def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank):

@@ -107,6 +107,10 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *   shadow_walk    wavefront shadow rays: 0 = the four-wide tree built on
  *                  upload when the scene allows it (same occlusion), 1 =
  *                  the binary ordered walk.
+ *   graphs         batched refinement (oxpt_batch.h) as one CUDA graph per
+ *                  refine step: each round's wavefront loop is a device-side
+ *                  while node (no host round trips), reused while the step's
+ *                  shape is unchanged; 0 = host-driven loop.
  */
 enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1, OXPT_MODE_WAVEFRONT_SPLIT = 2 };
 typedef struct oxpt_tuning {
@@ -122,6 +126,8 @@ typedef struct oxpt_tuning {
     uint32_t stack;
     uint32_t nee_variant;
     uint32_t shadow_walk;
+    uint32_t graphs;
+    uint32_t reserved;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);
@@ -137,10 +143,15 @@ oxpt_status oxpt_diag_bvh4(const oxpt_ctx* ctx, uint32_t out[4]);
  * more than 16 triangles). Needs no GPU. */
 oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint32_t* out, size_t cap,
                                  size_t* words, uint32_t* root, uint32_t* stack_need);
-/* Wavefront bounces (logic + extend + shadow launches) run so far. */
+/* Wavefront bounces (logic + extend + shadow launches) run so far (waits
+ * for the context's stream when graph-resident loops have run). */
 oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* ctx, uint64_t* out);
+/* CUDA graphs instantiated for batched refinement so far. */
+oxpt_status oxpt_diag_graph_builds(const oxpt_ctx* ctx, uint64_t* out);
 
-/* Number of trace / reduce / resolve kernels launched by this context. */
+/* Number of kernels launched by this context (waits for the context's
+ * stream when graph-resident loops have run, whose launches the device
+ * counts). */
 oxpt_status oxpt_diag_launch_count(const oxpt_ctx* ctx, uint64_t* out);
 
 #ifdef __cplusplus

@@ -103,13 +103,15 @@ class PreparedView(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("mode", u32), ("threads", u32), ("blocks_per_sm", u32), ("wave_slots", u32),
                 ("max_paths", u64), ("wave_items", u64), ("check_every", u32), ("shade_variant", u32),
-                ("trace_variant", u32), ("stack", u32), ("nee_variant", u32), ("shadow_walk", u32)]
+                ("trace_variant", u32), ("stack", u32), ("nee_variant", u32), ("shadow_walk", u32),
+                ("graphs", u32), ("reserved", u32)]
 
 
 MODE_MEGAKERNEL, MODE_WAVEFRONT, MODE_WAVEFRONT_SPLIT = 0, 1, 2
 
 assert C.sizeof(Params) == 176
 assert C.sizeof(ResolveParams) == 48
+assert C.sizeof(Tuning) == 64
 
 _SIGS = {
     # oxpt.h
@@ -147,6 +149,7 @@ _SIGS = {
     "oxpt_get_tuning": (cint, [vp, C.POINTER(Tuning)]),
     "oxpt_diag_wave_iterations": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_bvh4": (cint, [vp, C.POINTER(u32 * 4)]),
+    "oxpt_diag_graph_builds": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_bvh4_build": (cint, [vp, u32, vp, sz, C.POINTER(sz), C.POINTER(u32), C.POINTER(u32)]),
     "oxpt_diag_timing_kinds": (cint, [vp, vp, vp]),
     "oxpt_diag_counters_split": (cint, [vp, vp]),

@@ -89,6 +89,14 @@ struct oxpt_ctx {
     oxd::BatchFrame* batch_dev = nullptr;
     size_t batch_cap = 0;
     cudaEvent_t batch_done = nullptr;
+    std::vector<oxpt_ctx*> batch_ctx;  // frame contexts of the current batch
+    // CUDA-graph batches: the instantiated graph of the last step shape
+    uint32_t graphs = 0;
+    cudaStream_t capture = nullptr;  // stream the loop bodies are captured on
+    cudaGraphExec_t bgraph = nullptr;
+    std::vector<uint64_t> bgraph_key;
+    uint64_t graph_builds = 0;
+    unsigned long long* dev_tally = nullptr;  // graph loops: kernels launched, iterations
 };
 
 namespace {
@@ -306,18 +314,56 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     return wave_loop(c, wa, count, four, sd, sd4, c->params.dims[3]);
 }
 
-// Iterates the wavefront's kernels over `wa` until every slot is empty.
-// The bound on iterations (four times the bounces of every path a slot can
-// take, plus slack) turns a wavefront that does not drain into an error.
+// The iteration bound of a wavefront run: four times the bounces of every
+// path a slot can take, plus slack. A run that has not drained by then is
+// an error, not a hang.
+uint64_t wave_cap(const oxd::WaveArgs& wa, uint32_t max_bounces) {
+    uint64_t per_slot = wa.total / wa.slots + 1;
+    uint64_t bounces = std::min<uint64_t>(max_bounces, 1u << 20);
+    return 4 * (bounces + 2) * per_slot + 1024;
+}
+
+cudaError_t wave_init(const oxd::WaveArgs& wa, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(wa.st.rad, 0, (size_t)wa.slots * 16, st);
+    if (!e) e = cudaMemsetAsync(wa.st.nee_n, 0, (size_t)wa.slots * 4, st);
+    if (!e) e = cudaMemsetAsync(wa.ctr, 0, 64, st);
+    return e;
+}
+
+// Kernels of one wavefront iteration on `st`: queue reset, shading
+// (one logic kernel, or logic + surface shading + NEE jobs in the split
+// plan), extension and shadow traversal. `wrap(kind, launch)` runs each
+// launch (timing hooks); returns the kernels enqueued, or -1 on error.
+template <class Wrap>
+int enqueue_iteration(oxpt_ctx* c, const oxd::WaveArgs& wa, const oxd::WaveArgs& wsh, bool count, bool four, int sd,
+                      int sd4, cudaStream_t st, Wrap&& wrap, cudaError_t* err) {
+    int n = 0;
+    auto run = [&](int kind, auto&& launch) {
+        if (*err) return;
+        *err = wrap(kind, launch);
+        n++;
+    };
+    *err = cudaMemsetAsync(wa.ctr, 0, 32, st);
+    if (c->mode == OXPT_MODE_WAVEFRONT_SPLIT) {
+        run(2, [&] { return oxd::launch_split_logic(wa, count, st); });
+        run(5, [&] { return oxd::launch_split_shade(wa, count, (int)c->shade_variant, c->sms, st); });
+        run(6, [&] { return oxd::launch_split_nee(wa, count, (int)c->nee_variant, c->sms, st); });
+    } else {
+        run(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, st); });
+    }
+    run(3, [&] { return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, sd, c->sms, st); });
+    run(4, [&] {
+        return oxd::launch_wave_shadow(wsh, count, four, (int)c->trace_variant, four ? sd4 : sd, c->sms, st);
+    });
+    return *err ? -1 : n;
+}
+
+// Iterates the wavefront's kernels over `wa` until every slot is empty,
+// checking the active-slot count on the host every check_every iterations.
 oxpt_status wave_loop(oxpt_ctx* c, const oxd::WaveArgs& wa, bool count, bool four, int sd, int sd4,
                       uint32_t max_bounces) {
-    const uint32_t P = wa.slots;
-    CK(c, cudaMemsetAsync(wa.st.rad, 0, (size_t)P * 16, c->stream), "wave init");
-    CK(c, cudaMemsetAsync(wa.st.nee_n, 0, (size_t)P * 4, c->stream), "wave init");
-    CK(c, cudaMemsetAsync(wa.ctr, 0, 64, c->stream), "wave init");
-    uint64_t per_slot = wa.total / P + 1;
-    uint64_t bounces = std::min<uint64_t>(max_bounces, 1u << 20);
-    uint64_t cap = 4 * (bounces + 2) * per_slot + 1024;
+    CK(c, wave_init(wa, c->stream), "wave init");
+    const uint64_t cap = wave_cap(wa, max_bounces);
     oxd::WaveArgs wsh = wa;  // shadow rays count into the second counter half
     if (wsh.counters) wsh.counters += oxd::C_N;
     auto timed = [&](int kind, auto&& launch) -> cudaError_t {
@@ -336,27 +382,10 @@ oxpt_status wave_loop(oxpt_ctx* c, const oxd::WaveArgs& wa, bool count, bool fou
     };
     for (uint64_t it = 0;; it++) {
         if (it > cap) return fail(c, OXPT_E_TIMEOUT, "wavefront did not drain within its iteration bound");
-        CK(c, cudaMemsetAsync(wa.ctr, 0, 32, c->stream), "queue reset");
-        if (c->mode == OXPT_MODE_WAVEFRONT_SPLIT) {
-            CK(c, timed(2, [&] { return oxd::launch_split_logic(wa, count, c->stream); }), "split logic");
-            CK(c, timed(5, [&] {
-                   return oxd::launch_split_shade(wa, count, (int)c->shade_variant, c->sms, c->stream);
-               }), "split shade");
-            CK(c, timed(6, [&] { return oxd::launch_split_nee(wa, count, (int)c->nee_variant, c->sms, c->stream); }),
-               "split nee");
-            c->launches += 2;
-        } else {
-            CK(c, timed(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, c->stream); }),
-               "wave logic");
-        }
-        CK(c, timed(3, [&] {
-               return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, sd, c->sms, c->stream);
-           }), "wave extend");
-        CK(c, timed(4, [&] {
-               return oxd::launch_wave_shadow(wsh, count, four, (int)c->trace_variant, four ? sd4 : sd, c->sms,
-                                              c->stream);
-           }), "wave shadow");
-        c->launches += 3;
+        cudaError_t e = cudaSuccess;
+        int n = enqueue_iteration(c, wa, wsh, count, four, sd, sd4, c->stream, timed, &e);
+        if (n < 0) return cuda_fail(c, e, "wavefront iteration");
+        c->launches += (uint64_t)n;
         c->wave_iterations++;
         if ((it + 1) % c->check_every == 0) {
             CK(c, cudaMemcpyAsync(c->wave_host, wa.ctr, 16, cudaMemcpyDeviceToHost, c->stream), "queue readback");
@@ -479,6 +508,9 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
                     c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev};
     if (c->batch_done) cudaEventDestroy(c->batch_done);
+    if (c->bgraph) cudaGraphExecDestroy(c->bgraph);
+    if (c->dev_tally) cudaFree(c->dev_tally);
+    if (c->capture) cudaStreamDestroy(c->capture);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->wave_host) cudaFreeHost(c->wave_host);
@@ -638,6 +670,7 @@ oxpt_status oxpt_finish(oxpt_ctx* c) {
     CK(c, cudaMemcpy(&e, c->dev_err, 4, cudaMemcpyDeviceToHost), "error word");
     if (e) {
         cudaMemset(c->dev_err, 0, 4);
+        if (e & 8u) return fail(c, OXPT_E_TIMEOUT, "wavefront did not drain within its iteration bound");
         return fail(c, OXPT_E_LIMIT, "traversal exceeded the node count: malformed BVH");
     }
     return OXPT_OK;
@@ -828,7 +861,9 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     if (t->stack && t->stack != 32 && t->stack != 64) return fail(c, OXPT_E_INVALID, "stack is 0, 32 or 64");
     if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
     if (t->shadow_walk > 1) return fail(c, OXPT_E_INVALID, "shadow_walk is 0 or 1");
+    if (t->graphs > 1) return fail(c, OXPT_E_INVALID, "graphs is 0 or 1");
     c->shadow_walk = t->shadow_walk;
+    c->graphs = t->graphs;
     c->shade_variant = t->shade_variant;
     c->trace_variant = t->trace_variant;
     c->nee_variant = t->nee_variant;
@@ -851,6 +886,26 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->nee_variant = c->nee_variant;
     t->stack = c->stack;
     t->shadow_walk = c->shadow_walk;
+    t->graphs = c->graphs;
+    return OXPT_OK;
+}
+
+// Device-side tally of graph-resident loops: {kernels, iterations}.
+static void read_tally(const oxpt_ctx* c, uint64_t out[2]) {
+    out[0] = out[1] = 0;
+    if (!c->dev_tally) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    unsigned long long v[2] = {0, 0};
+    if (cudaMemcpy(v, c->dev_tally, 16, cudaMemcpyDeviceToHost) == cudaSuccess) {
+        out[0] = v[0];
+        out[1] = v[1];
+    }
+}
+
+oxpt_status oxpt_diag_graph_builds(const oxpt_ctx* c, uint64_t* out) {
+    if (!c || !out) return OXPT_E_INVALID;
+    *out = c->graph_builds;
     return OXPT_OK;
 }
 
@@ -878,7 +933,9 @@ oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint
 
 oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* c, uint64_t* out) {
     if (!c || !out) return OXPT_E_INVALID;
-    *out = c->wave_iterations;
+    uint64_t t[2];
+    read_tally(c, t);
+    *out = c->wave_iterations + t[1];
     return OXPT_OK;
 }
 
@@ -926,9 +983,127 @@ oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* c, double ms[8], uint64_t n[8
 
 oxpt_status oxpt_diag_launch_count(const oxpt_ctx* c, uint64_t* out) {
     if (!c || !out) return OXPT_E_INVALID;
-    *out = c->launches;
+    uint64_t t[2];
+    read_tally(c, t);
+    *out = c->launches + t[0];
     return OXPT_OK;
 }
+
+// ---------------------------------------------------------------------
+// Batched refinement as one CUDA graph per refine step.
+// ---------------------------------------------------------------------
+
+}  // extern "C"
+
+namespace {
+
+// Key of a batch graph: everything baked into its nodes (plan, buffers,
+// launch shapes, per-round sizes, reduce targets). Frame records (sample
+// indices, scene views) live in device memory and are re-uploaded before
+// every launch, so a refine step with the same shape reuses the graph.
+template <class Reduces>
+oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
+                            const std::vector<std::vector<oxpt::BatchPiece>>& rounds, int sd, bool four,
+                            uint32_t max_bounces, size_t pieces, Reduces&& enqueue_reduces) {
+    if (!e->dev_tally) {
+        CK(e, cudaMalloc((void**)&e->dev_tally, 16), "graph tally");
+        CK(e, cudaMemset(e->dev_tally, 0, 16), "graph tally");
+    }
+    if (!e->capture) CK(e, cudaStreamCreateWithFlags(&e->capture, cudaStreamNonBlocking), "capture stream");
+    std::vector<uint64_t> key = {e->mode, e->shade_variant, e->trace_variant, e->nee_variant, (uint64_t)sd,
+                                 four ? 1ull : 0ull, (uint64_t)e->sms, (uint64_t)(uintptr_t)e->wave_mem,
+                                 (uint64_t)(uintptr_t)e->out, (uint64_t)(uintptr_t)e->dev_err,
+                                 (uint64_t)(uintptr_t)e->stream, args.empty() ? 0 : args[0].vcap,
+                                 args.empty() ? 0 : args[0].jobs};
+    for (size_t k = 0; k < rounds.size(); k++) {
+        const oxd::WaveArgs& wa = args[k];
+        key.insert(key.end(), {wa.slots, wa.total, (uint64_t)(uintptr_t)wa.frames, wa.nframes,
+                               wave_cap(wa, max_bounces)});
+        for (const oxpt::BatchPiece& pc : rounds[k]) {
+            const oxpt_ctx* c = e->batch_ctx[pc.frame];
+            key.insert(key.end(), {(uint64_t)(uintptr_t)c->accum, c->w, pc.base, pc.y0, pc.rows, pc.count});
+        }
+    }
+    if (key != e->bgraph_key || !e->bgraph) {
+        if (e->bgraph) cudaGraphExecDestroy(e->bgraph);
+        e->bgraph = nullptr;
+        e->bgraph_key.clear();
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+        if (ce) return cuda_fail(e, ce, "graph capture");
+        auto abort_capture = [&](cudaError_t why, const char* what) {
+            cudaGraph_t dead = nullptr;
+            cudaStreamEndCapture(e->stream, &dead);
+            if (dead) cudaGraphDestroy(dead);
+            return cuda_fail(e, why, what);
+        };
+        for (size_t k = 0; k < rounds.size(); k++) {
+            const oxd::WaveArgs& wa = args[k];
+            if ((ce = wave_init(wa, e->stream))) return abort_capture(ce, "graph wave init");
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t cg = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            if ((ce = cudaStreamGetCaptureInfo(e->stream, &cs, nullptr, &cg, &deps, &nd)))
+                return abort_capture(ce, "graph capture info");
+            cudaGraphConditionalHandle h;
+            if ((ce = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault)))
+                return abort_capture(ce, "graph condition");
+            cudaGraphNodeParams np{};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            cudaGraphNode_t loop;
+            if ((ce = cudaGraphAddNode(&loop, cg, deps, nd, &np))) return abort_capture(ce, "graph loop node");
+            if ((ce = cudaStreamUpdateCaptureDependencies(e->stream, &loop, 1, cudaStreamSetCaptureDependencies)))
+                return abort_capture(ce, "graph loop dependency");
+            cudaGraph_t body = np.conditional.phGraph_out[0];
+            if ((ce = cudaStreamBeginCaptureToGraph(e->capture, body, nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeThreadLocal)))
+                return abort_capture(ce, "graph body capture");
+            cudaError_t ie = cudaSuccess;
+            int kernels = enqueue_iteration(e, wa, wa, false, four, sd, sd, e->capture,
+                                            [](int, auto&& launch) { return launch(); }, &ie);
+            if (kernels >= 0) {
+                uint64_t cap = std::min<uint64_t>(wave_cap(wa, max_bounces), 0xffffffffull);
+                ie = oxd::launch_wave_continue(h, wa.ctr, (uint32_t)cap, e->dev_err, e->dev_tally,
+                                               (uint32_t)kernels + 1u, e->capture);
+            }
+            cudaGraph_t body_out = nullptr;
+            cudaError_t ee = cudaStreamEndCapture(e->capture, &body_out);
+            if (ie) return abort_capture(ie, "graph body");
+            if (ee) return abort_capture(ee, "graph body capture end");
+            if ((ce = enqueue_reduces(k, e->stream))) return abort_capture(ce, "graph reduce");
+        }
+        if ((ce = cudaStreamEndCapture(e->stream, &g))) return cuda_fail(e, ce, "graph capture end");
+        ce = cudaGraphInstantiate(&e->bgraph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce) {
+            e->bgraph = nullptr;
+            return cuda_fail(e, ce, "graph instantiate");
+        }
+        e->bgraph_key = key;
+        e->graph_builds++;
+    }
+    oxpt_ctx::Timed tt{nullptr, nullptr, 0};
+    if (e->timing) {
+        cudaEventCreate(&tt.a);
+        cudaEventCreate(&tt.b);
+        cudaEventRecord(tt.a, e->stream);
+    }
+    CK(e, cudaGraphLaunch(e->bgraph, e->stream), "graph launch");
+    if (e->timing) {
+        cudaEventRecord(tt.b, e->stream);
+        e->timed.push_back(tt);
+    }
+    e->launches += pieces;  // reduces; the wavefront kernels are tallied on the device
+    return OXPT_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 // ---------------------------------------------------------------------
 // Batched refinement (oxpt_batch.h).
@@ -991,6 +1166,8 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
     uint64_t cap = e->wave_items;
     for (uint32_t k = 0; k < n; k++)
         if (fr[k].count && fr[k].rows) cap = std::max<uint64_t>(cap, fr[k].ctx->w);
+    e->batch_ctx.assign(n, nullptr);
+    for (uint32_t k = 0; k < n; k++) e->batch_ctx[k] = fr[k].ctx;
     auto rounds = oxpt::plan_batch(in, cap);
     if (rounds.empty()) return OXPT_OK;
     // Frame records of every round, uploaded at once.
@@ -1026,48 +1203,69 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
     if ((s = ensure_out(e, cap))) return s;
     uint32_t saved_mode = e->mode;
     if (e->mode == OXPT_MODE_MEGAKERNEL) e->mode = OXPT_MODE_WAVEFRONT_SPLIT;
-    size_t off = 0;
+    // Path state for the largest round, allocated before any launch (and
+    // before a graph capture, which allows no allocation).
+    std::vector<oxd::WaveArgs> args;
+    uint32_t pmax = 1;
     for (auto& r : rounds) {
         uint64_t total = 0;
         for (const oxpt::BatchPiece& pc : r) total += (uint64_t)fr[pc.frame].ctx->w * pc.rows * pc.count;
-        uint32_t P = (uint32_t)std::min<uint64_t>(total, e->wave_slots);
-        oxd::WaveArgs wa;
-        if ((s = ensure_wave(e, P, J, &wa.st, &wa.q, &wa.ctr, &wa.work))) break;
-        wa.s = recs[off].s;
-        wa.slots = P;
-        wa.vcap = P;
+        pmax = std::max(pmax, (uint32_t)std::min<uint64_t>(total, e->wave_slots));
+        oxd::WaveArgs wa{};
+        wa.total = total;
+        args.push_back(wa);
+    }
+    oxd::WaveArgs base{};
+    if ((s = ensure_wave(e, pmax, J, &base.st, &base.q, &base.ctr, &base.work))) {
+        e->mode = saved_mode;
+        return s;
+    }
+    size_t off = 0;
+    for (size_t k = 0; k < rounds.size(); k++) {
+        oxd::WaveArgs& wa = args[k];
+        uint64_t total = wa.total;
+        wa = base;
+        wa.slots = (uint32_t)std::min<uint64_t>(total, e->wave_slots);
+        wa.vcap = pmax;
         wa.jobs = J;
-        wa.first = wa.y0 = wa.npix = 0;
         wa.total = total;
         wa.out = e->out;
         wa.counters = nullptr;
         wa.err = e->dev_err;
         wa.frames = e->batch_dev + off;
-        wa.nframes = (uint32_t)r.size();
-        oxpt_ctx::Timed tt{nullptr, nullptr, 0};
-        if (e->timing) {
-            cudaEventCreate(&tt.a);
-            cudaEventCreate(&tt.b);
-            cudaEventRecord(tt.a, e->stream);
-        }
-        if ((s = wave_loop(e, wa, false, e->shadow_walk == 0, sd, sd, max_bounces))) break;
-        if (e->timing) {
-            cudaEventRecord(tt.b, e->stream);
-            e->timed.push_back(tt);
-        }
-        for (size_t k = 0; k < r.size(); k++) {
-            const oxpt::BatchPiece& pc = r[k];
+        wa.nframes = (uint32_t)rounds[k].size();
+        off += rounds[k].size();
+    }
+    const bool four = e->shadow_walk == 0;
+    auto enqueue_reduces = [&](size_t k, cudaStream_t st) -> cudaError_t {
+        for (const oxpt::BatchPiece& pc : rounds[k]) {
             oxpt_ctx* c = fr[pc.frame].ctx;
             oxd::ReduceArgs ra{c->accum, e->out + pc.base, c->w, pc.y0, c->w * pc.rows, pc.count};
-            cudaError_t ce = oxd::launch_reduce(ra, e->stream);
-            if (ce != cudaSuccess) {
-                s = cuda_fail(e, ce, "batch reduce");
-                break;
-            }
-            e->launches += 1;
+            cudaError_t ce = oxd::launch_reduce(ra, st);
+            if (ce != cudaSuccess) return ce;
         }
-        if (s) break;
-        off += r.size();
+        return cudaSuccess;
+    };
+    size_t pieces = off;
+    if (e->graphs) {
+        s = batch_graph_run(e, args, rounds, sd, four, max_bounces, pieces, enqueue_reduces);
+    } else {
+        for (size_t k = 0; k < rounds.size() && !s; k++) {
+            oxpt_ctx::Timed tt{nullptr, nullptr, 0};
+            if (e->timing) {
+                cudaEventCreate(&tt.a);
+                cudaEventCreate(&tt.b);
+                cudaEventRecord(tt.a, e->stream);
+            }
+            if ((s = wave_loop(e, args[k], false, four, sd, sd, max_bounces))) break;
+            if (e->timing) {
+                cudaEventRecord(tt.b, e->stream);
+                e->timed.push_back(tt);
+            }
+            cudaError_t ce = enqueue_reduces(k, e->stream);
+            if (ce != cudaSuccess) s = cuda_fail(e, ce, "batch reduce");
+            e->launches += rounds[k].size();
+        }
     }
     e->mode = saved_mode;
     if (s) return s;

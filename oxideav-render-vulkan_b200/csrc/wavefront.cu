@@ -352,6 +352,28 @@ static cudaError_t launch_trav(const WaveArgs& a, bool count, bool ext, bool fou
     return cudaLaunchKernel(fn, dim3(blocks), dim3(WAVE_TRAVERSE_THREADS), args, 0, st);
 }
 
+// ctr[10] counts the iterations of the current run (zeroed with the run's
+// counters; the per-iteration queue reset clears ctr[0..7] only).
+__global__ void wave_continue(cudaGraphConditionalHandle h, uint32_t* ctr, uint32_t cap, uint32_t* err,
+                              unsigned long long* tally, uint32_t kernels) {
+    uint32_t it = ctr[10] + 1u;
+    ctr[10] = it;
+    bool more = ctr[2] != 0u;
+    if (more && it >= cap) {
+        atomicOr(err, 8u);
+        more = false;
+    }
+    tally[0] += kernels;
+    tally[1] += 1ull;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+cudaError_t launch_wave_continue(cudaGraphConditionalHandle h, uint32_t* ctr, uint32_t cap, uint32_t* err,
+                                 unsigned long long* tally, uint32_t kernels, cudaStream_t st) {
+    wave_continue<<<1, 1, 0, st>>>(h, ctr, cap, err, tally, kernels);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
     return launch_trav(a, count, true, false, variant, stack, sms, st);
 }

@@ -78,6 +78,12 @@ cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int s
 // binary one; stack: 32 or 64 entries, enough for the tree walked.
 cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, bool four, int variant, int stack, int sms,
                                cudaStream_t st);
+// Graph-resident loop: after an iteration, sets the enclosing while node's
+// condition to "slots still active and fewer than `cap` iterations"; on
+// reaching the bound it sets bit 3 of *err instead. tally[0] += kernels
+// (the iteration's launches, this one included), tally[1] += 1.
+cudaError_t launch_wave_continue(cudaGraphConditionalHandle h, uint32_t* ctr, uint32_t cap, uint32_t* err,
+                                 unsigned long long* tally, uint32_t kernels, cudaStream_t st);
 // Split wavefront (wave_split.cu); shade variants 2 / 3 / 4 blocks per SM,
 // NEE variants 4 / 5 / 6.
 cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st);

@@ -34,10 +34,11 @@ class Plan:
     wave_slots: int = 1 << 20
     nee_variant: int = 0
     shadow_walk: int = 0
+    graphs: int = 0
 
     def key(self):
         return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant,
-                self.shadow_walk)
+                self.shadow_walk, self.graphs)
 
 
 SPACE = {
@@ -49,7 +50,7 @@ SPACE = {
     "nee_variant": [0, 1, 2],
     "shadow_walk": [0, 1],
 }
-WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk")
+WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk", "graphs")
 SPLIT_ONLY = ("nee_variant",)
 
 
@@ -86,7 +87,7 @@ def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] =
 def apply(tracer, plan: Plan):
     tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
                       stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant,
-                      shadow_walk=plan.shadow_walk)
+                      shadow_walk=plan.shadow_walk, graphs=plan.graphs)
 
 
 def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:
@@ -116,6 +117,47 @@ def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> 
     plan = coordinate_descent(measure, log=log)
     apply(tracer, plan)
     tracer.reset()
+    return plan
+
+
+def tune_batch(tracers, executor, spp: int = 1, log: Optional[list] = None,
+               space: Dict[str, List[int]] = None) -> Plan:
+    """Tune `executor`'s plan for batched refinement of `tracers` (already
+    synced): each candidate traces `spp` samples of every tracer at the
+    tuner's sample indices as one batch, timed with CUDA events on the
+    executor's stream; the tracers' accumulations are reset afterwards.
+    The megakernel is not a batch plan."""
+    L = N.lib()
+    ctx = executor.ctx
+    frames = (N.BatchFrame * len(tracers))()
+    for k, t in enumerate(tracers):
+        t.prepared()  # binds tables and params
+        w, h = t.size()
+        frames[k] = N.BatchFrame(t.ctx, TUNE_FIRST_SAMPLE, spp, 0, h)
+    space = space or {k: v for k, v in SPACE.items() if k != "mode"}
+    space = {"mode": [N.MODE_WAVEFRONT_SPLIT, N.MODE_WAVEFRONT], **space, "graphs": [0, 1]}
+
+    def measure(p: Plan) -> float:
+        apply(executor, p)
+        best = float("inf")
+        for r in range(2):
+            L.oxpt_diag_set_timing(ctx, 1)
+            L.oxpt_diag_timing(ctx, None, None, None, None)
+            t0 = time.perf_counter()
+            st = L.oxpt_refine_batch(ctx, frames, len(tracers))
+            if st != N.OK:
+                raise RuntimeError(L.oxpt_last_error(ctx).decode())
+            ms = C.c_double()
+            L.oxpt_diag_timing(ctx, C.byref(ms), None, None, None)
+            L.oxpt_diag_set_timing(ctx, 0)
+            if r > 0:
+                best = min(best, ms.value / 1e3 if ms.value > 0 else time.perf_counter() - t0)
+        return best
+
+    plan = coordinate_descent(measure, start=Plan(mode=N.MODE_WAVEFRONT_SPLIT), space=space, log=log)
+    apply(executor, plan)
+    for t in tracers:
+        t.reset()
     return plan
 
 

@@ -55,6 +55,8 @@ def _alone(pkg, cases, chunks):
     dict(mode=1, shadow_walk=1),
     dict(mode=2, wave_items=3000, wave_slots=700),   # many rounds, row bands, slot reuse across frames
     dict(mode=0),                                     # a megakernel executor runs the split wavefront
+    dict(mode=2, graphs=1),                           # one CUDA graph, device-side while loops
+    dict(mode=1, graphs=1, wave_items=3000, wave_slots=700),
 ])
 def test_batch_matches_each_scene_alone(pkg, plan):
     cases = _cases(pkg)
@@ -107,3 +109,27 @@ def test_batch_rejects_a_frame_without_a_scene(pkg):
         assert b"batch frame 1" in L.oxpt_last_error(t.ctx)
     finally:
         L.oxpt_destroy(bare)
+
+
+def test_graph_is_reused_while_the_step_shape_is_unchanged(pkg):
+    """Two refine steps of the same shape: one graph instantiation, and the
+    second step (new sample indices, read from device memory) still matches
+    each scene refined alone."""
+    import ctypes as C
+    cases = _cases(pkg)
+    want = _alone(pkg, cases, lambda c: [2, 2])
+    tracers = [_tracer(pkg, c) for c in cases]
+    ex = pkg.GpuPathTracer(0)
+    ex.set_tuning(mode=2, graphs=1, wave_items=4000)
+    L = pkg._native.lib()
+    for _ in range(2):
+        pkg.refine_batch(tracers, 2, executor=ex)
+    builds = C.c_uint64()
+    assert L.oxpt_diag_graph_builds(ex.ctx, C.byref(builds)) == 0
+    assert builds.value == 1
+    for k, (t, w) in enumerate(zip(tracers, want)):
+        assert np.array_equal(t.read_accum().view(np.uint32), w.view(np.uint32)), f"scene {k} differs"
+    launches, iters = C.c_uint64(), C.c_uint64()
+    L.oxpt_diag_launch_count(ex.ctx, C.byref(launches))
+    L.oxpt_diag_wave_iterations(ex.ctx, C.byref(iters))
+    assert iters.value > 0 and launches.value > 5 * iters.value
