@@ -111,6 +111,9 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *                  refine step: each round's wavefront loop is a device-side
  *                  while node (no host round trips), reused while the step's
  *                  shape is unchanged; 0 = host-driven loop.
+ *   refill         wavefront traversal: a warp gives its idle lanes new rays
+ *                  once this many of its 32 lanes are idle (1 = as soon as
+ *                  one is; 32 = when all are); 0 = library default (8).
  */
 enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1, OXPT_MODE_WAVEFRONT_SPLIT = 2 };
 typedef struct oxpt_tuning {
@@ -127,7 +130,7 @@ typedef struct oxpt_tuning {
     uint32_t nee_variant;
     uint32_t shadow_walk;
     uint32_t graphs;
-    uint32_t reserved;
+    uint32_t refill;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);

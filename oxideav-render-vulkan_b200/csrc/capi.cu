@@ -80,6 +80,7 @@ struct oxpt_ctx {
     bool bvh4_built = false;
     uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
     uint32_t shadow_walk = 0;
+    uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
     void* wave_mem = nullptr;
     size_t wave_bytes = 0;
     uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
@@ -298,6 +299,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     wa.slots = P;
     wa.vcap = P;
     wa.jobs = J;
+    wa.refill = c->refill;
     wa.first = ta.first;
     wa.y0 = ta.y0;
     wa.npix = ta.npix;
@@ -862,6 +864,8 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
     if (t->shadow_walk > 1) return fail(c, OXPT_E_INVALID, "shadow_walk is 0 or 1");
     if (t->graphs > 1) return fail(c, OXPT_E_INVALID, "graphs is 0 or 1");
+    if (t->refill > 32) return fail(c, OXPT_E_INVALID, "refill is 0 (default) to 32");
+    c->refill = t->refill ? t->refill : 8u;
     c->shadow_walk = t->shadow_walk;
     c->graphs = t->graphs;
     c->shade_variant = t->shade_variant;
@@ -887,6 +891,7 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->stack = c->stack;
     t->shadow_walk = c->shadow_walk;
     t->graphs = c->graphs;
+    t->refill = c->refill;
     return OXPT_OK;
 }
 
@@ -1228,6 +1233,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.slots = (uint32_t)std::min<uint64_t>(total, e->wave_slots);
         wa.vcap = pmax;
         wa.jobs = J;
+        wa.refill = e->refill;
         wa.total = total;
         wa.out = e->out;
         wa.counters = nullptr;
@@ -1236,7 +1242,9 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.nframes = (uint32_t)rounds[k].size();
         off += rounds[k].size();
     }
-    const bool four = e->shadow_walk == 0;
+    bool four = e->shadow_walk == 0;
+    for (uint32_t k = 0; k < n; k++)
+        if (fr[k].count && fr[k].rows && !bvh4_usable(fr[k].ctx)) four = false;
     auto enqueue_reduces = [&](size_t k, cudaStream_t st) -> cudaError_t {
         for (const oxpt::BatchPiece& pc : rounds[k]) {
             oxpt_ctx* c = fr[pc.frame].ctx;

@@ -234,29 +234,61 @@ __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ 
     }
 }
 
+// Traversal kernels: persistent grids over the ray queues, one walk per
+// lane. A lane whose ray is finished takes the next queued ray (warp-
+// aggregated fetch from a queue head) while the other lanes of its warp
+// keep walking, once at least `a.refill` lanes of the warp are idle (1:
+// at once; 32: only when the whole warp is idle), so warps are not held
+// by their longest ray (Aila & Laine 2009, "Understanding the efficiency
+// of ray traversal on GPUs": persistent threads, replacing terminated
+// rays). Each walk performs the same steps as a single-ray loop.
+constexpr unsigned FULL_WARP = 0xffffffffu;
+
 template <bool COUNT, int MINB, int SD, bool BATCH>
 __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
     const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        uint32_t i = a.q.ext[q];
-        float4 o = a.st.org[i], d = a.st.dir[i];
-        uint4 sd = a.st.seed[i];
-        Sampler smp{sd.x, sd.y, sd.z};
-        uint32_t k = sd.w;
-        Hit h;
-        uint32_t m = 0u;
-        bump<COUNT>(cnt, C_PATH_RAYS);
-        bool got = traverse<COUNT, SD>(scene_of<BATCH>(a, i), make_ray(xyz(o), xyz(d)), INF, smp, k << 16u, k == 0u,
-                                       false, NONE, &h, &m, cnt, a.err);
-        if (got) {
-            f3 b = h.b;
-            a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(b.y), __float_as_uint(b.z));
-            a.st.hmeta[i] = m | (h.front ? 0x80000000u : 0u);
-        } else {
-            a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+    bool active = false, drained = false;
+    uint32_t i = 0u, k = 0u;
+    const Scene* sc = &a.s;
+    Ray r;
+    Sampler smp{0u, 0u, 0u};
+    Walk2<SD> w;
+    for (;;) {
+        const bool idle = !active && !drained;
+        const unsigned idle_mask = __ballot_sync(FULL_WARP, idle);
+        const unsigned act_mask = __ballot_sync(FULL_WARP, active);
+        if (idle_mask == 0u && act_mask == 0u) break;
+        if (idle_mask != 0u && (act_mask == 0u || __popc(idle_mask) >= a.refill)) {
+            if (idle) {
+                uint32_t q = append(&a.ctr[5]);
+                if (q < n) {
+                    i = a.q.ext[q];
+                    sc = BATCH ? &a.frames[a.st.frame[i]].s : &a.s;
+                    float4 o = a.st.org[i], d = a.st.dir[i];
+                    uint4 sd = a.st.seed[i];
+                    smp = Sampler{sd.x, sd.y, sd.z};
+                    k = sd.w;
+                    bump<COUNT>(cnt, C_PATH_RAYS);
+                    r = make_ray(xyz(o), xyz(d));
+                    if (walk2_begin<COUNT, SD>(*sc, r, INF, w, cnt)) active = true;
+                    else a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+                } else {
+                    drained = true;
+                }
+            }
+        }
+        if (active && walk2_step<COUNT, SD>(*sc, r, smp, k << 16u, k == 0u, false, NONE, w, cnt, a.err)) {
+            active = false;
+            if (w.hit_any) {
+                const Hit& h = w.best;
+                a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(h.b.y), __float_as_uint(h.b.z));
+                a.st.hmeta[i] = w.best_mat | (h.front ? 0x80000000u : 0u);
+            } else {
+                a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+            }
         }
     }
     if (COUNT)
@@ -264,28 +296,67 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const
             if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
 }
 
-// FOUR: walk the four-wide tree (same occlusion as the binary walk); in a
-// batched launch only for the scenes that have one.
+// FOUR: walk the four-wide tree (same occlusion as the binary walk); a
+// batched launch uses it only when every frame's scene has one.
+template <int SD, bool FOUR>
+struct ShadowWalk {
+    Walk2<SD> w;
+};
+template <int SD>
+struct ShadowWalk<SD, true> {
+    Walk4<SD> w;
+};
+
 template <bool COUNT, int MINB, int SD, bool FOUR, bool BATCH>
 __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const __grid_constant__ WaveArgs a) {
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
     const uint32_t n = *((volatile uint32_t*)&a.ctr[1]);
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
-        uint4 m = a.q.sh_m[q];
-        const Scene& s = scene_of<BATCH>(a, m.x);
-        Sampler smp{0u, 0u, m.w};
-        Hit h;
-        uint32_t mat = 0u;
-        bump<COUNT>(cnt, C_SHADOW_RAYS);
-        Ray r = make_ray(xyz(o), xyz(d));
-        bool got = (FOUR && (!BATCH || s.bvh4_ok))
-                       ? occluded4<COUNT, SD>(s, r, o.w, smp, m.z, false, __float_as_uint(d.w), &h, &mat, cnt, a.err)
-                       : traverse<COUNT, SD>(s, r, o.w, smp, m.z, false, true, __float_as_uint(d.w), &h, &mat, cnt,
-                                             a.err);
-        if (!got) a.st.pend[(uint64_t)m.x * a.jobs + m.y].w = 2.0f;
+    bool active = false, drained = false;
+    uint32_t slot = 0u, job = 0u, rid = 0u, skip = NONE;
+    const Scene* sc = &a.s;
+    Ray r;
+    Sampler smp{0u, 0u, 0u};
+    ShadowWalk<SD, FOUR> sw;
+    for (;;) {
+        const bool idle = !active && !drained;
+        const unsigned idle_mask = __ballot_sync(FULL_WARP, idle);
+        const unsigned act_mask = __ballot_sync(FULL_WARP, active);
+        if (idle_mask == 0u && act_mask == 0u) break;
+        if (idle_mask != 0u && (act_mask == 0u || __popc(idle_mask) >= a.refill)) {
+            if (idle) {
+                uint32_t q = append(&a.ctr[6]);
+                if (q < n) {
+                    float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
+                    uint4 m = a.q.sh_m[q];
+                    slot = m.x;
+                    job = m.y;
+                    rid = m.z;
+                    skip = __float_as_uint(d.w);
+                    smp = Sampler{0u, 0u, m.w};
+                    sc = BATCH ? &a.frames[a.st.frame[slot]].s : &a.s;
+                    bump<COUNT>(cnt, C_SHADOW_RAYS);
+                    r = make_ray(xyz(o), xyz(d));
+                    bool started;
+                    if constexpr (FOUR) started = walk4_begin<SD>(*sc, r, o.w, sw.w);
+                    else started = walk2_begin<COUNT, SD>(*sc, r, o.w, sw.w, cnt);
+                    if (started) active = true;
+                    else a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;  // nothing in the way
+                } else {
+                    drained = true;
+                }
+            }
+        }
+        if (active) {
+            bool done;
+            if constexpr (FOUR) done = walk4_step<COUNT, SD>(*sc, r, smp, rid, false, skip, sw.w, cnt, a.err);
+            else done = walk2_step<COUNT, SD>(*sc, r, smp, rid, false, true, skip, sw.w, cnt, a.err);
+            if (done) {
+                active = false;
+                if (!sw.w.hit_any) a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;
+            }
+        }
     }
     if (COUNT)
         for (int c = 0; c < C_N; c++)

@@ -58,7 +58,9 @@ struct WaveArgs {
     unsigned long long total;   // items of this launch (npix x samples)
     unsigned long long* work;   // next item
     uint32_t* ctr;              // [0] continuation rays, [1] shadow rays, [2] active slots,
-                                // [3] hits to shade, [4] vertex records
+                                // [3] hits to shade, [4] vertex records, [5] / [6] next
+                                // continuation / shadow ray to walk
+    uint32_t refill;            // traversal: idle lanes of a warp that take new rays
     float4* out;
     unsigned long long* counters;
     uint32_t* err;

@@ -35,10 +35,11 @@ class Plan:
     nee_variant: int = 0
     shadow_walk: int = 0
     graphs: int = 0
+    refill: int = 8
 
     def key(self):
         return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant,
-                self.shadow_walk, self.graphs)
+                self.shadow_walk, self.graphs, self.refill)
 
 
 SPACE = {
@@ -49,8 +50,10 @@ SPACE = {
     "wave_slots": [1 << 19, 1 << 20, 1 << 21],
     "nee_variant": [0, 1, 2],
     "shadow_walk": [0, 1],
+    "refill": [1, 8, 16, 32],
 }
-WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk", "graphs")
+WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk", "graphs",
+             "refill")
 SPLIT_ONLY = ("nee_variant",)
 
 
@@ -87,7 +90,7 @@ def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] =
 def apply(tracer, plan: Plan):
     tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
                       stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant,
-                      shadow_walk=plan.shadow_walk, graphs=plan.graphs)
+                      shadow_walk=plan.shadow_walk, graphs=plan.graphs, refill=plan.refill)
 
 
 def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:

@@ -205,11 +205,12 @@ def test_images_vs_libm_oracle_psnr_at_least_60db(pkg, oracle):
     assert psnr >= 60.0, psnr
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode,refill", [(0, 0), (1, 8), (2, 8), (1, 1), (2, 32), (2, 16)])
 @pytest.mark.parametrize("which", ["materials", "layered", "alpha"])
-def test_both_execution_modes_bit_exact(pkg, oracle, mode, which):
+def test_both_execution_modes_bit_exact(pkg, oracle, mode, refill, which):
     """Megakernel and wavefront plans give the oracle's accumulator, also
-    with few wavefront slots (path regeneration) and split launches."""
+    with few wavefront slots (path regeneration), split launches and every
+    traversal refill policy (lanes taking new rays while others walk)."""
     if which == "materials":
         scene, env = scenes.materials_scene(pkg), None
     elif which == "alpha":
@@ -219,7 +220,7 @@ def test_both_execution_modes_bit_exact(pkg, oracle, mode, which):
                                     n_emissive=16, material_mix=1)
         env = pkg.EnvironmentMap.sky(64, 32)
     t = _tracer(pkg, scene, _opts(pkg, 40, 28, 6, bounces=10), env)
-    t.set_tuning(mode=mode, wave_slots=333, wave_items=2000, max_paths=2000, check_every=3)
+    t.set_tuning(mode=mode, wave_slots=333, wave_items=2000, max_paths=2000, check_every=3, refill=refill)
     t.refine(6)
     gpu = t.read_accum()
     cpu, _ = oracle.render(t.prepared(), 6)
