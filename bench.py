@@ -348,7 +348,7 @@ def main():
         pt.set_tuning(**kw)
     elif not a.no_tune:
         from oxideav_render_vulkan_b200 import tuner
-        tuner.tune(pt, spp=1, repeats=1, log=tune_log)
+        tuner.tune(pt, spp=min(a.spp, 4), repeats=1, log=tune_log)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):
@@ -484,7 +484,8 @@ def plan_of(pt):
     t = pt.tuning()
     return {"mode": ["megakernel", "wavefront", "wavefront-split"][t.mode], "wave_slots": t.wave_slots,
             "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack,
-            "nee_variant": t.nee_variant, "shadow_walk": ["four-wide", "binary"][t.shadow_walk]}
+            "nee_variant": t.nee_variant, "shadow_walk": ["four-wide", "binary"][t.shadow_walk],
+            "refill": t.refill}
 
 
 def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank):

@@ -241,8 +241,10 @@ __global__ void __launch_bounds__(128, MINB) wave_logic(const __grid_constant__ 
 // at once; 32: only when the whole warp is idle), so warps are not held
 // by their longest ray (Aila & Laine 2009, "Understanding the efficiency
 // of ray traversal on GPUs": persistent threads, replacing terminated
-// rays). Each walk performs the same steps as a single-ray loop.
+// rays). The warp checks for idle lanes every STEPS walk steps. Each walk
+// performs the same steps as a single-ray loop.
 constexpr unsigned FULL_WARP = 0xffffffffu;
+constexpr int STEPS = 4;
 
 template <bool COUNT, int MINB, int SD, bool BATCH>
 __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const __grid_constant__ WaveArgs a) {
@@ -250,19 +252,18 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
     const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
-    bool active = false, drained = false;
+    bool active = false, warp_drained = false;
     uint32_t i = 0u, k = 0u;
     const Scene* sc = &a.s;
     Ray r;
     Sampler smp{0u, 0u, 0u};
     Walk2<SD> w;
     for (;;) {
-        const bool idle = !active && !drained;
-        const unsigned idle_mask = __ballot_sync(FULL_WARP, idle);
-        const unsigned act_mask = __ballot_sync(FULL_WARP, active);
-        if (idle_mask == 0u && act_mask == 0u) break;
-        if (idle_mask != 0u && (act_mask == 0u || __popc(idle_mask) >= a.refill)) {
-            if (idle) {
+        const unsigned act = __ballot_sync(FULL_WARP, active);
+        if (act == 0u && warp_drained) break;
+        if (!warp_drained && 32 - __popc(act) >= (act ? a.refill : 1u)) {
+            bool none_left = false;
+            if (!active) {
                 uint32_t q = append(&a.ctr[5]);
                 if (q < n) {
                     i = a.q.ext[q];
@@ -276,18 +277,23 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_extend(const
                     if (walk2_begin<COUNT, SD>(*sc, r, INF, w, cnt)) active = true;
                     else a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
                 } else {
-                    drained = true;
+                    none_left = true;
                 }
             }
+            warp_drained = __any_sync(FULL_WARP, none_left);
         }
-        if (active && walk2_step<COUNT, SD>(*sc, r, smp, k << 16u, k == 0u, false, NONE, w, cnt, a.err)) {
-            active = false;
-            if (w.hit_any) {
-                const Hit& h = w.best;
-                a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(h.b.y), __float_as_uint(h.b.z));
-                a.st.hmeta[i] = w.best_mat | (h.front ? 0x80000000u : 0u);
-            } else {
-                a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+#pragma unroll 1
+        for (int st = 0; st < STEPS && active; st++) {
+            if (walk2_step<COUNT, SD>(*sc, r, smp, k << 16u, k == 0u, false, NONE, w, cnt, a.err)) {
+                active = false;
+                if (w.hit_any) {
+                    const Hit& h = w.best;
+                    a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(h.b.y),
+                                             __float_as_uint(h.b.z));
+                    a.st.hmeta[i] = w.best_mat | (h.front ? 0x80000000u : 0u);
+                } else {
+                    a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+                }
             }
         }
     }
@@ -313,19 +319,18 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
     const uint32_t n = *((volatile uint32_t*)&a.ctr[1]);
-    bool active = false, drained = false;
+    bool active = false, warp_drained = false;
     uint32_t slot = 0u, job = 0u, rid = 0u, skip = NONE;
     const Scene* sc = &a.s;
     Ray r;
     Sampler smp{0u, 0u, 0u};
     ShadowWalk<SD, FOUR> sw;
     for (;;) {
-        const bool idle = !active && !drained;
-        const unsigned idle_mask = __ballot_sync(FULL_WARP, idle);
-        const unsigned act_mask = __ballot_sync(FULL_WARP, active);
-        if (idle_mask == 0u && act_mask == 0u) break;
-        if (idle_mask != 0u && (act_mask == 0u || __popc(idle_mask) >= a.refill)) {
-            if (idle) {
+        const unsigned act = __ballot_sync(FULL_WARP, active);
+        if (act == 0u && warp_drained) break;
+        if (!warp_drained && 32 - __popc(act) >= (act ? a.refill : 1u)) {
+            bool none_left = false;
+            if (!active) {
                 uint32_t q = append(&a.ctr[6]);
                 if (q < n) {
                     float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
@@ -344,11 +349,13 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
                     if (started) active = true;
                     else a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;  // nothing in the way
                 } else {
-                    drained = true;
+                    none_left = true;
                 }
             }
+            warp_drained = __any_sync(FULL_WARP, none_left);
         }
-        if (active) {
+#pragma unroll 1
+        for (int st = 0; st < STEPS && active; st++) {
             bool done;
             if constexpr (FOUR) done = walk4_step<COUNT, SD>(*sc, r, smp, rid, false, skip, sw.w, cnt, a.err);
             else done = walk2_step<COUNT, SD>(*sc, r, smp, rid, false, true, skip, sw.w, cnt, a.err);
