@@ -69,8 +69,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
                     help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch"],
-                    help="single: the large scene (headline); batch: 64 mixed scenes in batched launches")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell"],
+                    help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
+                         "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
     ap.add_argument("--scenes", type=int, default=64, help="batch workload: number of scenes")
     return ap.parse_args()
 
@@ -306,8 +307,61 @@ def run_batch(a):
     print(json.dumps(line), flush=True)
 
 
+def run_cornell(a):
+    """The reference's pt_bench shape: procedural Cornell box, 256x256,
+    8 bounces, roulette from bounce 3, seed 0, `--spp` samples (64 by
+    default); refine alone and refine + image() readback."""
+    import torch
+    torch.cuda.set_device(0)
+    __graft_entry__.build()
+    pkg = __graft_entry__.load_package()
+    from oxideav_render_vulkan_b200 import tuner
+    spp = a.spp
+    pt = pkg.GpuPathTracer(0)
+    opts = pkg.RenderOptions(width=256, height=256,
+                             path_trace=pkg.PathTraceOptions(samples_per_pixel=spp, max_bounces=8, rr_start=3,
+                                                             seed=0))
+    pt.sync(pkg.Scene.cornell(), opts)
+    pt.prepared()
+    tune_log = []
+    plan = None
+    if not a.no_tune:
+        plan = tuner.tune(pt, spp=min(spp, 16), repeats=1, log=tune_log)
+
+    def measure(with_image):
+        ms = []
+        for i in range(a.warmup + a.steps):
+            pt.reset()
+            pt.finish()
+            t0 = time.perf_counter()
+            pt.refine(spp)
+            if with_image:
+                pt.image()
+            pt.finish()
+            if i >= a.warmup:
+                ms.append(1e3 * (time.perf_counter() - t0))
+        return statistics.median(ms)
+
+    refine_ms = measure(False)
+    render_ms = measure(True)
+    paths = 256 * 256 * spp
+    line = {"metric": "Msamples/s", "value": paths / refine_ms / 1e3, "unit": "Msamples/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": refine_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "procedural Cornell box (36 triangles), 256x256, 8 bounces, roulette from 3, "
+                                   f"seed 0, {spp} spp", "timing": "host wall clock, median, refine + finish"},
+            "render_ms": render_ms, "refine_ms": refine_ms,
+            "reference_rtx5080_context": {"refine_ms_64spp": 31.8, "render_ms_64spp": 32.2,
+                                          "note": "published on RTX 5080 through Vulkan; cross-hardware context only"},
+            "plan": plan_of(pt), "tuner_trials": len(tune_log)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
+    if a.workload == "cornell":
+        run_cornell(a)
+        return
     if a.impl == "reference":
         run_reference(a)
         return

@@ -404,6 +404,11 @@ oxpt_status wave_loop(oxpt_ctx* c, const oxd::WaveArgs& wa, bool count, bool fou
 oxpt_status run_frame(oxpt_ctx* c, const oxpt_frame& f, bool count) {
     if (f.count == 0 || f.rows == 0) return OXPT_OK;
     if (f.y0 >= c->h || f.rows > c->h - f.y0) return fail(c, OXPT_E_INVALID, "frame rows outside the image");
+    if (c->graphs && !count && c->mode != OXPT_MODE_MEGAKERNEL) {
+        // Graph plan: the frame as a batch of one, one CUDA graph per step.
+        oxpt_batch_frame bf{c, f.first, f.count, f.y0, f.rows};
+        return oxpt_refine_batch(c, &bf, 1);
+    }
     bool wave = c->mode != OXPT_MODE_MEGAKERNEL;
     uint64_t cap = std::max<uint64_t>(wave ? c->wave_items : c->max_paths, c->w);
     uint32_t rows_per = f.rows, per = f.count;
@@ -1163,6 +1168,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         if (o0 + 128 > c->table_words || o1 + 512 > c->table_words)
             return fail(e, OXPT_E_INVALID, at + "tables too short for the Sobol' and sheen words");
         if (c->stream != e->stream) CK(e, cudaStreamSynchronize(c->stream), "frame context sync");
+        if (n == 1) continue;  // a single frame stages its own tables
         CK(e, cudaMemcpy(tab.data(), c->tables + o0, 128 * 4, cudaMemcpyDeviceToHost), "table check");
         CK(e, cudaMemcpy(tab.data() + 128, c->tables + o1, 512 * 4, cudaMemcpyDeviceToHost), "table check");
         if (ref_tables.empty()) ref_tables = tab;

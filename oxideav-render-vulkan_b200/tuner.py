@@ -51,6 +51,7 @@ SPACE = {
     "nee_variant": [0, 1, 2],
     "shadow_walk": [0, 1],
     "refill": [1, 8, 16, 32],
+    "graphs": [0, 1],
 }
 WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk", "graphs",
              "refill")
@@ -138,7 +139,7 @@ def tune_batch(tracers, executor, spp: int = 1, log: Optional[list] = None,
         w, h = t.size()
         frames[k] = N.BatchFrame(t.ctx, TUNE_FIRST_SAMPLE, spp, 0, h)
     space = space or {k: v for k, v in SPACE.items() if k != "mode"}
-    space = {"mode": [N.MODE_WAVEFRONT_SPLIT, N.MODE_WAVEFRONT], **space, "graphs": [0, 1]}
+    space = {"mode": [N.MODE_WAVEFRONT_SPLIT, N.MODE_WAVEFRONT], **space}
 
     def measure(p: Plan) -> float:
         apply(executor, p)

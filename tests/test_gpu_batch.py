@@ -133,3 +133,16 @@ def test_graph_is_reused_while_the_step_shape_is_unchanged(pkg):
     L.oxpt_diag_launch_count(ex.ctx, C.byref(launches))
     L.oxpt_diag_wave_iterations(ex.ctx, C.byref(iters))
     assert iters.value > 0 and launches.value > 5 * iters.value
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_single_tracer_graph_plan_matches_the_oracle(pkg, oracle, mode):
+    """With graphs on, a tracer's own refine runs as a one-frame batch in a
+    CUDA graph; refine(2) + refine(3) equals the oracle's 5 samples."""
+    c = _cases(pkg)[1]
+    t = _tracer(pkg, c)
+    t.set_tuning(mode=mode, graphs=1, wave_slots=500)
+    t.refine(2)
+    t.refine(3)
+    cpu, _ = oracle.render(t.prepared(), 5)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
