@@ -470,6 +470,22 @@ def main():
     peak, peak_kind = measured_peak()
     kms, kn = (C.c_double * 8)(), (C.c_uint64 * 8)()
     L.oxpt_diag_timing_kinds(pt.ctx, kms, kn)
+    kernel_timing = "timed region"
+    if pt.tuning().graphs:
+        # A graph step records no per-kernel events: time the same kernels
+        # over the same number of frames with the graph off (untimed for
+        # `value`), one event pair per launch.
+        pt.set_tuning(graphs=0)
+        L.oxpt_diag_set_timing(pt.ctx, 1)
+        L.oxpt_diag_timing(pt.ctx, None, None, None, None)
+        for _ in range(a.steps):
+            step()
+        pt.finish()
+        L.oxpt_diag_timing(pt.ctx, None, None, None, None)
+        L.oxpt_diag_set_timing(pt.ctx, 0)
+        L.oxpt_diag_timing_kinds(pt.ctx, kms, kn)
+        pt.set_tuning(graphs=1)
+        kernel_timing = "same frames re-run without the graph (per-launch CUDA events)"
     paths_timed = paths_step * a.steps
     mode = pt.tuning().mode
     kinds = {0: ((0, "trace_paths"),), 1: ((2, "wave_logic"), (3, "wave_extend"), (4, "wave_shadow")),
@@ -524,7 +540,8 @@ def main():
                              "algorithmic_bytes_per_launch": kd["algorithmic_bytes_per_launch"],
                              "launch_ms": kd["launch_ms"], "launches": kd["launches"],
                              "algorithmic_bytes_per_path": bytes_per_path, "kernels": kernels,
-                             "trace_phase_ms": tms.value, "reduce_ms_total": rms.value},
+                             "trace_phase_ms": tms.value, "reduce_ms_total": rms.value,
+                             "kernel_timing": kernel_timing},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(n1.value - n0.value),
                 "clocks": clk.summary(), "rays_per_path": rays_per_path,
                 "plan": plan_of(pt), "tuner_trials": len(tune_log)}
@@ -539,7 +556,7 @@ def plan_of(pt):
     return {"mode": ["megakernel", "wavefront", "wavefront-split"][t.mode], "wave_slots": t.wave_slots,
             "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack,
             "nee_variant": t.nee_variant, "shadow_walk": ["four-wide", "binary"][t.shadow_walk],
-            "refill": t.refill}
+            "refill": t.refill, "graphs": t.graphs}
 
 
 def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank):
