@@ -147,6 +147,16 @@ oxpt_status oxpt_device_summary(const oxpt_ctx* ctx, char* buf, size_t len);
  * tables with the environment words appended. */
 oxpt_status oxpt_upload_scene(oxpt_ctx* ctx, const oxpt_scene_desc* scene);
 oxpt_status oxpt_set_tables(oxpt_ctx* ctx, const uint32_t* words, size_t count);
+/*
+ * Borrow another context's device scene (geometry, attributes, atlas,
+ * four-wide tree) or tables instead of uploading copies: contexts that
+ * render the same scene from different cameras, resolutions or sample
+ * counts (serving sessions) keep one resident copy. The lending context
+ * must outlive the borrower; a later upload / set_tables on the borrower
+ * replaces the borrowed buffers with its own. No reference counterpart.
+ */
+oxpt_status oxpt_share_scene(oxpt_ctx* ctx, const oxpt_ctx* owner);
+oxpt_status oxpt_share_tables(oxpt_ctx* ctx, const oxpt_ctx* owner);
 oxpt_status oxpt_set_params(oxpt_ctx* ctx, const oxpt_params* params);
 
 /* ---- accumulation (sync's accumulator, :551-564; reset, :495-502) */

@@ -1,4 +1,4 @@
-"""ctypes bindings of liboxpt.so (include/oxpt.h, oxpt_batch.h, oxpt_host.h, oxpt_diag.h).
+"""ctypes bindings of liboxpt.so (include/oxpt.h, oxpt_batch.h, oxpt_serve.h, oxpt_host.h, oxpt_diag.h).
 
 The library is built in-tree by ``build.py``. Loading fails loudly when it
 is missing: there is no CPU fallback on this path.
@@ -124,6 +124,8 @@ _SIGS = {
     "oxpt_device_summary": (cint, [vp, C.c_char_p, sz]),
     "oxpt_upload_scene": (cint, [vp, C.POINTER(SceneDesc)]),
     "oxpt_set_tables": (cint, [vp, vp, sz]),
+    "oxpt_share_scene": (cint, [vp, vp]),
+    "oxpt_share_tables": (cint, [vp, vp]),
     "oxpt_set_params": (cint, [vp, C.POINTER(Params)]),
     "oxpt_resize": (cint, [vp, u32, u32]),
     "oxpt_reset": (cint, [vp]),
@@ -154,6 +156,12 @@ _SIGS = {
     "oxpt_diag_timing_kinds": (cint, [vp, vp, vp]),
     "oxpt_diag_counters_split": (cint, [vp, vp]),
     "oxpt_diag_timing": (cint, [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(u64)]),
+    # oxpt_serve.h
+    "oxpt_ctx_device": (cint, [vp]),
+    "oxpt_ctx_memory": (cint, [vp, C.POINTER(u64 * 4)]),
+    "oxpt_tracer_new_view": (cint, [vp, C.POINTER(vp)]),
+    "oxpt_tracer_view_sync": (cint, [vp, C.POINTER(RenderOptions), C.POINTER(cint)]),
+    "oxpt_tracer_set_camera": (cint, [vp, C.c_void_p]),
     # oxpt_host.h
     "oxpt_material_default": (None, [C.POINTER(Material)]),
     "oxpt_scene_new": (vp, []),

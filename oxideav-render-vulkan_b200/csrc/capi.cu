@@ -19,6 +19,7 @@
 #include "../../include/oxpt.h"
 #include "../../include/oxpt_batch.h"
 #include "../../include/oxpt_diag.h"
+#include "../../include/oxpt_serve.h"
 #include "kernels.cuh"
 #include "wavefront.cuh"
 #include "../host/batch.hpp"
@@ -40,6 +41,8 @@ struct oxpt_ctx {
     uint32_t node_count = 0;
     uint32_t* tables = nullptr;
     size_t table_words = 0;
+    // scene buffers / tables borrowed from another context (oxpt_share_*)
+    bool borrowed_scene = false, borrowed_tables = false;
     oxpt_params params{};
     bool has_scene = false, has_tables = false, has_params = false;
     // accumulation + outputs
@@ -139,6 +142,17 @@ oxpt_status realloc_dev(oxpt_ctx* c, T** p, size_t bytes, const char* what) {
 // overflows its 64-entry stack (at most 64 levels).
 bool bvh4_usable(const oxpt_ctx* c) {
     return c->bvh4_built && c->params.env[3] == c->node_count && c->bvh_depth <= 64 && c->bvh4_need <= 64;
+}
+
+// A borrowed scene is not freed here: the lending context owns it.
+void drop_borrowed_scene(oxpt_ctx* c) {
+    if (!c->borrowed_scene) return;
+    c->geom = nullptr;
+    c->attrs = nullptr;
+    c->atlas = nullptr;
+    c->bvh4 = nullptr;
+    c->borrowed_scene = false;
+    c->bvh4_built = false;
 }
 
 oxd::Scene scene_view(const oxpt_ctx* c) {
@@ -512,6 +526,8 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
     }
+    drop_borrowed_scene(c);
+    if (c->borrowed_tables) c->tables = nullptr;
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
                     c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev};
     if (c->batch_done) cudaEventDestroy(c->batch_done);
@@ -579,6 +595,7 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     if (s) return s;
     CK(c, cudaStreamSynchronize(c->stream), "sync before upload");
     c->has_scene = false;
+    drop_borrowed_scene(c);
     size_t gbytes = d->geom_words * 4, abytes = d->attr_floats * 4;
     size_t tbytes = (size_t)d->atlas_side * d->atlas_side * d->atlas_layers * 8;
     if ((s = realloc_dev(c, &c->geom, gbytes, "geom buffer"))) return s;
@@ -606,10 +623,63 @@ oxpt_status oxpt_set_tables(oxpt_ctx* c, const uint32_t* words, size_t count) {
     if (s) return s;
     CK(c, cudaStreamSynchronize(c->stream), "sync before tables");
     c->has_tables = false;
+    if (c->borrowed_tables) {
+        c->tables = nullptr;
+        c->borrowed_tables = false;
+    }
     if ((s = realloc_dev(c, &c->tables, count * 4, "tables"))) return s;
     CK(c, cudaMemcpyAsync(c->tables, words, count * 4, cudaMemcpyHostToDevice, c->stream), "tables upload");
     CK(c, cudaStreamSynchronize(c->stream), "tables upload");
     c->table_words = count;
+    c->has_tables = true;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_share_scene(oxpt_ctx* c, const oxpt_ctx* owner) {
+    if (!c || !owner || c == owner) return fail(c, OXPT_E_INVALID, "sharing needs two contexts");
+    if (!owner->has_scene) return fail(c, OXPT_E_INVALID, "the lending context has no scene");
+    if (owner->device != c->device) return fail(c, OXPT_E_INVALID, "the lending context is on another device");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before sharing");
+    CK(c, cudaStreamSynchronize(owner->stream), "sync before sharing");
+    drop_borrowed_scene(c);
+    void* own[] = {c->geom, c->attrs, c->atlas, c->bvh4};
+    for (void* p : own)
+        if (p) cudaFree(p);
+    c->geom = owner->geom;
+    c->geom_vec4 = owner->geom_vec4;
+    c->attrs = owner->attrs;
+    c->slot_count = owner->slot_count;
+    c->atlas = owner->atlas;
+    c->side = owner->side;
+    c->layers = owner->layers;
+    c->node_count = owner->node_count;
+    c->bvh_depth = owner->bvh_depth;
+    c->bvh4 = owner->bvh4;
+    c->bvh4_built = owner->bvh4_built;
+    c->bvh4_nodes = owner->bvh4_nodes;
+    c->bvh4_root = owner->bvh4_root;
+    c->bvh4_need = owner->bvh4_need;
+    c->borrowed_scene = true;
+    c->has_scene = true;
+    if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_share_tables(oxpt_ctx* c, const oxpt_ctx* owner) {
+    if (!c || !owner || c == owner) return fail(c, OXPT_E_INVALID, "sharing needs two contexts");
+    if (!owner->has_tables) return fail(c, OXPT_E_INVALID, "the lending context has no tables");
+    if (owner->device != c->device) return fail(c, OXPT_E_INVALID, "the lending context is on another device");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before sharing");
+    CK(c, cudaStreamSynchronize(owner->stream), "sync before sharing");
+    if (c->borrowed_tables) c->tables = nullptr;
+    else if (c->tables) cudaFree(c->tables);
+    c->tables = owner->tables;
+    c->table_words = owner->table_words;
+    c->borrowed_tables = true;
     c->has_tables = true;
     return OXPT_OK;
 }
@@ -911,6 +981,23 @@ static void read_tally(const oxpt_ctx* c, uint64_t out[2]) {
         out[0] = v[0];
         out[1] = v[1];
     }
+}
+
+int oxpt_ctx_device(const oxpt_ctx* c) { return c ? c->device : -1; }
+
+oxpt_status oxpt_ctx_memory(const oxpt_ctx* c, uint64_t out[4]) {
+    if (!c || !out) return OXPT_E_INVALID;
+    uint64_t scene = 0;
+    if (!c->borrowed_scene && c->has_scene) {
+        scene = (uint64_t)c->geom_vec4 * 16 + (uint64_t)c->slot_count * 192 +
+                (uint64_t)c->side * c->side * c->layers * 8 + (uint64_t)c->bvh4_nodes * 128;
+    }
+    out[0] = scene;
+    out[1] = c->borrowed_tables ? 0 : (uint64_t)c->table_words * 4;
+    uint64_t px = (uint64_t)c->w * c->h;
+    out[2] = c->accum ? px * 16 + (c->img8 ? px * 4 : 0) + (c->img32 ? px * 16 : 0) : 0;
+    out[3] = c->out_cap * 16 + c->wave_bytes + c->batch_cap * sizeof(oxd::BatchFrame);
+    return OXPT_OK;
 }
 
 oxpt_status oxpt_diag_graph_builds(const oxpt_ctx* c, uint64_t* out) {

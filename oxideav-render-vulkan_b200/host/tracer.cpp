@@ -11,6 +11,7 @@
 #include <string>
 
 #include "../../include/oxpt_batch.h"
+#include "../../include/oxpt_serve.h"
 #include "model.hpp"
 
 namespace {
@@ -54,7 +55,11 @@ struct oxpt_tracer {
     oxpt_render_options opts{};
     std::optional<float> prep;  // PrepareOptions: the headlight intensity
     bool dirty = true;
-    std::unique_ptr<oxpt::SceneBuffers> scene;
+    std::shared_ptr<oxpt::SceneBuffers> scene;
+    // A view shares `owner`'s prepared scene and device buffers and never
+    // prepares itself (serving sessions); `cam` overrides the camera.
+    const oxpt_tracer* owner = nullptr;
+    std::optional<oxpt_camera> cam;
     oxpt::Framing framing;
     std::optional<oxpt::Env> env;
     std::optional<oxpt::EnvWords> env_words;
@@ -101,10 +106,13 @@ struct oxpt_tracer {
         return OXPT_OK;
     }
 
-    oxpt_status sync(const oxpt_scene& s, const oxpt_render_options& o, bool* did_reset) {
+    // s may be null for a view (which never prepares).
+    oxpt_status sync(const oxpt_scene* s, const oxpt_render_options& o, bool* did_reset) {
         *did_reset = false;
         float p = o.light_intensity;
         bool need_prepare = dirty || !scene || !prep || *prep != p;
+        if ((owner || !s) && need_prepare)
+            return fail(OXPT_E_INVALID, "a view cannot prepare: its owner's scene and light intensity are fixed");
         bool changed = need_prepare || !(radiance_key(o) == radiance_key(opts));
         opts = o;
         if (!changed) return OXPT_OK;
@@ -113,12 +121,12 @@ struct oxpt_tracer {
             return fail(OXPT_E_INVALID, std::to_string(width) + "x" + std::to_string(height) +
                                             " exceeds the tracer's " + std::to_string(MAX_DIM) + " maximum side");
         if (need_prepare) {
-            oxpt_status st = upload(s, p);
+            oxpt_status st = upload(*s, p);
             if (st) return st;
             prep = p;
             dirty = false;
         }
-        camera = oxpt::resolve_camera(framing, o, width, height);
+        camera = resolve(o, width, height);
         if (w != width || h != height || !has_accum) {
             w = width;
             h = height;
@@ -133,11 +141,25 @@ struct oxpt_tracer {
         return OXPT_OK;
     }
 
+    oxpt::ResolvedCamera resolve(const oxpt_render_options& o, uint32_t width, uint32_t height) const {
+        if (!cam) return oxpt::resolve_camera(framing, o, width, height);
+        oxpt::Framing f = framing;
+        f.cameras = {*cam};
+        oxpt_render_options oc = o;
+        oc.scene_camera = 0;
+        return oxpt::resolve_camera(f, oc, width, height);
+    }
+
     oxpt_status ensure_binding() {
         if (binding) return OXPT_OK;
         if (env && !env_words) env_words = oxpt::env_words(*env);
         oxpt::bind_params(*scene, env ? &*env_words : nullptr, *camera, opts, w, h, &tables, &params);
-        oxpt_status st = check(oxpt_set_tables(ctx, tables.data(), tables.size()));
+        oxpt_status st;
+        if (owner && owner->binding && owner->tables == tables) {
+            st = check(oxpt_share_tables(ctx, owner->ctx));  // the owner's resident tables
+        } else {
+            st = check(oxpt_set_tables(ctx, tables.data(), tables.size()));
+        }
         if (st) return st;
         st = check(oxpt_set_params(ctx, &params));
         if (st) return st;
@@ -232,7 +254,7 @@ void oxpt_tracer_size(const oxpt_tracer* t, uint32_t* w, uint32_t* h) {
 oxpt_status oxpt_tracer_sync(oxpt_tracer* t, const oxpt_scene* scene, const oxpt_render_options* opts, int* did_reset) {
     if (!t || !scene || !opts) return OXPT_E_INVALID;
     bool r = false;
-    oxpt_status s = t->sync(*scene, *opts, &r);
+    oxpt_status s = t->sync(scene, *opts, &r);
     if (did_reset) *did_reset = r ? 1 : 0;
     return s;
 }
@@ -267,6 +289,48 @@ oxpt_status oxpt_tracers_refine_batch(oxpt_tracer* const* ts, uint32_t count, co
     }
     for (uint32_t k = 0; k < count; k++) ts[k]->samples += adds[k];
     return OXPT_OK;
+}
+
+oxpt_status oxpt_tracer_new_view(const oxpt_tracer* owner, oxpt_tracer** out) {
+    if (!owner || !out) return OXPT_E_INVALID;
+    *out = nullptr;
+    if (!owner->scene || owner->owner) return OXPT_E_INVALID;
+    oxpt_tracer* t = nullptr;
+    oxpt_status s = oxpt_tracer_new(oxpt_ctx_device(owner->ctx), &t);
+    if (s) return s;
+    s = oxpt_share_scene(t->ctx, owner->ctx);
+    if (s) {
+        oxpt_tracer_free(t);
+        return s;
+    }
+    t->owner = owner;
+    t->scene = owner->scene;
+    t->framing = owner->framing;
+    t->env = owner->env;
+    t->env_words = owner->env_words;
+    t->prep = owner->prep;
+    t->dirty = false;
+    *out = t;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_tracer_view_sync(oxpt_tracer* t, const oxpt_render_options* opts, int* did_reset) {
+    if (!t || !opts || !t->owner) return OXPT_E_INVALID;
+    bool r = false;
+    oxpt_status s = t->sync(nullptr, *opts, &r);
+    if (did_reset) *did_reset = r ? 1 : 0;
+    return s;
+}
+
+oxpt_status oxpt_tracer_set_camera(oxpt_tracer* t, const oxpt_camera* cam) {
+    if (!t) return OXPT_E_INVALID;
+    if (cam) t->cam = *cam;
+    else t->cam.reset();
+    if (!t->scene) return OXPT_OK;
+    uint32_t width = std::max(t->opts.width, 1u), height = std::max(t->opts.height, 1u);
+    t->camera = t->resolve(t->opts, width, height);
+    t->binding = false;
+    return t->reset();  // a camera move resets the accumulation, as sync does
 }
 
 oxpt_status oxpt_tracer_finish(oxpt_tracer* t) { return t->check(oxpt_finish(t->ctx)); }

@@ -317,6 +317,41 @@ class GpuPathTracer:
         if st != N.OK:
             _raise(st, N.lib().oxpt_last_error(self.ctx).decode())
 
+    def view(self) -> "GpuPathTracer":
+        """A session on this tracer's scene (oxpt_serve.h): its own camera,
+        resolution, options and accumulator, sharing the resident prepared
+        scene and device buffers. Sync it with sync_view()."""
+        h = C.c_void_p()
+        st = N.lib().oxpt_tracer_new_view(self._h, C.byref(h))
+        if st != N.OK:
+            _raise(st, "cannot make a view: the owner must be a synced tracer, not a view")
+        v = GpuPathTracer.__new__(GpuPathTracer)
+        v._h = h.value
+        v._env = self._env
+        v._owner = self  # the owner's device buffers must outlive the view
+        return v
+
+    def sync_view(self, opts: "RenderOptions") -> bool:
+        o = opts.to_c()
+        r = C.c_int()
+        self._check(N.lib().oxpt_tracer_view_sync(self._h, C.byref(o), C.byref(r)))
+        return bool(r.value)
+
+    def set_camera(self, eye=None, target=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), yfov=0.7853982,
+                   orthographic=False, ymag=1.0):
+        """Camera override (None: the options' camera); resets the accumulation."""
+        if eye is None:
+            self._check(N.lib().oxpt_tracer_set_camera(self._h, None))
+            return
+        cam = N.Camera((N.f32 * 3)(*eye), (N.f32 * 3)(*target), (N.f32 * 3)(*up), yfov, int(orthographic), ymag)
+        self._check(N.lib().oxpt_tracer_set_camera(self._h, C.cast(C.pointer(cam), C.c_void_p)))
+
+    def memory(self) -> dict:
+        """Device bytes held (oxpt_ctx_memory): scene, tables, images, working."""
+        out = (N.u64 * 4)()
+        N.lib().oxpt_ctx_memory(self.ctx, out)
+        return {"scene": int(out[0]), "tables": int(out[1]), "images": int(out[2]), "working": int(out[3])}
+
     def adapter_summary(self) -> str:
         buf = C.create_string_buffer(256)
         N.lib().oxpt_device_summary(self.ctx, buf, 256)
