@@ -69,7 +69,12 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
                     help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell"],
+    ap.add_argument("--requests", type=int, default=300, help="serve workload: requests in the stream")
+    ap.add_argument("--rate", type=float, default=40.0, help="serve workload: Poisson arrival rate per second")
+    ap.add_argument("--spp-scale", type=int, default=16,
+                    help="serve workload: spp targets {4..1024} divided by this (one GPU cannot keep up with the "
+                         "full stream)")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
     ap.add_argument("--scenes", type=int, default=64, help="batch workload: number of scenes")
@@ -357,8 +362,101 @@ def run_cornell(a):
     print(json.dumps(line), flush=True)
 
 
+SERVE_RES = [(128, 128), (256, 256), (512, 512), (1280, 720), (1920, 1080)]
+SERVE_SPP = [4, 16, 64, 256, 1024]
+
+
+def serve_stream(serve, a, n_scenes, seed=3):
+    """Poisson arrivals at `rate`; each new session picks a resident scene,
+    a resolution and an spp target (scaled by 1/spp_scale); 30% of requests
+    are camera moves on an already opened session."""
+    rng = np.random.default_rng(seed)
+    reqs, opened, t = [], [], 0.0
+    for rid in range(a.requests):
+        t += float(rng.exponential(1.0 / a.rate))
+        if opened and rng.random() < 0.3:
+            base = reqs[opened[int(rng.integers(len(opened)))]]
+            key = base.session if base.session is not None else base.rid
+            spp = max(1, SERVE_SPP[int(rng.integers(len(SERVE_SPP)))] // a.spp_scale)
+            ang = float(rng.uniform(-0.6, 0.6))
+            cam = ((2.6 * np.sin(ang), 0.4, 2.6 * np.cos(ang)), (0.0, 0.0, 0.0))
+            reqs.append(serve.Request(rid, t, base.scene, base.width, base.height, spp, cam, key))
+        else:
+            w, h = SERVE_RES[int(rng.integers(len(SERVE_RES)))]
+            spp = max(1, SERVE_SPP[int(rng.integers(len(SERVE_SPP)))] // a.spp_scale)
+            reqs.append(serve.Request(rid, t, int(rng.integers(n_scenes)), w, h, spp))
+            opened.append(rid)
+    return reqs
+
+
+def run_serve(a):
+    """The served stream: continuous batching against serial plain launches."""
+    import torch
+    torch.cuda.set_device(0)
+    __graft_entry__.build()
+    pkg = __graft_entry__.load_package()
+    from oxideav_render_vulkan_b200 import serve
+    rng = np.random.default_rng(5)
+    n_scenes = a.scenes
+    env = pkg.EnvironmentMap.sky(256, 128)
+    owners, tris = [], 0
+    for k in range(n_scenes):
+        t_k = float(np.exp(rng.uniform(np.log(1e3), np.log(2e6))))
+        if k % 2 == 0:
+            sc = pkg.Scene.icosphere(freq=max(8, int(round(np.sqrt(t_k / 20.0)))), seed=300 + k, n_materials=16,
+                                     n_textures=2, tex_size=256, n_punctual=4, n_emissive=16, material_mix=1)
+        else:
+            sc = pkg.Scene.box_field(max(1, int(t_k / 12)), seed=300 + k, material_mix=1)
+        tris += int(sc.triangle_count())
+        o = pkg.GpuPathTracer(0)
+        o.set_environment(env)
+        o.sync(sc, pkg.RenderOptions(width=64, height=64, scene_camera=0,
+                                     path_trace=pkg.PathTraceOptions(samples_per_pixel=1, max_bounces=8)))
+        o.refine(1)  # binds tables and params
+        o.finish()
+        owners.append(o)
+    reqs = serve_stream(serve, a, n_scenes)
+
+    def options(r):
+        return pkg.RenderOptions(width=r.width, height=r.height, scene_camera=0,
+                                 path_trace=pkg.PathTraceOptions(samples_per_pixel=r.spp, max_bounces=8))
+
+    check = set(int(x) for x in np.random.default_rng(9).choice(a.requests, size=4, replace=False))
+    ex = serve.GpuExecutor(pkg, owners, options, keep=lambda o: o.rid in check)
+    ex.exe.set_tuning(mode=2, graphs=1)
+    budget = 150 << 30
+    served = serve.Server(ex, budget, tick_paths=1 << 24).run(reqs)
+    ex2 = serve.GpuExecutor(pkg, owners, options)
+    serial = serve.run_serial(ex2, reqs)
+    by = {r.rid: r for r in reqs}
+    same = []
+    for rid, acc in ex.kept.items():
+        v = ex2.open(by[rid])
+        v.refine(by[rid].spp)
+        same.append(bool(np.array_equal(acc.view(np.uint32), v.read_accum().view(np.uint32))))
+    line = {"metric": "Msamples/s", "value": served.msamples_per_s(), "unit": "Msamples/s", "n_gpus": 1,
+            "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"served stream: {a.requests} requests, Poisson {a.rate}/s, {n_scenes} resident "
+                                   "scenes (1e3..2e6 triangles log-uniform), resolutions 128^2..1920x1080, spp "
+                                   f"targets {{4,16,64,256,1024}}/{a.spp_scale}, 30% camera moves, 150 GB budget",
+                       "triangles": tris},
+            "p50_latency_s": served.percentile(50), "p99_latency_s": served.percentile(99),
+            "completed": len(served.completed()), "superseded": sum(o.superseded for o in served.outcomes),
+            "ticks": served.ticks, "peak_device_bytes_accounted": served.peak_bytes,
+            "serial_plain": {"msamples_per_s": serial.msamples_per_s(), "p50_latency_s": serial.percentile(50),
+                             "p99_latency_s": serial.percentile(99), "completed": len(serial.completed()),
+                             "wall_s": serial.wall},
+            "served_wall_s": served.wall, "throughput_vs_serial": served.msamples_per_s() / serial.msamples_per_s(),
+            "same_alone_and_in_mix": same}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
+    if a.workload == "serve":
+        run_serve(a)
+        return
     if a.workload == "cornell":
         run_cornell(a)
         return
