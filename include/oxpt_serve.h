@@ -16,6 +16,14 @@ extern "C" {
 /* CUDA device of a context. */
 int oxpt_ctx_device(const oxpt_ctx* ctx);
 
+/* Stream marks: oxpt_mark records the current position of the context's
+ * stream; oxpt_wait_mark blocks until the stream has passed it (the last
+ * 64 marks are kept; an older one waits for the newest). A scheduler that
+ * queues the next batch before the previous one is done uses them to learn
+ * when each finished. */
+oxpt_status oxpt_mark(oxpt_ctx* ctx, uint64_t* mark);
+oxpt_status oxpt_wait_mark(oxpt_ctx* ctx, uint64_t mark);
+
 /* Device bytes a context holds: out[0] its own scene buffers (geometry,
  * attributes, atlas, four-wide tree; 0 when borrowed), out[1] its own
  * tables, out[2] accumulator and output images, out[3] working buffers

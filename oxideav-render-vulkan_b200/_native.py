@@ -158,6 +158,8 @@ _SIGS = {
     "oxpt_diag_timing": (cint, [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(u64)]),
     # oxpt_serve.h
     "oxpt_ctx_device": (cint, [vp]),
+    "oxpt_mark": (cint, [vp, C.POINTER(u64)]),
+    "oxpt_wait_mark": (cint, [vp, u64]),
     "oxpt_ctx_memory": (cint, [vp, C.POINTER(u64 * 4)]),
     "oxpt_tracer_new_view": (cint, [vp, C.POINTER(vp)]),
     "oxpt_tracer_view_sync": (cint, [vp, C.POINTER(RenderOptions), C.POINTER(cint)]),

@@ -43,6 +43,11 @@ struct oxpt_ctx {
     size_t table_words = 0;
     // scene buffers / tables borrowed from another context (oxpt_share_*)
     bool borrowed_scene = false, borrowed_tables = false;
+    std::vector<uint32_t> table_head;  // host copy of the first table words (fixed tables)
+    cudaEvent_t ready = nullptr;       // this context's stream position, for batches
+    // stream marks (oxpt_mark): a ring of events
+    std::vector<cudaEvent_t> marks;
+    uint64_t next_mark = 0;
     oxpt_params params{};
     bool has_scene = false, has_tables = false, has_params = false;
     // accumulation + outputs
@@ -93,6 +98,8 @@ struct oxpt_ctx {
     oxd::BatchFrame* batch_dev = nullptr;
     size_t batch_cap = 0;
     cudaEvent_t batch_done = nullptr;
+    oxd::BatchFrame* batch_host = nullptr;  // pinned staging of the records
+    cudaEvent_t batch_copied = nullptr;     // the staging buffer's last upload
     std::vector<oxpt_ctx*> batch_ctx;  // frame contexts of the current batch
     // CUDA-graph batches: the instantiated graph of the last step shape
     uint32_t graphs = 0;
@@ -531,6 +538,10 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
                     c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev};
     if (c->batch_done) cudaEventDestroy(c->batch_done);
+    if (c->batch_copied) cudaEventDestroy(c->batch_copied);
+    if (c->batch_host) cudaFreeHost(c->batch_host);
+    if (c->ready) cudaEventDestroy(c->ready);
+    for (cudaEvent_t ev : c->marks) cudaEventDestroy(ev);
     if (c->bgraph) cudaGraphExecDestroy(c->bgraph);
     if (c->dev_tally) cudaFree(c->dev_tally);
     if (c->capture) cudaStreamDestroy(c->capture);
@@ -629,6 +640,7 @@ oxpt_status oxpt_set_tables(oxpt_ctx* c, const uint32_t* words, size_t count) {
     }
     if ((s = realloc_dev(c, &c->tables, count * 4, "tables"))) return s;
     CK(c, cudaMemcpyAsync(c->tables, words, count * 4, cudaMemcpyHostToDevice, c->stream), "tables upload");
+    c->table_head.assign(words, words + std::min<size_t>(count, 4096));
     CK(c, cudaStreamSynchronize(c->stream), "tables upload");
     c->table_words = count;
     c->has_tables = true;
@@ -679,6 +691,7 @@ oxpt_status oxpt_share_tables(oxpt_ctx* c, const oxpt_ctx* owner) {
     else if (c->tables) cudaFree(c->tables);
     c->tables = owner->tables;
     c->table_words = owner->table_words;
+    c->table_head = owner->table_head;
     c->borrowed_tables = true;
     c->has_tables = true;
     return OXPT_OK;
@@ -985,6 +998,35 @@ static void read_tally(const oxpt_ctx* c, uint64_t out[2]) {
 
 int oxpt_ctx_device(const oxpt_ctx* c) { return c ? c->device : -1; }
 
+constexpr size_t MARK_RING = 64;
+
+oxpt_status oxpt_mark(oxpt_ctx* c, uint64_t* mark) {
+    if (!c || !mark) return OXPT_E_INVALID;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    if (c->marks.empty()) {
+        c->marks.resize(MARK_RING, nullptr);
+        for (auto& ev : c->marks) CK(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "mark event");
+    }
+    uint64_t m = c->next_mark++;
+    CK(c, cudaEventRecord(c->marks[m % MARK_RING], c->stream), "mark");
+    *mark = m;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_wait_mark(oxpt_ctx* c, uint64_t mark) {
+    if (!c) return OXPT_E_INVALID;
+    if (mark >= c->next_mark) return fail(c, OXPT_E_INVALID, "mark not recorded yet");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    if (c->next_mark - mark > MARK_RING) {  // overwritten: everything up to the newest mark
+        CK(c, cudaEventSynchronize(c->marks[(c->next_mark - 1) % MARK_RING]), "mark wait");
+        return OXPT_OK;
+    }
+    CK(c, cudaEventSynchronize(c->marks[mark % MARK_RING]), "mark wait");
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_ctx_memory(const oxpt_ctx* c, uint64_t out[4]) {
     if (!c || !out) return OXPT_E_INVALID;
     uint64_t scene = 0;
@@ -1254,10 +1296,21 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         uint64_t o0 = c->params.offs0[0], o1 = c->params.offs0[1];
         if (o0 + 128 > c->table_words || o1 + 512 > c->table_words)
             return fail(e, OXPT_E_INVALID, at + "tables too short for the Sobol' and sheen words");
-        if (c->stream != e->stream) CK(e, cudaStreamSynchronize(c->stream), "frame context sync");
+        if (c->stream != e->stream) {
+            // The batch starts after the frame context's queued work (no host wait).
+            if (!c->ready) CK(e, cudaEventCreateWithFlags(&c->ready, cudaEventDisableTiming), "frame event");
+            CK(e, cudaEventRecord(c->ready, c->stream), "frame event");
+            CK(e, cudaStreamWaitEvent(e->stream, c->ready, 0), "frame event");
+        }
         if (n == 1) continue;  // a single frame stages its own tables
-        CK(e, cudaMemcpy(tab.data(), c->tables + o0, 128 * 4, cudaMemcpyDeviceToHost), "table check");
-        CK(e, cudaMemcpy(tab.data() + 128, c->tables + o1, 512 * 4, cudaMemcpyDeviceToHost), "table check");
+        if (o0 + 128 <= c->table_head.size() && o1 + 512 <= c->table_head.size()) {
+            std::copy(c->table_head.begin() + o0, c->table_head.begin() + o0 + 128, tab.begin());
+            std::copy(c->table_head.begin() + o1, c->table_head.begin() + o1 + 512, tab.begin() + 128);
+        } else {
+            CK(e, cudaStreamSynchronize(c->stream), "frame context sync");
+            CK(e, cudaMemcpy(tab.data(), c->tables + o0, 128 * 4, cudaMemcpyDeviceToHost), "table check");
+            CK(e, cudaMemcpy(tab.data() + 128, c->tables + o1, 512 * 4, cudaMemcpyDeviceToHost), "table check");
+        }
         if (ref_tables.empty()) ref_tables = tab;
         else if (tab != ref_tables) return fail(e, OXPT_E_INVALID, at + "Sobol' or sheen table differs from the first frame's");
     }
@@ -1288,16 +1341,23 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
             if (c->bvh_depth > 32) sd = 64;
             if (e->shadow_walk == 0 && bvh4_usable(c) && c->bvh4_need > 32) sd = 64;
         }
+    // Records go through pinned staging: the host waits only until the
+    // previous batch's records were copied, not for that batch to finish.
+    if (e->batch_copied) CK(e, cudaEventSynchronize(e->batch_copied), "batch records staging");
     if (recs.size() > e->batch_cap) {
-        if ((s = realloc_dev(e, &e->batch_dev, recs.size() * sizeof(oxd::BatchFrame), "batch frame records"))) {
-            e->batch_cap = 0;
+        if (e->batch_host) cudaFreeHost(e->batch_host);
+        e->batch_host = nullptr;
+        e->batch_cap = 0;
+        if ((s = realloc_dev(e, &e->batch_dev, recs.size() * sizeof(oxd::BatchFrame), "batch frame records")))
             return s;
-        }
+        CK(e, cudaMallocHost((void**)&e->batch_host, recs.size() * sizeof(oxd::BatchFrame)), "batch records staging");
         e->batch_cap = recs.size();
     }
-    CK(e, cudaMemcpyAsync(e->batch_dev, recs.data(), recs.size() * sizeof(oxd::BatchFrame), cudaMemcpyHostToDevice,
+    std::memcpy((void*)e->batch_host, (const void*)recs.data(), recs.size() * sizeof(oxd::BatchFrame));
+    CK(e, cudaMemcpyAsync(e->batch_dev, e->batch_host, recs.size() * sizeof(oxd::BatchFrame), cudaMemcpyHostToDevice,
                           e->stream), "batch frame records");
-    CK(e, cudaStreamSynchronize(e->stream), "batch frame records");
+    if (!e->batch_copied) CK(e, cudaEventCreateWithFlags(&e->batch_copied, cudaEventDisableTiming), "batch event");
+    CK(e, cudaEventRecord(e->batch_copied, e->stream), "batch event");
     if ((s = ensure_out(e, cap))) return s;
     uint32_t saved_mode = e->mode;
     if (e->mode == OXPT_MODE_MEGAKERNEL) e->mode = OXPT_MODE_WAVEFRONT_SPLIT;

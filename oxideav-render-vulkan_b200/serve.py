@@ -116,13 +116,33 @@ class Server:
         out: Dict[int, Outcome] = {}
         pending = collections.deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
         waiting: collections.deque = collections.deque()
-        active: Dict[int, _Session] = {}     # session key -> session
+        active: Dict[int, _Session] = {}     # session key -> session (samples counted as queued)
         current: Dict[int, int] = {}         # session key -> request id it is rendering
         closed: Dict[int, Request] = {}      # finished sessions, for later moves
-        base = self.ex.resident_bytes()
-        used = base
+        inflight = None                      # (mark, [(session, request id, n)]) of the queued tick
+        used = self.ex.resident_bytes()
         t0 = self.clock()
-        while pending or waiting or active:
+
+        def retire(tick):
+            mark, work = tick
+            self.ex.wait(mark)
+            now = self.clock() - t0
+            for sess, rid, n in work:
+                o = out[rid]
+                if o.superseded:
+                    continue
+                o.paths += n * sess.req.pixels
+                if current.get(sess.key) == rid and sess.samples >= sess.req.spp and sess.key in active:
+                    o.finished = now
+                    self.ex.finished(sess.handle, o)
+                    self.ex.close(sess.handle)
+                    closed[sess.key] = sess.req
+                    del active[sess.key]
+                    del current[sess.key]
+                    nonlocal used
+                    used -= sess.bytes
+
+        while pending or waiting or active or inflight:
             now = self.clock() - t0
             while pending and pending[0].arrival <= now:
                 r = pending.popleft()
@@ -130,12 +150,14 @@ class Server:
                 stats.outcomes.append(out[r.rid])
                 key = r.session if r.session is not None else r.rid
                 if r.session is not None and key in active:
-                    # camera move on a running session: reset it in place
-                    s = active[key]
+                    # camera move on an open session: reset it in place (the
+                    # reset is ordered after any queued tick on the device)
+                    sess = active[key]
                     out[current[key]].superseded = True
-                    self.ex.move(s.handle, r.camera, r.spp)
-                    s.req = Request(r.rid, r.arrival, s.req.scene, s.req.width, s.req.height, r.spp, r.camera, key)
-                    s.samples = 0
+                    self.ex.move(sess.handle, r.camera, r.spp)
+                    sess.req = Request(r.rid, r.arrival, sess.req.scene, sess.req.width, sess.req.height, r.spp,
+                                       r.camera, key)
+                    sess.samples = 0
                     current[key] = r.rid
                     out[r.rid].admitted = now
                     continue
@@ -153,7 +175,7 @@ class Server:
             while waiting and len(active) < self.max_sessions:
                 r = waiting[0]
                 need = self.ex.footprint(r)
-                if used + need > self.budget and active:
+                if used + need > self.budget and (active or inflight):
                     break
                 waiting.popleft()
                 key = r.session if r.session is not None else r.rid
@@ -163,34 +185,27 @@ class Server:
                 used += need
                 out[r.rid].admitted = self.clock() - t0
             stats.peak_bytes = max(stats.peak_bytes, used)
-            if not active:
-                if pending:
-                    wait = pending[0].arrival - (self.clock() - t0)
-                    if wait > 0:
-                        self.sleep(wait)
-                continue
-            # one tick: an equal share of the path budget per session
-            share = max(1, self.tick_paths // len(active))
-            work = []
-            for s in active.values():
-                n = max(1, min(s.req.spp - s.samples, share // max(1, s.req.pixels)))
-                work.append((s, n))
-            self.ex.refine([(s.handle, n) for s, n in work])
-            self.ex.sync()
-            stats.ticks += 1
-            now = self.clock() - t0
-            for s, n in work:
-                s.samples += n
-                out[current[s.key]].paths += n * s.req.pixels
-                if s.samples >= s.req.spp:
-                    o = out[current[s.key]]
-                    o.finished = now
-                    self.ex.finished(s.handle, o)
-                    self.ex.close(s.handle)
-                    used -= s.bytes
-                    closed[s.key] = s.req
-                    del active[s.key]
-                    del current[s.key]
+            # queue the next tick: an equal share of the path budget for every
+            # session with samples left
+            todo = [sess for sess in active.values() if sess.samples < sess.req.spp]
+            tick = None
+            if todo:
+                share = max(1, self.tick_paths // len(todo))
+                work = []
+                for sess in todo:
+                    n = max(1, min(sess.req.spp - sess.samples, share // max(1, sess.req.pixels)))
+                    sess.samples += n
+                    work.append((sess, current[sess.key], n))
+                mark = self.ex.refine([(sess.handle, n) for sess, _, n in work])
+                tick = (mark, work)
+                stats.ticks += 1
+            if inflight is not None:
+                retire(inflight)
+            inflight = tick
+            if inflight is None and not active and not waiting and pending:
+                wait = pending[0].arrival - (self.clock() - t0)
+                if wait > 0:
+                    self.sleep(wait)
         stats.wall = self.clock() - t0
         return stats
 
@@ -270,7 +285,15 @@ class GpuExecutor:
             v.set_camera(None)
 
     def refine(self, work):
+        """Queues one batched tick; returns a mark to wait for."""
+        import ctypes as C
         self.pkg.refine_batch([v for v, _ in work], [n for _, n in work], executor=self.exe)
+        m = C.c_uint64()
+        self.pkg._native.lib().oxpt_mark(self.exe.ctx, C.byref(m))
+        return m.value
+
+    def wait(self, mark):
+        self.pkg._native.lib().oxpt_wait_mark(self.exe.ctx, mark)
 
     def refine_alone(self, v, n: int):
         v.refine(n)

@@ -49,6 +49,7 @@ class FakeExecutor:
         self.cur = {}       # session id -> samples since the last reset
         self.next_id = 0
         self.open_sessions = set()
+        self.busy_until = 0.0
 
     def resident_bytes(self):
         return 1000
@@ -74,8 +75,15 @@ class FakeExecutor:
         return n * px
 
     def refine(self, work):
+        # the device runs ticks back to back: a queued tick starts when the
+        # previous one ends, or now if the device is idle
         paths = sum(self._trace(h, n, self.px[h]) for h, n in work)
-        self.clock.t += paths / self.rate + self.launch_cost
+        start = max(self.busy_until, self.clock.t)
+        self.busy_until = start + paths / self.rate + self.launch_cost
+        return self.busy_until
+
+    def wait(self, mark):
+        self.clock.t = max(self.clock.t, mark)
 
     def refine_alone(self, h, n):
         self.clock.t += self._trace(h, n, self.px[h]) / self.rate + self.launch_cost * max(1, n // 4)
