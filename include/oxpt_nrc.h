@@ -1,0 +1,53 @@
+/*
+ * oxpt_nrc.h — neural radiance cache: a small MLP trained online on the
+ * tracer's own path samples, which ends paths after a few bounces with its
+ * prediction of the radiance still to come. No counterpart in the
+ * reference (its tracer is the unbiased plain form, which stays the
+ * fallback and the judge here too).
+ *
+ * Network: inputs = position (normalised to the scene bounds), outgoing
+ * direction, shading normal (each component mapped to [0, 1]) and
+ * roughness, 12 sine / cosine frequencies each (plus the raw values and a
+ * constant), 5 layers 256 -> 64 -> 64 -> 64 -> 64 -> 3 with ReLU, BF16
+ * weights and activations, FP32 accumulation on the tensor cores; loss =
+ * relative L2; Adam (lr 1e-2 by default).
+ */
+#ifndef OXPT_NRC_H
+#define OXPT_NRC_H
+
+#include "oxpt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oxpt_nrc oxpt_nrc;
+
+#define OXPT_NRC_PARAMS 29696u /* FP32 weights: 64x256, 3 x 64x64, 16x64 (rows 3..15 unused), row-major */
+#define OXPT_NRC_INPUTS 12u    /* floats per sample: pos.xyz, roughness, dir.xyz, 0, normal.xyz, 0 */
+
+/* A cache on `ctx`'s device and stream, weights initialised from `seed`
+ * (uniform He initialisation), Adam state zero. */
+oxpt_status oxpt_nrc_create(oxpt_ctx* ctx, uint64_t seed, oxpt_nrc** out);
+void oxpt_nrc_destroy(oxpt_nrc* nrc);
+const char* oxpt_nrc_last_error(const oxpt_nrc* nrc);
+
+oxpt_status oxpt_nrc_get_weights(oxpt_nrc* nrc, float* out);
+/* Replaces the weights and clears the Adam moments and step count. */
+oxpt_status oxpt_nrc_set_weights(oxpt_nrc* nrc, const float* weights);
+oxpt_status oxpt_nrc_set_adam(oxpt_nrc* nrc, float lr, float beta1, float beta2, float eps);
+
+/* Predictions for n samples (inputs n x 12 floats, out n x 4: rgb, 0),
+ * host buffers. */
+oxpt_status oxpt_nrc_infer(oxpt_nrc* nrc, const float* inputs, uint32_t n, float* out);
+/* One training step on n samples (targets n x 4: rgb, unused): forward,
+ * backward, and an Adam update when `apply` is non-zero. *loss = the mean
+ * relative L2 loss before the update; `grad` (optional) receives the
+ * gradient of that loss (OXPT_NRC_PARAMS floats). Host buffers. */
+oxpt_status oxpt_nrc_train(oxpt_nrc* nrc, const float* inputs, const float* targets, uint32_t n, int apply,
+                           float* loss, float* grad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OXPT_NRC_H */

@@ -44,6 +44,8 @@ class DeviceScene(C.Structure):
 
 
 NOALLOC_MAX_PATHS = 1 << 18
+NRC_PARAMS = 29696
+NRC_INPUTS = 12
 
 
 class BatchFrame(C.Structure):
@@ -156,6 +158,15 @@ _SIGS = {
     "oxpt_diag_timing_kinds": (cint, [vp, vp, vp]),
     "oxpt_diag_counters_split": (cint, [vp, vp]),
     "oxpt_diag_timing": (cint, [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), C.POINTER(u64)]),
+    # oxpt_nrc.h
+    "oxpt_nrc_create": (cint, [vp, u64, C.POINTER(vp)]),
+    "oxpt_nrc_destroy": (None, [vp]),
+    "oxpt_nrc_last_error": (C.c_char_p, [vp]),
+    "oxpt_nrc_get_weights": (cint, [vp, vp]),
+    "oxpt_nrc_set_weights": (cint, [vp, vp]),
+    "oxpt_nrc_set_adam": (cint, [vp, f32, f32, f32, f32]),
+    "oxpt_nrc_infer": (cint, [vp, vp, u32, vp]),
+    "oxpt_nrc_train": (cint, [vp, vp, vp, u32, cint, C.POINTER(f32), vp]),
     # oxpt_serve.h
     "oxpt_ctx_device": (cint, [vp]),
     "oxpt_mark": (cint, [vp, C.POINTER(u64)]),

@@ -1,0 +1,420 @@
+// Neural radiance cache: a 5-layer MLP (256 -> 64 -> 64 -> 64 -> 64 -> 3,
+// ReLU, no biases) with BF16 weights and activations and FP32 accumulation
+// on the fifth-generation tensor cores, trained online with Adam.
+//
+// The reference has no learned component; this follows the neural
+// radiance cache of Mueller, Rousselle, Novak and Keller (2021, "Real-time
+// neural radiance caching for path tracing"): inputs are a surface
+// vertex's position (normalised to the scene bounds), outgoing direction,
+// shading normal and roughness, encoded by 12 sine / cosine frequencies
+// each; the loss is the relative L2 (y - t)^2 / (sg(y)^2 + 0.01).
+//
+// Kernels (one warpgroup per CTA, 128 samples per tile, persistent grids):
+//   nrc_forward   encodes a tile into shared memory, then per layer issues
+//                 tcgen05.mma over the K slices (A = activations, B = the
+//                 layer's weights, both resident in shared memory), waits
+//                 on an mbarrier, reads the 128 x N FP32 accumulator from
+//                 TMEM (one row per thread), applies ReLU and writes the
+//                 next layer's BF16 operand. Inference writes predictions
+//                 (or adds beta * max(prediction, 0) into path results);
+//                 training also stores the hidden activations and the loss
+//                 gradient.
+//   nrc_backward  propagates the gradient down the layers with tcgen05
+//                 (delta_{l-1} = delta_l x W_l through W_l^T, masked by
+//                 ReLU) and accumulates the weight gradients delta^T x a
+//                 on the CUDA cores, one atomic add per weight per tile.
+//   nrc_adam      Adam on the FP32 master weights; rewrites the BF16
+//                 operand copies (forward and transposed layouts).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "nrc.cuh"
+#include "umma.cuh"
+
+namespace oxd {
+namespace nrc {
+
+using umma::cm_offset;
+
+// ---------------------------------------------------------------------
+// Shared-memory plans.
+// ---------------------------------------------------------------------
+constexpr uint32_t FWD_W = W_BYTES;                 // forward weights, all layers
+constexpr uint32_t FWD_A0 = FWD_W;                  // 128 x 256 encoded inputs
+constexpr uint32_t FWD_H = FWD_A0 + TILE * IN * 2;  // 128 x 64 hidden
+constexpr uint32_t FWD_BAR = FWD_H + TILE * HID * 2;
+constexpr uint32_t FWD_SMEM = FWD_BAR + 64;
+
+constexpr uint32_t BWD_WT = 0;                            // transposed weights, layers 1..4
+constexpr uint32_t BWD_GCM = BWD_WT + WT_BYTES;           // gradient operand, 128 x 64 bf16
+constexpr uint32_t BWD_G = BWD_GCM + TILE * HID * 2;      // gradient rows, 128 x 64 fp32
+constexpr uint32_t BWD_ACT = BWD_G + TILE * HID * 4;      // layer input rows, 128 x 64 bf16
+constexpr uint32_t BWD_A0 = BWD_ACT + TILE * HID * 2;     // encoded inputs, 128 x 256 bf16
+constexpr uint32_t BWD_BAR = BWD_A0 + TILE * IN * 2;
+constexpr uint32_t BWD_SMEM = BWD_BAR + 64;
+
+constexpr uint32_t WAIT_LIMIT = 1u << 26;
+
+// ---------------------------------------------------------------------
+// Encoding: 10 inputs x 12 frequencies x (sin, cos), the raw inputs, 1.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ void encode(const float4* in, uint32_t s, uint32_t n, float* f /* IN */) {
+    float x[RAW];
+    if (s < n) {
+        float4 a = in[3 * (size_t)s], b = in[3 * (size_t)s + 1], c = in[3 * (size_t)s + 2];
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+        x[8] = c.x; x[9] = c.y; x[10] = c.z; x[11] = c.w;
+    } else {
+        for (int i = 0; i < RAW; i++) x[i] = 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < USED; i++) {
+        float scale = 1.0f;
+#pragma unroll
+        for (int j = 0; j < FREQS; j++) {
+            float sv, cv;
+            sincospif(x[i] * scale, &sv, &cv);
+            f[2 * FREQS * i + 2 * j] = sv;
+            f[2 * FREQS * i + 2 * j + 1] = cv;
+            scale *= 2.0f;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < USED; i++) f[2 * FREQS * USED + i] = x[i];
+    f[2 * FREQS * USED + USED] = 1.0f;
+#pragma unroll
+    for (int i = 2 * FREQS * USED + USED + 1; i < IN; i++) f[i] = 0.0f;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+
+// Row r (K values in f) into a K-major core-matrix tile.
+template <int K>
+__device__ __forceinline__ void put_row(char* tile, uint32_t r, const float* f) {
+#pragma unroll
+    for (int kb = 0; kb < K / 8; kb++) {
+        uint4 v = make_uint4(pack_bf16(f[8 * kb], f[8 * kb + 1]), pack_bf16(f[8 * kb + 2], f[8 * kb + 3]),
+                             pack_bf16(f[8 * kb + 4], f[8 * kb + 5]), pack_bf16(f[8 * kb + 6], f[8 * kb + 7]));
+        *reinterpret_cast<uint4*>(tile + cm_offset(r, 8 * kb, K)) = v;
+    }
+}
+
+// Issues D = A x B^T over K (multiple of 16) with one thread and commits
+// to `bar`. A is 128 x K at `a`, B is N x K at `b`, both core-matrix tiles.
+__device__ __forceinline__ void layer_mma(uint32_t tmem, uint32_t a, uint32_t b, uint32_t K, uint32_t N,
+                                          uint64_t* bar) {
+    const uint32_t idesc = umma::idesc_bf16(TILE, N);
+    const uint32_t sbo = (K / 8) * 128;
+    for (uint32_t kk = 0; kk < K / 16; kk++)
+        umma::mma_bf16(tmem, umma::smem_desc(a + kk * 256, 128, sbo), umma::smem_desc(b + kk * 256, 128, sbo), idesc,
+                       kk > 0);
+    umma::commit(bar);
+}
+
+// Everyone: make shared-memory writes visible to the tensor core and
+// order them before the MMA thread's issue.
+__device__ __forceinline__ void publish_smem() {
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+}
+
+// Waits for the MMA batch; all threads see the same result.
+__device__ __forceinline__ bool await_mma(uint64_t* bar, uint32_t* phase, uint32_t* err) {
+    bool ok = umma::bar_wait(bar, *phase, WAIT_LIMIT);
+    *phase ^= 1u;
+    umma::fence_after_sync();
+    if (!ok) atomicOr(err, 16u);
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// This thread's TMEM row: `cols` FP32 values starting at column 0.
+__device__ __forceinline__ void read_row(uint32_t tmem, uint32_t cols, float* v) {
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t base = tmem + ((warp * 32u) << 16);
+    for (uint32_t c = 0; c < cols; c += 16) umma::tmem_ld16(base + c, v + c);
+}
+
+__global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ Args a) {
+    extern __shared__ __align__(1024) char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + FWD_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + FWD_BAR + 8);
+    const uint32_t t = threadIdx.x;
+    // Weights: a straight copy of the core-matrix image.
+    for (uint32_t i = t; i < FWD_W / 16; i += TILE)
+        reinterpret_cast<uint4*>(smem)[i] = reinterpret_cast<const uint4*>(a.wf)[i];
+    if (t == 0) umma::bar_init(bar, 1);
+    if (t < 32) umma::tmem_alloc(tslot, 64);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const uint32_t s_w = umma::smem_addr(smem), s_a0 = s_w + FWD_A0, s_h = s_w + FWD_H;
+    uint32_t phase = 0;
+    const uint32_t tiles = (a.n + TILE - 1) / TILE;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t s = tile * TILE + t;
+        float f[IN];
+        encode(a.in, s, a.n, f);
+        put_row<IN>(smem + FWD_A0, t, f);
+        publish_smem();
+        bool ok = true;
+        float v[HID];
+        for (int l = 0; l < LAYERS && ok; l++) {
+            const uint32_t K = l == 0 ? IN : HID, N = l == LAYERS - 1 ? OUT_PAD : HID;
+            if (t == 0) layer_mma(tmem, l == 0 ? s_a0 : s_h, s_w + W_OFF(l), K, N, bar);
+            ok = await_mma(bar, &phase, a.err);
+            if (!ok) break;
+            read_row(tmem, N, v);
+            if (l < LAYERS - 1) {
+#pragma unroll
+                for (int k = 0; k < HID; k++) v[k] = fmaxf(v[k], 0.0f);
+                umma::fence_before_sync();
+                __syncthreads();  // every row read before the next MMA overwrites D
+                put_row<HID>(smem + FWD_H, t, v);
+                if (a.acts && s < a.n) {
+                    uint4* dst = reinterpret_cast<uint4*>(a.acts + ((size_t)s * (LAYERS - 1) + l) * HID);
+#pragma unroll
+                    for (int kb = 0; kb < HID / 8; kb++)
+                        dst[kb] = make_uint4(pack_bf16(v[8 * kb], v[8 * kb + 1]), pack_bf16(v[8 * kb + 2], v[8 * kb + 3]),
+                                             pack_bf16(v[8 * kb + 4], v[8 * kb + 5]),
+                                             pack_bf16(v[8 * kb + 6], v[8 * kb + 7]));
+                }
+                publish_smem();
+            }
+        }
+        if (!ok) break;
+        // Outputs: v[0..2] radiance.
+        if (s < a.n) {
+            if (a.pred) a.pred[s] = make_float4(v[0], v[1], v[2], 0.0f);
+            if (a.query_out) {
+                float4 b = a.query_beta[s];
+                unsigned long long item = a.query_item[s];
+                float4 o = a.query_out[item];
+                o.x += b.x * fmaxf(v[0], 0.0f);
+                o.y += b.y * fmaxf(v[1], 0.0f);
+                o.z += b.z * fmaxf(v[2], 0.0f);
+                a.query_out[item] = o;
+            }
+        }
+        if (a.target) {
+            float loss = 0.0f;
+            float g[OUT_PAD];
+#pragma unroll
+            for (int c = 0; c < OUT_PAD; c++) g[c] = 0.0f;
+            if (s < a.n) {
+                float4 tg = a.target[s];
+                const float tv[3] = {tg.x, tg.y, tg.z};
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    float d = v[c] - tv[c];
+                    float w = 1.0f / (v[c] * v[c] + 0.01f);
+                    loss += d * d * w;
+                    g[c] = 2.0f * d * w * a.grad_scale;
+                }
+                float4* dst = reinterpret_cast<float4*>(a.dy + (size_t)s * OUT_PAD);
+#pragma unroll
+                for (int q = 0; q < OUT_PAD / 4; q++) dst[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+            if ((t & 31) == 0 && loss != 0.0f) atomicAdd(a.loss, loss);
+        }
+        umma::fence_before_sync();
+        __syncthreads();  // D and A0 are reused by the next tile
+        umma::fence_after_sync();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (t < 32) umma::tmem_free(tmem, 64);
+}
+
+__global__ void __launch_bounds__(TILE, 1) nrc_backward(const __grid_constant__ Args a) {
+    extern __shared__ __align__(1024) char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + BWD_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + BWD_BAR + 8);
+    float* G = reinterpret_cast<float*>(smem + BWD_G);                  // [128][64] fp32
+    uint16_t* ACT = reinterpret_cast<uint16_t*>(smem + BWD_ACT);        // [128][64] bf16
+    uint16_t* A0 = reinterpret_cast<uint16_t*>(smem + BWD_A0);          // [128][256] bf16
+    const uint32_t t = threadIdx.x;
+    for (uint32_t i = t; i < WT_BYTES / 16; i += TILE)
+        reinterpret_cast<uint4*>(smem + BWD_WT)[i] = reinterpret_cast<const uint4*>(a.wt)[i];
+    if (t == 0) umma::bar_init(bar, 1);
+    if (t < 32) umma::tmem_alloc(tslot, 64);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const uint32_t s_base = umma::smem_addr(smem), s_gcm = s_base + BWD_GCM;
+    uint32_t phase = 0;
+    const uint32_t tiles = (a.n + TILE - 1) / TILE;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t s = tile * TILE + t;
+        const bool live = s < a.n;
+        // Output gradient (N = 16) into G and its operand tile.
+        float g[HID];
+        for (int c = 0; c < OUT_PAD; c++) g[c] = live ? a.dy[(size_t)s * OUT_PAD + c] : 0.0f;
+        for (int c = 0; c < OUT_PAD; c++) G[t * HID + c] = g[c];
+        put_row<OUT_PAD>(smem + BWD_GCM, t, g);
+        bool ok = true;
+        for (int l = LAYERS - 1; l >= 1 && ok; l--) {
+            const uint32_t N = l == LAYERS - 1 ? OUT_PAD : HID;  // width of the gradient G
+            // Input of layer l (h_{l-1}) into ACT.
+            {
+                const uint4* src = reinterpret_cast<const uint4*>(a.acts + ((size_t)s * (LAYERS - 1) + (l - 1)) * HID);
+                uint4* dst = reinterpret_cast<uint4*>(ACT + t * HID);
+                for (int q = 0; q < HID / 8; q++) dst[q] = live ? src[q] : make_uint4(0, 0, 0, 0);
+            }
+            publish_smem();
+            // delta_{l-1} = G x W_l on the tensor cores (B = W_l^T, 64 x N).
+            if (t == 0) layer_mma(tmem, s_gcm, s_base + BWD_WT + WT_OFF(l), N, HID, bar);
+            // Meanwhile dW_l += G^T x ACT on the CUDA cores.
+            {
+                const uint32_t k = t % HID, half = t / HID;  // two threads per input column
+                const uint32_t n0 = half * (N / 2), n1 = n0 + N / 2;
+                float acc[HID / 2];
+                for (uint32_t i = 0; i < N / 2; i++) acc[i] = 0.0f;
+                for (uint32_t r = 0; r < TILE; r++) {
+                    float av = __uint_as_float((uint32_t)ACT[r * HID + k] << 16);
+                    if (av == 0.0f) continue;
+                    for (uint32_t nn = n0; nn < n1; nn++) acc[nn - n0] += G[r * HID + nn] * av;
+                }
+                for (uint32_t nn = n0; nn < n1; nn++)
+                    if (acc[nn - n0] != 0.0f) atomicAdd(a.grad + P_OFF(l) + nn * HID + k, acc[nn - n0]);
+            }
+            ok = await_mma(bar, &phase, a.err);
+            if (!ok) break;
+            float d[HID];
+            read_row(tmem, HID, d);
+            for (int k = 0; k < HID; k++) {
+                float h = __uint_as_float((uint32_t)ACT[t * HID + k] << 16);
+                d[k] = h > 0.0f ? d[k] : 0.0f;
+            }
+            umma::fence_before_sync();
+            __syncthreads();  // G, ACT and D reads done
+            for (int k = 0; k < HID; k++) G[t * HID + k] = d[k];
+            put_row<HID>(smem + BWD_GCM, t, d);
+            __syncthreads();
+        }
+        if (!ok) break;
+        // dW_0 += G^T x encoded inputs.
+        {
+            float f[IN];
+            encode(a.in, s, a.n, f);
+            for (int k = 0; k < IN; k += 2)
+                reinterpret_cast<uint32_t*>(A0)[(t * IN + k) >> 1] = pack_bf16(f[k], f[k + 1]);
+        }
+        __syncthreads();
+        {
+            const uint32_t k = 2 * t;  // columns k, k + 1
+            for (uint32_t n0 = 0; n0 < HID; n0 += 16) {
+                float acc0[16], acc1[16];
+                for (int i = 0; i < 16; i++) acc0[i] = acc1[i] = 0.0f;
+                for (uint32_t r = 0; r < TILE; r++) {
+                    uint32_t pv = reinterpret_cast<const uint32_t*>(A0)[(r * IN + k) >> 1];
+                    float x0 = bf16_lo(pv), x1 = bf16_hi(pv);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) {
+                        float gv = G[r * HID + n0 + i];
+                        acc0[i] += gv * x0;
+                        acc1[i] += gv * x1;
+                    }
+                }
+                for (int i = 0; i < 16; i++) {
+                    if (acc0[i] != 0.0f) atomicAdd(a.grad + P_OFF(0) + (n0 + i) * IN + k, acc0[i]);
+                    if (acc1[i] != 0.0f) atomicAdd(a.grad + P_OFF(0) + (n0 + i) * IN + k + 1, acc1[i]);
+                }
+            }
+        }
+        umma::fence_before_sync();
+        __syncthreads();
+        umma::fence_after_sync();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (t < 32) umma::tmem_free(tmem, 64);
+}
+
+// Layer, row (output) and column (input) of parameter i.
+__device__ __forceinline__ void locate(uint32_t i, int* l, uint32_t* n, uint32_t* k) {
+    int L = 0;
+    while (L < LAYERS - 1 && i >= P_OFF(L + 1)) L++;
+    uint32_t K = L == 0 ? IN : HID, j = i - P_OFF(L);
+    *l = L;
+    *n = j / K;
+    *k = j % K;
+}
+
+// BF16 operand images of parameter i (value w).
+__device__ __forceinline__ void publish_weight(const Args& a, uint32_t i, float w) {
+    int l;
+    uint32_t n, k;
+    locate(i, &l, &n, &k);
+    const uint32_t K = l == 0 ? IN : HID, N = l == LAYERS - 1 ? OUT_PAD : HID;
+    __nv_bfloat16 h = __float2bfloat16_rn(w);
+    *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(a.wf) + W_OFF(l) + cm_offset(n, k, K)) = h;
+    if (l >= 1)  // W_l^T: rows = inputs k, K dimension = outputs n
+        *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(a.wt) + WT_OFF(l) + cm_offset(k, n, N)) = h;
+}
+
+__global__ void nrc_adam(const __grid_constant__ Args a, AdamStep st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= PARAMS) return;
+    float w = a.master[i];
+    if (st.apply) {
+        float g = a.grad[i];
+        float m = st.b1 * a.m1[i] + (1.0f - st.b1) * g;
+        float v = st.b2 * a.m2[i] + (1.0f - st.b2) * g * g;
+        a.m1[i] = m;
+        a.m2[i] = v;
+        w -= st.lr * (m * st.c1) / (sqrtf(v * st.c2) + st.eps);
+        a.master[i] = w;
+    }
+    publish_weight(a, i, w);
+}
+
+cudaError_t launch_forward(const Args& a, int sms, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(nrc_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM);
+        if (e) return e;
+        attr = true;
+    }
+    uint32_t tiles = (a.n + TILE - 1) / TILE;
+    if (tiles == 0) return cudaSuccess;
+    uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
+    nrc_forward<<<grid, TILE, FWD_SMEM, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward(const Args& a, int sms, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(nrc_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, BWD_SMEM);
+        if (e) return e;
+        attr = true;
+    }
+    uint32_t tiles = (a.n + TILE - 1) / TILE;
+    if (tiles == 0) return cudaSuccess;
+    uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
+    nrc_backward<<<grid, TILE, BWD_SMEM, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adam(const Args& a, const AdamStep& s, cudaStream_t st) {
+    nrc_adam<<<(PARAMS + 255) / 256, 256, 0, st>>>(a, s);
+    return cudaGetLastError();
+}
+
+}  // namespace nrc
+}  // namespace oxd

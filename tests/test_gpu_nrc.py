@@ -1,0 +1,120 @@
+"""Radiance-cache network on the tensor cores against the FP64 model
+(oracle/nrc.py): forward outputs, loss, gradients (the backward kernel),
+one Adam step, and that online training drives the loss down.
+
+Tolerances: the GPU multiplies BF16 operands with FP32 accumulation; the
+model rounds the same operands to BF16 and sums in FP64, so the remaining
+differences are summation order and the rare BF16 rounding that a last-bit
+difference flips (2% relative on outputs, 3% on each layer's gradient).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import nrc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def cache(pkg):
+    L = pkg._native.lib()
+    t = pkg.GpuPathTracer(0)
+    h = C.c_void_p()
+    assert L.oxpt_nrc_create(t.ctx, 11, C.byref(h)) == 0
+    yield L, h
+    L.oxpt_nrc_destroy(h)
+
+
+def _inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    x = np.zeros((n, 12), np.float32)
+    x[:, :10] = rng.random((n, 10))
+    return x
+
+
+def _target(x):
+    t = np.zeros((x.shape[0], 4), np.float32)
+    t[:, 0] = 0.6 + 0.4 * np.sin(3.0 * x[:, 0]) * np.cos(2.0 * x[:, 3])
+    t[:, 1] = 0.3 + 0.5 * x[:, 1] * x[:, 9]
+    t[:, 2] = 1.0 + 0.5 * np.cos(5.0 * x[:, 2] + x[:, 6])
+    return t
+
+
+def _set(L, h, w):
+    w = np.ascontiguousarray(w, np.float32)
+    assert L.oxpt_nrc_set_weights(h, w.ctypes.data) == 0
+
+
+def test_forward_matches_the_fp64_model(cache):
+    L, h = cache
+    w = nrc.init(7)
+    _set(L, h, w)
+    x = _inputs(1037, 1)  # not a multiple of the 128-sample tile
+    out = np.zeros((x.shape[0], 4), np.float32)
+    assert L.oxpt_nrc_infer(h, x.ctypes.data, x.shape[0], out.ctypes.data) == 0
+    y, _ = nrc.forward(w, x, bf=True)
+    ref = y[:, :3]
+    err = np.abs(out[:, :3] - ref) / (np.abs(ref) + 0.05 * np.mean(np.abs(ref)))
+    assert np.quantile(err, 0.999) < 0.02 and err.max() < 0.1, (np.quantile(err, 0.999), err.max())
+    assert np.all(out[:, 3] == 0.0)
+
+
+def test_loss_and_gradient_match_the_fp64_model(cache):
+    L, h = cache
+    w = nrc.init(9)
+    _set(L, h, w)
+    x = _inputs(1000, 2)
+    t = _target(x)
+    loss = C.c_float()
+    g = np.zeros(nrc.PARAMS, np.float32)
+    assert L.oxpt_nrc_train(h, x.ctypes.data, t.ctypes.data, x.shape[0], 0, C.byref(loss), g.ctypes.data) == 0
+    want_loss, want_g = nrc.loss_grad(w, x, t, bf=True)
+    assert abs(loss.value - want_loss) <= 2e-3 * want_loss
+    for l in range(nrc.LAYERS):
+        a, b = g[nrc.OFFS[l]:nrc.OFFS[l + 1]], want_g[nrc.OFFS[l]:nrc.OFFS[l + 1]]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel < 0.03, (l, rel)
+    # weights unchanged without `apply`
+    w2 = np.zeros(nrc.PARAMS, np.float32)
+    assert L.oxpt_nrc_get_weights(h, w2.ctypes.data) == 0
+    assert np.array_equal(w2, w)
+
+
+def test_adam_step_on_the_device_gradient(cache):
+    L, h = cache
+    w = nrc.init(3)
+    _set(L, h, w)
+    x = _inputs(640, 3)
+    t = _target(x)
+    loss = C.c_float()
+    g = np.zeros(nrc.PARAMS, np.float32)
+    assert L.oxpt_nrc_train(h, x.ctypes.data, t.ctypes.data, x.shape[0], 1, C.byref(loss), g.ctypes.data) == 0
+    w1 = np.zeros(nrc.PARAMS, np.float32)
+    L.oxpt_nrc_get_weights(h, w1.ctypes.data)
+    want, _, _ = nrc.adam(w.astype(np.float64), g.astype(np.float64), 0.0, 0.0, 1)
+    assert np.allclose(w1, want, rtol=1e-5, atol=1e-6)
+
+
+def test_online_training_reduces_the_loss(cache):
+    L, h = cache
+    rng = np.random.default_rng(4)
+    losses = []
+    for step in range(300):
+        x = _inputs(4096, 100 + step)
+        t = _target(x)
+        loss = C.c_float()
+        assert L.oxpt_nrc_train(h, x.ctypes.data, t.ctypes.data, x.shape[0], 1, C.byref(loss), None) == 0
+        losses.append(loss.value)
+    assert np.isfinite(losses).all()
+    assert np.mean(losses[-20:]) < 0.2 * np.mean(losses[:5]), (losses[:5], losses[-5:])
+    # and it generalises to unseen inputs
+    x = _inputs(2048, 9999)
+    out = np.zeros((x.shape[0], 4), np.float32)
+    assert L.oxpt_nrc_infer(h, x.ctypes.data, x.shape[0], out.ctypes.data) == 0
+    t = _target(x)
+    rel = np.mean((out[:, :3] - t[:, :3]) ** 2 / (t[:, :3] ** 2 + 0.01))
+    assert rel < 0.02, rel
