@@ -16,6 +16,7 @@
 #define OXPT_NRC_H
 
 #include "oxpt.h"
+#include "oxpt_host.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -46,6 +47,44 @@ oxpt_status oxpt_nrc_infer(oxpt_nrc* nrc, const float* inputs, uint32_t n, float
  * gradient of that loss (OXPT_NRC_PARAMS floats). Host buffers. */
 oxpt_status oxpt_nrc_train(oxpt_nrc* nrc, const float* inputs, const float* targets, uint32_t n, int apply,
                            float* loss, float* grad);
+
+/*
+ * Rendering with the cache: each frame traces one sample per pixel of
+ * `ctx`'s image with the split wavefront. A path that is not a training
+ * path stops at the vertex hit by ray `query_bounce` (2: after two bounces;
+ * it keeps that vertex's emission) and the cache's prediction times its
+ * throughput there is added instead of the rest of the path. One path in
+ * `train_one_in` (by its path seed) is traced to the end as the plain
+ * tracer would and becomes a training sample: the vertex's inputs and the
+ * radiance it gathered from there on per unit throughput. After a frame's
+ * results are reduced into the accumulator, the cache takes one Adam step
+ * on that frame's samples (at most `max_train`) when `train` is set.
+ * `enabled` = 0 renders plain frames (the ablation). The frame must fit
+ * one launch of the context's plan (width x height <= its items per
+ * launch).
+ */
+typedef struct oxpt_nrc_config {
+    uint32_t enabled;
+    uint32_t query_bounce;
+    uint32_t train_one_in;  /* a power of two */
+    uint32_t max_train;
+    uint32_t train;
+    uint32_t reserved[3];
+} oxpt_nrc_config;
+void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1 */
+
+/* `count` cache frames with sample indices first_sample.. on `ctx`'s
+ * accumulator; *loss (optional, waits for the GPU) = the last frame's mean
+ * training loss before its update. */
+oxpt_status oxpt_nrc_refine(oxpt_nrc* nrc, oxpt_ctx* ctx, uint32_t first_sample, uint32_t count,
+                            const oxpt_nrc_config* cfg, float* loss);
+/* refine() of a tracer with cache frames: `frames` samples per pixel, one
+ * per frame, on the tracer's bound scene and options; its sample count
+ * advances as with oxpt_tracer_refine. */
+oxpt_status oxpt_tracer_refine_nrc(oxpt_tracer* t, oxpt_nrc* nrc, uint32_t frames, const oxpt_nrc_config* cfg,
+                                   float* loss);
+/* Training samples and cache queries of the last frame (waits). */
+oxpt_status oxpt_nrc_frame_counts(oxpt_nrc* nrc, uint32_t* queries, uint32_t* samples);
 
 #ifdef __cplusplus
 }

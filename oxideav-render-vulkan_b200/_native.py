@@ -52,6 +52,11 @@ class BatchFrame(C.Structure):
     _fields_ = [("ctx", vp), ("first", u32), ("count", u32), ("y0", u32), ("rows", u32)]
 
 
+class NrcConfig(C.Structure):
+    _fields_ = [("enabled", u32), ("query_bounce", u32), ("train_one_in", u32), ("max_train", u32),
+                ("train", u32), ("reserved", u32 * 3)]
+
+
 class DevImage(C.Structure):
     _fields_ = [("data", vp), ("width", u32), ("height", u32), ("pitch_bytes", u32), ("format", u32)]
 
@@ -167,6 +172,10 @@ _SIGS = {
     "oxpt_nrc_set_adam": (cint, [vp, f32, f32, f32, f32]),
     "oxpt_nrc_infer": (cint, [vp, vp, u32, vp]),
     "oxpt_nrc_train": (cint, [vp, vp, vp, u32, cint, C.POINTER(f32), vp]),
+    "oxpt_nrc_config_default": (None, [C.c_void_p]),
+    "oxpt_nrc_refine": (cint, [vp, vp, u32, u32, C.c_void_p, C.POINTER(f32)]),
+    "oxpt_nrc_frame_counts": (cint, [vp, C.POINTER(u32), C.POINTER(u32)]),
+    "oxpt_tracer_refine_nrc": (cint, [vp, vp, u32, C.c_void_p, C.POINTER(f32)]),
     # oxpt_serve.h
     "oxpt_ctx_device": (cint, [vp]),
     "oxpt_mark": (cint, [vp, C.POINTER(u64)]),

@@ -22,6 +22,9 @@
 #include "../../include/oxpt_serve.h"
 #include "kernels.cuh"
 #include "wavefront.cuh"
+#include "../../include/oxpt_nrc.h"
+#include "nrc.cuh"
+#include "nrc_state.hpp"
 #include "../host/batch.hpp"
 #include "../host/bvh4.hpp"
 
@@ -309,7 +312,7 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
 oxpt_status wave_loop(oxpt_ctx* c, const oxd::WaveArgs& wa, bool count, bool four, int sd, int sd4,
                       uint32_t max_bounces);
 
-oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
+oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const oxd::NrcWave* nrc = nullptr) {
     uint32_t J = c->params.cfg[2] + 1u;
     uint64_t total = ta.total;
     uint32_t P = (uint32_t)std::min<uint64_t>(total, c->wave_slots);
@@ -330,6 +333,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count) {
     wa.err = ta.err;
     wa.frames = nullptr;
     wa.nframes = 0;
+    wa.nrc = nrc ? *nrc : oxd::NrcWave{};
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
     bool four = c->shadow_walk == 0 && bvh4_usable(c);
@@ -1437,6 +1441,186 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         oxpt_ctx* c = fr[k].ctx;
         if (c && c->stream != e->stream) CK(e, cudaStreamWaitEvent(c->stream, e->batch_done, 0), "batch event");
     }
+    return OXPT_OK;
+}
+
+// ---------------------------------------------------------------------
+// Radiance-cache frames (oxpt_nrc.h).
+// ---------------------------------------------------------------------
+
+void oxpt_nrc_config_default(oxpt_nrc_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->enabled = 1;
+    cfg->query_bounce = 2;
+    cfg->train_one_in = 16;
+    cfg->max_train = 65536;
+    cfg->train = 1;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class T>
+oxpt_status grow(oxpt_ctx* c, T** p, size_t* cap, size_t need, size_t elems_per, const char* what) {
+    if (need <= *cap && *p) return OXPT_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    CK(c, cudaMalloc((void**)p, need * elems_per * sizeof(T)), what);
+    *cap = need;
+    return OXPT_OK;
+}
+
+oxpt_status nrc_buffers(oxpt_ctx* c, oxpt_nrc* r, size_t q, size_t t, size_t slots) {
+    oxpt_status s;
+    size_t dummy = 0;
+    if (!r->counts && (s = grow(c, &r->counts, &dummy, 2, 1, "cache counters"))) return s;
+    if (q > r->q_cap) {
+        size_t c1 = 0, c2 = 0, c3 = 0;
+        if ((s = grow(c, &r->q_in, &c1, q, 3, "cache queries"))) return s;
+        if ((s = grow(c, &r->q_beta, &c2, q, 1, "cache queries"))) return s;
+        if ((s = grow(c, &r->q_item, &c3, q, 1, "cache queries"))) return s;
+        r->q_cap = q;
+    }
+    if (t > r->t_cap) {
+        size_t c1 = 0, c2 = 0;
+        if ((s = grow(c, &r->t_in, &c1, t, 3, "cache training samples"))) return s;
+        if ((s = grow(c, &r->t_target, &c2, t, 1, "cache training samples"))) return s;
+        r->t_cap = t;
+    }
+    if (slots > r->s_cap) {
+        size_t c1 = 0, c2 = 0, c3 = 0;
+        if ((s = grow(c, &r->s_pre, &c1, slots, 1, "cache slot state"))) return s;
+        if ((s = grow(c, &r->s_beta, &c2, slots, 1, "cache slot state"))) return s;
+        if ((s = grow(c, &r->s_tidx, &c3, slots, 1, "cache slot state"))) return s;
+        r->s_cap = slots;
+    }
+    return OXPT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t count, const oxpt_nrc_config* cfg,
+                            float* loss) {
+    if (!r || !c || !cfg) return fail(c, OXPT_E_INVALID, "null argument");
+    if (r->device != c->device) return fail(c, OXPT_E_INVALID, "the cache lives on another device");
+    if (count == 0) return OXPT_OK;
+    if (!cfg->enabled) {
+        oxpt_frame f{first, count, 0, c->h};
+        return oxpt_dispatch(c, &f);
+    }
+    if (cfg->train_one_in == 0 || (cfg->train_one_in & (cfg->train_one_in - 1)) != 0)
+        return fail(c, OXPT_E_INVALID, "train_one_in must be a power of two");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    if ((s = ready(c))) return s;
+    const uint64_t npix = (uint64_t)c->w * c->h;
+    if (npix > c->wave_items) return fail(c, OXPT_E_LIMIT, "a cache frame must fit one launch (width x height <= wave_items)");
+    const uint32_t P = (uint32_t)std::min<uint64_t>(npix, c->wave_slots);
+    const uint32_t max_train = std::max(cfg->max_train, 1u);
+    if ((s = nrc_buffers(c, r, npix, max_train, P))) return s;
+    if ((s = oxd::nrc::ensure_scratch(r, max_train))) return s;
+    if ((s = ensure_out(c, npix))) return s;
+    uint32_t saved_mode = c->mode;
+    c->mode = OXPT_MODE_WAVEFRONT_SPLIT;
+    for (uint32_t i = 0; i < count && !s; i++) {
+        cudaError_t ce = cudaMemsetAsync(r->counts, 0, 8, c->stream);
+        if (ce) {
+            s = cuda_fail(c, ce, "cache counters");
+            break;
+        }
+        oxd::TraceArgs ta;
+        ta.s = scene_view(c);
+        ta.first = first + i;
+        ta.count = 1;
+        ta.y0 = 0;
+        ta.rows = c->h;
+        ta.npix = (uint32_t)npix;
+        ta.total = npix;
+        ta.out = c->out;
+        ta.counters = nullptr;
+        ta.err = c->dev_err;
+        oxd::NrcWave nw{};
+        nw.on = 1;
+        nw.query_k = cfg->query_bounce;
+        nw.train_mask = cfg->train_one_in - 1;
+        nw.q_cap = (uint32_t)npix;
+        nw.t_cap = max_train;
+        nw.counts = r->counts;
+        nw.q_in = r->q_in;
+        nw.q_beta = r->q_beta;
+        nw.q_item = r->q_item;
+        nw.t_in = r->t_in;
+        nw.t_target = r->t_target;
+        nw.s_pre = r->s_pre;
+        nw.s_beta = r->s_beta;
+        nw.s_tidx = r->s_tidx;
+        if ((s = run_wave(c, ta, false, &nw))) break;
+        // The cache's predictions complete the rendering paths.
+        oxd::nrc::Args a = oxd::nrc::base_args(r);
+        a.in = r->q_in;
+        a.n = (uint32_t)npix;
+        a.n_dev = r->counts;
+        a.query_beta = r->q_beta;
+        a.query_item = r->q_item;
+        a.query_out = c->out;
+        if ((ce = oxd::nrc::launch_forward(a, c->sms, c->stream))) {
+            s = cuda_fail(c, ce, "cache inference");
+            break;
+        }
+        oxd::ReduceArgs ra{c->accum, c->out, c->w, 0, (uint32_t)npix, 1};
+        if ((ce = oxd::launch_reduce(ra, c->stream))) {
+            s = cuda_fail(c, ce, "reduce");
+            break;
+        }
+        c->launches += 2;
+        if (cfg->train) {
+            ce = cudaMemsetAsync(r->grad, 0, oxd::nrc::PARAMS * 4, c->stream);
+            if (!ce) ce = cudaMemsetAsync(r->loss, 0, 4, c->stream);
+            oxd::nrc::Args b = oxd::nrc::base_args(r);
+            b.in = r->t_in;
+            b.n = max_train;
+            b.n_dev = r->counts + 1;
+            b.target = r->t_target;
+            b.acts = r->acts;
+            b.dy = r->dy;
+            b.grad_scale = 0.0f;
+            if (!ce) ce = oxd::nrc::launch_forward(b, c->sms, c->stream);
+            if (!ce) ce = oxd::nrc::launch_backward(b, c->sms, c->stream);
+            if (!ce) ce = oxd::nrc::adam_step(r, c->stream);
+            if (ce) {
+                s = cuda_fail(c, ce, "cache training");
+                break;
+            }
+            c->launches += 3;
+        }
+    }
+    c->mode = saved_mode;
+    if (s) return s;
+    if (loss) {
+        float l = 0.0f;
+        uint32_t n[2] = {0, 0};
+        CK(c, cudaMemcpyAsync(&l, r->loss, 4, cudaMemcpyDeviceToHost, c->stream), "cache loss");
+        CK(c, cudaMemcpyAsync(n, r->counts, 8, cudaMemcpyDeviceToHost, c->stream), "cache counters");
+        CK(c, cudaStreamSynchronize(c->stream), "cache loss");
+        uint32_t m = std::min(n[1], max_train);
+        *loss = m ? l / (3.0f * (float)m) : 0.0f;
+    }
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_nrc_frame_counts(oxpt_nrc* r, uint32_t* queries, uint32_t* samples) {
+    if (!r || !r->counts) return OXPT_E_INVALID;
+    uint32_t n[2] = {0, 0};
+    if (cudaSetDevice(r->device) != cudaSuccess) return OXPT_E_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(n, r->counts, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return OXPT_E_CUDA;
+    if (queries) *queries = n[0];
+    if (samples) *samples = n[1];
     return OXPT_OK;
 }
 

@@ -136,6 +136,13 @@ __device__ __forceinline__ bool await_mma(uint64_t* bar, uint32_t* phase, uint32
     return __syncthreads_and(ok ? 1 : 0) != 0;
 }
 
+// Samples of this launch: a.n, or fewer when the count is on the device.
+__device__ __forceinline__ uint32_t count_of(const Args& a) {
+    if (!a.n_dev) return a.n;
+    uint32_t d = *((volatile const uint32_t*)a.n_dev);
+    return d < a.n ? d : a.n;
+}
+
 // This thread's TMEM row: `cols` FP32 values starting at column 0.
 __device__ __forceinline__ void read_row(uint32_t tmem, uint32_t cols, float* v) {
     const uint32_t warp = threadIdx.x >> 5;
@@ -159,11 +166,13 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
     const uint32_t tmem = *tslot;
     const uint32_t s_w = umma::smem_addr(smem), s_a0 = s_w + FWD_A0, s_h = s_w + FWD_H;
     uint32_t phase = 0;
-    const uint32_t tiles = (a.n + TILE - 1) / TILE;
+    const uint32_t n = count_of(a);
+    const float grad_scale = a.grad_scale != 0.0f ? a.grad_scale : 1.0f / (3.0f * (float)(n ? n : 1u));
+    const uint32_t tiles = (n + TILE - 1) / TILE;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t s = tile * TILE + t;
         float f[IN];
-        encode(a.in, s, a.n, f);
+        encode(a.in, s, n, f);
         put_row<IN>(smem + FWD_A0, t, f);
         publish_smem();
         bool ok = true;
@@ -180,7 +189,7 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
                 umma::fence_before_sync();
                 __syncthreads();  // every row read before the next MMA overwrites D
                 put_row<HID>(smem + FWD_H, t, v);
-                if (a.acts && s < a.n) {
+                if (a.acts && s < n) {
                     uint4* dst = reinterpret_cast<uint4*>(a.acts + ((size_t)s * (LAYERS - 1) + l) * HID);
 #pragma unroll
                     for (int kb = 0; kb < HID / 8; kb++)
@@ -193,7 +202,7 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
         }
         if (!ok) break;
         // Outputs: v[0..2] radiance.
-        if (s < a.n) {
+        if (s < n) {
             if (a.pred) a.pred[s] = make_float4(v[0], v[1], v[2], 0.0f);
             if (a.query_out) {
                 float4 b = a.query_beta[s];
@@ -210,7 +219,7 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
             float g[OUT_PAD];
 #pragma unroll
             for (int c = 0; c < OUT_PAD; c++) g[c] = 0.0f;
-            if (s < a.n) {
+            if (s < n) {
                 float4 tg = a.target[s];
                 const float tv[3] = {tg.x, tg.y, tg.z};
 #pragma unroll
@@ -218,7 +227,7 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
                     float d = v[c] - tv[c];
                     float w = 1.0f / (v[c] * v[c] + 0.01f);
                     loss += d * d * w;
-                    g[c] = 2.0f * d * w * a.grad_scale;
+                    g[c] = 2.0f * d * w * grad_scale;
                 }
                 float4* dst = reinterpret_cast<float4*>(a.dy + (size_t)s * OUT_PAD);
 #pragma unroll
@@ -256,10 +265,11 @@ __global__ void __launch_bounds__(TILE, 1) nrc_backward(const __grid_constant__ 
     const uint32_t tmem = *tslot;
     const uint32_t s_base = umma::smem_addr(smem), s_gcm = s_base + BWD_GCM;
     uint32_t phase = 0;
-    const uint32_t tiles = (a.n + TILE - 1) / TILE;
+    const uint32_t n = count_of(a);
+    const uint32_t tiles = (n + TILE - 1) / TILE;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t s = tile * TILE + t;
-        const bool live = s < a.n;
+        const bool live = s < n;
         // Output gradient (N = 16) into G and its operand tile.
         float g[HID];
         for (int c = 0; c < OUT_PAD; c++) g[c] = live ? a.dy[(size_t)s * OUT_PAD + c] : 0.0f;
@@ -309,7 +319,7 @@ __global__ void __launch_bounds__(TILE, 1) nrc_backward(const __grid_constant__ 
         // dW_0 += G^T x encoded inputs.
         {
             float f[IN];
-            encode(a.in, s, a.n, f);
+            encode(a.in, s, n, f);
             for (int k = 0; k < IN; k += 2)
                 reinterpret_cast<uint32_t*>(A0)[(t * IN + k) >> 1] = pack_bf16(f[k], f[k + 1]);
         }

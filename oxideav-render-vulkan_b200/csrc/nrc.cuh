@@ -42,7 +42,8 @@ struct Args {
     uint16_t* wf;                 // forward operand image (W_BYTES)
     uint16_t* wt;                 // transposed operand image (WT_BYTES)
     const float4* in;             // n x 3 float4 inputs
-    uint32_t n;
+    uint32_t n;                   // samples (capacity of the arrays when n_dev is set)
+    const uint32_t* n_dev;        // optional: the sample count in device memory (min with n)
     float4* pred;                 // inference: n predictions (rgb, 0), or null
     const float4* query_beta;     // path queries: throughput per sample, or null
     const unsigned long long* query_item;  // path result index per sample
@@ -51,7 +52,7 @@ struct Args {
     uint16_t* acts;               // training: n x 4 x 64 bf16 hidden activations
     float* dy;                    // training: n x 16 loss gradient w.r.t. outputs
     float* loss;                  // training: summed relative L2 loss
-    float grad_scale;             // 1 / (3 n): the loss is a mean over samples and channels
+    float grad_scale;             // 1 / (3 n): the loss is a mean over samples and channels (0: from n)
     float* grad;                  // PARAMS gradient accumulator
     float* master;                // PARAMS FP32 weights
     float* m1;                    // Adam first moments

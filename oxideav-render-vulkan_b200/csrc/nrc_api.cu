@@ -11,25 +11,10 @@
 #include "../../include/oxpt_nrc.h"
 #include "../../include/oxpt_serve.h"
 #include "nrc.cuh"
+#include "nrc_state.hpp"
 
 using namespace oxd::nrc;
 
-struct oxpt_nrc {
-    oxpt_ctx* ctx = nullptr;
-    int device = 0, sms = 1;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *loss = nullptr;
-    uint16_t *wf = nullptr, *wt = nullptr;
-    uint32_t* err_dev = nullptr;
-    // scratch of the host-buffer calls
-    float4 *in = nullptr, *pred = nullptr, *target = nullptr;
-    uint16_t* acts = nullptr;
-    float* dy = nullptr;
-    size_t cap = 0;
-    float lr = 1e-2f, b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
-    uint64_t step = 0;
-};
 
 namespace {
 
@@ -48,7 +33,9 @@ oxpt_status ncuda(oxpt_nrc* c, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return ncuda(c, e_, what);   \
     } while (0)
 
-Args base_args(oxpt_nrc* c) {
+}  // namespace
+
+Args oxd::nrc::base_args(oxpt_nrc* c) {
     Args a;
     std::memset(&a, 0, sizeof(a));
     a.wf = c->wf;
@@ -62,7 +49,7 @@ Args base_args(oxpt_nrc* c) {
     return a;
 }
 
-oxpt_status ensure_scratch(oxpt_nrc* c, size_t n) {
+oxpt_status oxd::nrc::ensure_scratch(oxpt_nrc* c, size_t n) {
     if (n <= c->cap) return OXPT_OK;
     void* ptrs[] = {c->in, c->pred, c->target, c->acts, c->dy};
     for (void* p : ptrs)
@@ -79,6 +66,21 @@ oxpt_status ensure_scratch(oxpt_nrc* c, size_t n) {
     c->cap = n;
     return OXPT_OK;
 }
+
+cudaError_t oxd::nrc::adam_step(oxpt_nrc* c, cudaStream_t st) {
+    c->step++;
+    AdamStep a;
+    a.lr = c->lr;
+    a.b1 = c->b1;
+    a.b2 = c->b2;
+    a.eps = c->eps;
+    a.c1 = (float)(1.0 / (1.0 - std::pow((double)c->b1, (double)c->step)));
+    a.c2 = (float)(1.0 / (1.0 - std::pow((double)c->b2, (double)c->step)));
+    a.apply = 1;
+    return launch_adam(base_args(c), a, st);
+}
+
+namespace {
 
 // Rewrites the BF16 operand images from the FP32 master weights.
 oxpt_status publish(oxpt_nrc* c) {
@@ -163,7 +165,8 @@ void oxpt_nrc_destroy(oxpt_nrc* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->loss, c->wf, c->wt, c->err_dev,
-                    c->in, c->pred, c->target, c->acts, c->dy};
+                    c->in, c->pred, c->target, c->acts, c->dy, c->counts, c->q_in, c->q_beta, c->q_item,
+                    c->t_in, c->t_target, c->s_pre, c->s_beta, c->s_tidx};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;
@@ -237,18 +240,7 @@ oxpt_status oxpt_nrc_train(oxpt_nrc* c, const float* inputs, const float* target
     a.grad_scale = 1.0f / (3.0f * (float)n);
     NK(c, launch_forward(a, c->sms, c->stream), "nrc forward");
     NK(c, launch_backward(a, c->sms, c->stream), "nrc backward");
-    if (apply) {
-        c->step++;
-        AdamStep st;
-        st.lr = c->lr;
-        st.b1 = c->b1;
-        st.b2 = c->b2;
-        st.eps = c->eps;
-        st.c1 = (float)(1.0 / (1.0 - std::pow((double)c->b1, (double)c->step)));
-        st.c2 = (float)(1.0 / (1.0 - std::pow((double)c->b2, (double)c->step)));
-        st.apply = 1;
-        NK(c, launch_adam(a, st, c->stream), "nrc adam");
-    }
+    if (apply) NK(c, adam_step(c, c->stream), "nrc adam");
     float l = 0.0f;
     NK(c, cudaMemcpyAsync(&l, c->loss, 4, cudaMemcpyDeviceToHost, c->stream), "loss");
     if (grad) NK(c, cudaMemcpyAsync(grad, c->grad, PARAMS * 4, cudaMemcpyDeviceToHost, c->stream), "gradient");

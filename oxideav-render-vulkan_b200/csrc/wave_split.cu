@@ -159,6 +159,36 @@ __device__ __forceinline__ const Scene& tables_of(const WaveArgs& a) {
     return BATCH ? a.frames[0].s : a.s;
 }
 
+// Radiance-cache inputs of a vertex: position normalised to the scene's
+// root box, outgoing direction and shading normal mapped to [0, 1], GGX
+// alpha; three float4 (pos.xyz, alpha | dir.xyz, 0 | normal.xyz, 0).
+__device__ __forceinline__ void nrc_features(const Scene& s, const Vertex& vx, float4* out) {
+    float4 lo = geomv(s, 0), hi = geomv(s, 1);
+    f3 ext = mk(fmaxf(hi.x - lo.x, 1e-20f), fmaxf(hi.y - lo.y, 1e-20f), fmaxf(hi.z - lo.z, 1e-20f));
+    f3 p = vx.p;
+    const Bsdf& b = vx.bsdf;
+    out[0] = make_float4(clampf((p.x - lo.x) / ext.x, 0.0f, 1.0f), clampf((p.y - lo.y) / ext.y, 0.0f, 1.0f),
+                         clampf((p.z - lo.z) / ext.z, 0.0f, 1.0f), clampf(b.alpha, 0.0f, 1.0f));
+    out[1] = make_float4(0.5f * (b.v.x + 1.0f), 0.5f * (b.v.y + 1.0f), 0.5f * (b.v.z + 1.0f), 0.0f);
+    out[2] = make_float4(0.5f * (b.n.x + 1.0f), 0.5f * (b.n.y + 1.0f), 0.5f * (b.n.z + 1.0f), 0.0f);
+}
+
+// A finished training path: its target is the radiance gathered after the
+// recorded vertex, per unit throughput there.
+__device__ __forceinline__ void nrc_finish(const WaveArgs& a, uint32_t i, const PathCore& pc) {
+    uint32_t ti = a.nrc.s_tidx[i];
+    if (ti == NONE) return;
+    a.nrc.s_tidx[i] = NONE;
+    float4 pre = a.nrc.s_pre[i], b = a.nrc.s_beta[i];
+    f3 d = pc.radiance - xyz(pre);
+    float t[3] = {d.x, d.y, d.z}, bb[3] = {b.x, b.y, b.z};
+    for (int c = 0; c < 3; c++) {
+        float v = bb[c] > 0.0f ? t[c] / bb[c] : 0.0f;
+        t[c] = finite(v) ? fmaxf(v, 0.0f) : 0.0f;
+    }
+    a.nrc.t_target[ti] = make_float4(t[0], t[1], t[2], 1.0f);
+}
+
 }  // namespace
 
 template <bool COUNT, bool BATCH>
@@ -198,6 +228,7 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
             return;
         }
         a.out[a.st.item[i]] = path_result(pc, r != PATH_UNCOVERED);
+        if (a.nrc.on) nrc_finish(a, i, pc);
         need_new = true;
     }
     unsigned long long item = fetch1(a.work);
@@ -213,6 +244,7 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
         f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], y0 + yy, first + it, &smp, &pc);
         a.st.item[i] = item;
         if (BATCH) a.st.frame[i] = f;
+        if (a.nrc.on) a.nrc.s_tidx[i] = NONE;
         save_state(a, i, pc, smp, ST_TRACING);
         a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
         a.q.ext[append1(&a.ctr[0])] = i;
@@ -250,6 +282,34 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
         if (r != PATH_VERTEX) {
             save_state(a, i, pc, smp, ST_ENDING);
             continue;
+        }
+        if (a.nrc.on && pc.k == a.nrc.query_k) {
+            float4 f[3];
+            nrc_features(s, vx, f);
+            if ((smp.path_seed & a.nrc.train_mask) != 0u) {
+                // A rendering path ends here: the cache supplies the rest.
+                uint32_t q = atomicAdd(&a.nrc.counts[0], 1u);
+                if (q < a.nrc.q_cap) {
+                    a.nrc.q_in[3 * (size_t)q] = f[0];
+                    a.nrc.q_in[3 * (size_t)q + 1] = f[1];
+                    a.nrc.q_in[3 * (size_t)q + 2] = f[2];
+                    a.nrc.q_beta[q] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, 0.0f);
+                    a.nrc.q_item[q] = a.st.item[i];
+                }
+                a.st.nee_n[i] = 0u;
+                save_state(a, i, pc, smp, ST_ENDING);
+                continue;
+            }
+            uint32_t ti = atomicAdd(&a.nrc.counts[1], 1u);
+            if (ti < a.nrc.t_cap) {
+                a.nrc.t_in[3 * (size_t)ti] = f[0];
+                a.nrc.t_in[3 * (size_t)ti + 1] = f[1];
+                a.nrc.t_in[3 * (size_t)ti + 2] = f[2];
+                a.nrc.t_target[ti] = make_float4(0.f, 0.f, 0.f, 0.f);
+                a.nrc.s_pre[i] = make_float4(pc.radiance.x, pc.radiance.y, pc.radiance.z, 0.0f);
+                a.nrc.s_beta[i] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, 0.0f);
+                a.nrc.s_tidx[i] = ti;
+            }
         }
         uint32_t v = append1(&a.ctr[4]);
         put_vertex(a, v, vx, pc, smp.path_seed);

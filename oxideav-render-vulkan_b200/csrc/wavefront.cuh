@@ -38,6 +38,25 @@ struct BatchFrame {
     uint32_t first, y0, npix, pad;
 };
 
+// Radiance-cache frame (split plan only; `on` = 0 otherwise): paths that
+// are not training paths end at the vertex hit by ray `query_k` with a
+// cache query (features, throughput, result index); training paths (path
+// seed & train_mask == 0) continue to the end and record, at that vertex,
+// the inputs and, when they finish, the radiance they gathered from there
+// on divided by their throughput there: the cache's target.
+struct NrcWave {
+    uint32_t on, query_k, train_mask, q_cap, t_cap, pad0, pad1, pad2;
+    uint32_t* counts;              // [0] queries, [1] training samples
+    float4* q_in;                  // q_cap x 3 float4 inputs
+    float4* q_beta;                // throughput at the query vertex
+    unsigned long long* q_item;    // path result index
+    float4* t_in;                  // t_cap x 3 float4 inputs
+    float4* t_target;              // rgb target per training sample
+    float4* s_pre;                 // per slot: radiance before the training vertex's reflected light
+    float4* s_beta;                // per slot: throughput at the training vertex
+    uint32_t* s_tidx;              // per slot: training sample index, or 0xffffffff
+};
+
 struct WaveQueues {
     uint32_t* ext;  // slot ids with a continuation ray
     float4* sh_o;   // shadow ray origin, t_max
@@ -69,6 +88,7 @@ struct WaveArgs {
     // count of the frames and out is indexed by launch item.
     const BatchFrame* frames;
     uint32_t nframes;
+    NrcWave nrc;
 };
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3

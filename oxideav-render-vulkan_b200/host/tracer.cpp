@@ -12,6 +12,7 @@
 
 #include "../../include/oxpt_batch.h"
 #include "../../include/oxpt_serve.h"
+#include "../../include/oxpt_nrc.h"
 #include "model.hpp"
 
 namespace {
@@ -288,6 +289,19 @@ oxpt_status oxpt_tracers_refine_batch(oxpt_tracer* const* ts, uint32_t count, co
         return st;
     }
     for (uint32_t k = 0; k < count; k++) ts[k]->samples += adds[k];
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_tracer_refine_nrc(oxpt_tracer* t, oxpt_nrc* nrc, uint32_t frames, const oxpt_nrc_config* cfg,
+                                   float* loss) {
+    if (!t || !nrc || !cfg) return OXPT_E_INVALID;
+    if (!t->scene || frames == 0) return OXPT_OK;
+    frames = std::min(frames, 0xffffffffu - t->samples);
+    oxpt_status st = t->ensure_binding();
+    if (st) return st;
+    st = t->check(oxpt_nrc_refine(nrc, t->ctx, t->samples, frames, cfg, loss));
+    if (st) return st;
+    t->samples += frames;
     return OXPT_OK;
 }
 

@@ -118,3 +118,68 @@ def test_online_training_reduces_the_loss(cache):
     t = _target(x)
     rel = np.mean((out[:, :3] - t[:, :3]) ** 2 / (t[:, :3] ** 2 + 0.01))
     assert rel < 0.02, rel
+
+
+# ---------------------------------------------------------------------
+# Cache frames on the path tracer.
+# ---------------------------------------------------------------------
+
+import scenes  # noqa: E402
+
+
+def _tracer(pkg, w=96, h=64, bounces=8):
+    t = pkg.GpuPathTracer(0)
+    t.sync(scenes.materials_scene(pkg),
+           pkg.RenderOptions(width=w, height=h,
+                             path_trace=pkg.PathTraceOptions(samples_per_pixel=64, max_bounces=bounces)))
+    return t
+
+
+def test_zero_cache_ends_paths_exactly_at_the_query_bounce(pkg, oracle):
+    """With a cache that predicts zero and no training paths, a cache
+    frame is the plain tracer cut after two bounces (keeping the emission
+    of the vertex where it stops): bit for bit, against the oracle too."""
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg)
+    cache = RadianceCache(t)
+    cache.set_weights(np.zeros(nrc.PARAMS, np.float32))
+    cache.configure(train_one_in=1 << 31, train=0)
+    cache.refine(3)
+    assert t.samples() == 3
+    got = t.read_accum()
+    cut = _tracer(pkg, bounces=2)
+    cut.refine(3)
+    assert np.array_equal(got.view(np.uint32), cut.read_accum().view(np.uint32))
+    cpu, _ = oracle.render(cut.prepared(), 3)
+    assert np.array_equal(got.view(np.uint32), cpu.view(np.uint32))
+    q, s = cache.frame_counts()
+    assert q > 0 and s == 0
+
+
+def test_training_paths_are_the_plain_tracer(pkg):
+    """When every path is a training path nothing is cut: the frames equal
+    the plain tracer's, and the paths that reach the query vertex become
+    training samples."""
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg)
+    cache = RadianceCache(t)
+    cache.configure(train_one_in=1, train=0, max_train=1 << 20)
+    cache.refine(2)
+    plain = _tracer(pkg)
+    plain.refine(2)
+    assert np.array_equal(t.read_accum().view(np.uint32), plain.read_accum().view(np.uint32))
+    q, s = cache.frame_counts()
+    assert q == 0 and s > 1000
+
+
+def test_cache_frames_train_online(pkg):
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg, 128, 96)
+    cache = RadianceCache(t)
+    losses = [cache.refine(1, loss=True) for _ in range(60)]
+    assert np.isfinite(losses).all()
+    assert np.mean(losses[-10:]) < np.mean(losses[:3]), losses
+    q, s = cache.frame_counts()
+    assert q > 0 and 0 < s <= 65536
+    img = t.read_accum()
+    assert np.isfinite(img).all() and t.samples() == 60
