@@ -27,8 +27,10 @@ typedef struct oxpt_nrc oxpt_nrc;
 #define OXPT_NRC_PARAMS 29696u /* FP32 weights: 64x256, 3 x 64x64, 16x64 (rows 3..15 unused), row-major */
 #define OXPT_NRC_INPUTS 12u    /* floats per sample: pos.xyz, roughness, dir.xyz, 0, normal.xyz, 0 */
 
-/* A cache on `ctx`'s device and stream, weights initialised from `seed`
- * (uniform He initialisation), Adam state zero. */
+/* A cache on `ctx`'s device, weights initialised from `seed` (uniform He
+ * initialisation), Adam state zero. It has its own stream for the calls
+ * below that take host buffers; cache frames (oxpt_nrc_refine) run on the
+ * rendering context's stream. It may outlive `ctx`. */
 oxpt_status oxpt_nrc_create(oxpt_ctx* ctx, uint64_t seed, oxpt_nrc** out);
 void oxpt_nrc_destroy(oxpt_nrc* nrc);
 const char* oxpt_nrc_last_error(const oxpt_nrc* nrc);

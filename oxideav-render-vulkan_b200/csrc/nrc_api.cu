@@ -119,8 +119,10 @@ oxpt_status oxpt_nrc_create(oxpt_ctx* ctx, uint64_t seed, oxpt_nrc** out) {
     auto* c = new oxpt_nrc();
     c->ctx = ctx;
     c->device = oxpt_ctx_device(ctx);
-    c->stream = (cudaStream_t)oxpt_get_stream(ctx);
-    if (cudaSetDevice(c->device) != cudaSuccess) {
+    // Its own stream for the host-buffer calls: the cache may outlive the
+    // context it was made on (cache frames run on the rendering context's).
+    if (cudaSetDevice(c->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return OXPT_E_NODEV;
     }
@@ -163,7 +165,10 @@ oxpt_status oxpt_nrc_create(oxpt_ctx* ctx, uint64_t seed, oxpt_nrc** out) {
 void oxpt_nrc_destroy(oxpt_nrc* c) {
     if (!c) return;
     cudaSetDevice(c->device);
-    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
     void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->loss, c->wf, c->wt, c->err_dev,
                     c->in, c->pred, c->target, c->acts, c->dy, c->counts, c->q_in, c->q_beta, c->q_item,
                     c->t_in, c->t_target, c->s_pre, c->s_beta, c->s_tidx};

@@ -11,7 +11,7 @@
 struct oxpt_nrc {
     oxpt_ctx* ctx = nullptr;
     int device = 0, sms = 1;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // owned: host-buffer calls
     std::string err;
     float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *loss = nullptr;
     uint16_t *wf = nullptr, *wt = nullptr;
