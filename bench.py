@@ -74,7 +74,9 @@ def parse():
     ap.add_argument("--spp-scale", type=int, default=16,
                     help="serve workload: spp targets {4..1024} divided by this (one GPU cannot keep up with the "
                          "full stream)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve"],
+    ap.add_argument("--frames", type=int, default=512, help="nrc workload: frames of 1 spp")
+    ap.add_argument("--ref-spp", type=int, default=16384, help="nrc workload: spp of the plain reference")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve", "nrc"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
     ap.add_argument("--scenes", type=int, default=64, help="batch workload: number of scenes")
@@ -452,8 +454,110 @@ def run_serve(a):
     print(json.dumps(line), flush=True)
 
 
+def _psnr(a, b):
+    d = a[..., :3].astype(np.float64) - b[..., :3].astype(np.float64)
+    mse = float(np.mean(d * d))
+    return float("inf") if mse == 0 else 10.0 * np.log10(255.0 * 255.0 / mse)
+
+
+def _hdr_mean(t):
+    acc = t.read_accum()
+    return acc[..., :3] / np.maximum(acc[..., 3:4], 1.0)
+
+
+def run_nrc(a):
+    """Radiance-cache frames against the plain tracer on the large scene with
+    the mixed materials: 1 spp per frame, PSNR (RGBA8 images) and relative
+    MSE (HDR) against a high-spp plain reference after each doubling of the
+    frame count, and each method's wall time to reach 35 dB."""
+    import torch
+    torch.cuda.set_device(0)
+    __graft_entry__.build()
+    pkg = __graft_entry__.load_package()
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    scene = pkg.Scene.icosphere(freq=a.freq, seed=1, n_materials=64, n_textures=8, tex_size=a.tex, n_punctual=16,
+                                n_emissive=512, material_mix=1)
+    env = pkg.EnvironmentMap.sky(1024, 512, sun_dir=(0.3, 0.8, -0.5), sun_radiance=2000.0)
+
+    def tracer():
+        t = pkg.GpuPathTracer(0)
+        t.set_environment(env)
+        t.sync(scene, pkg.RenderOptions(width=a.width, height=a.height, scene_camera=0,
+                                        path_trace=pkg.PathTraceOptions(samples_per_pixel=a.ref_spp, max_bounces=12,
+                                                                        rr_start=3)))
+        t.set_tuning(mode=2)
+        t.prepared()
+        return t
+
+    ref = tracer()
+    t0 = time.perf_counter()
+    done = 0
+    while done < a.ref_spp:
+        n = min(256, a.ref_spp - done)
+        ref.refine(n)
+        done += n
+    ref.finish()
+    ref_s = time.perf_counter() - t0
+    ref_img, ref_hdr = ref.image(), _hdr_mean(ref)
+    del ref
+
+    checkpoints = [1 << k for k in range(20) if (1 << k) <= a.frames]
+
+    def progress(t, step):
+        out, wall, frames = [], 0.0, 0
+        for c in checkpoints:
+            t0 = time.perf_counter()
+            step(c - frames)
+            t.finish()
+            wall += time.perf_counter() - t0
+            frames = c
+            img = t.image()
+            hdr = _hdr_mean(t)
+            out.append({"frames": c, "seconds": wall, "psnr_db": _psnr(img, ref_img),
+                        "rel_mse": float(np.mean((hdr - ref_hdr) ** 2 / (ref_hdr ** 2 + 0.01)))})
+        return out
+
+    plain = tracer()
+    plain_curve = progress(plain, lambda n: plain.refine(n))
+    del plain
+    nt = tracer()
+    cache = RadianceCache(nt)
+    nrc_curve = progress(nt, lambda n: cache.refine(n))
+    q, smp = cache.frame_counts()
+
+    def time_to(curve, db):
+        prev = None
+        for p in curve:
+            if p["psnr_db"] >= db:
+                if prev is None:
+                    return p["seconds"]
+                f = (db - prev["psnr_db"]) / max(p["psnr_db"] - prev["psnr_db"], 1e-9)
+                return prev["seconds"] + f * (p["seconds"] - prev["seconds"])
+            prev = p
+        return None
+
+    tp, tn = time_to(plain_curve, 35.0), time_to(nrc_curve, 35.0)
+    frame_ms = lambda c: 1e3 * c[-1]["seconds"] / c[-1]["frames"]
+    line = {"metric": "seconds to 35 dB PSNR", "value": tn, "unit": "s", "n_gpus": 1, "steps": a.frames,
+            "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
+            "data": "synthetic",
+            "config": {"workload": "radiance cache: large scene (20 x freq^2 triangles) with the mixed material model, "
+                                   f"{a.width}x{a.height}, 1 spp per frame, {a.frames} frames, 12 bounces",
+                       "reference": f"plain tracer {a.ref_spp} spp ({ref_s:.1f} s)",
+                       "cache": "5 x 64 ReLU MLP, BF16 tcgen05, 12-frequency encoding, paths end after 2 bounces, "
+                                "1 in 16 paths trains, <= 65536 samples and one Adam step (lr 1e-2) per frame"},
+            "plain_seconds_to_35db": tp, "ratio_to_plain": (tn / tp) if (tn and tp) else None,
+            "plain_ms_per_frame": frame_ms(plain_curve), "cache_ms_per_frame": frame_ms(nrc_curve),
+            "plain": plain_curve, "cache": nrc_curve,
+            "last_frame_queries": q, "last_frame_training_samples": smp}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
+    if a.workload == "nrc":
+        run_nrc(a)
+        return
     if a.workload == "serve":
         run_serve(a)
         return
