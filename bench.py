@@ -518,6 +518,7 @@ def run_nrc(a):
         return out
 
     plain = tracer()
+    plain.set_tuning(wave_slots=1 << 21, graphs=1)  # the plain tracer's best 1-spp plan
     plain_curve = progress(plain, lambda n: plain.refine(n))
     del plain
     nt = tracer()

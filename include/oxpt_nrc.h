@@ -61,6 +61,10 @@ oxpt_status oxpt_nrc_train(oxpt_nrc* nrc, const float* inputs, const float* targ
  * radiance it gathered from there on per unit throughput. After a frame's
  * results are reduced into the accumulator, the cache takes one Adam step
  * on that frame's samples (at most `max_train`) when `train` is set.
+ * With `train_suffix` > 0 a training path ends into the cache that many
+ * bounces after the query vertex and its target adds the cache's
+ * prediction there (self-training, which keeps every path short). All of
+ * a frame's paths are in flight at once (one wavefront slot per pixel).
  * `enabled` = 0 renders plain frames (the ablation). The frame must fit
  * one launch of the context's plan (width x height <= its items per
  * launch).
@@ -71,9 +75,11 @@ typedef struct oxpt_nrc_config {
     uint32_t train_one_in;  /* a power of two */
     uint32_t max_train;
     uint32_t train;
-    uint32_t reserved[3];
+    uint32_t train_suffix;  /* training paths end into the cache this many bounces after the
+                               query vertex (self-training); 0 = they run to the end */
+    uint32_t reserved[2];
 } oxpt_nrc_config;
-void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1 */
+void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1, 4 */
 
 /* `count` cache frames with sample indices first_sample.. on `ctx`'s
  * accumulator; *loss (optional, waits for the GPU) = the last frame's mean

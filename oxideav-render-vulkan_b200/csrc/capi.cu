@@ -1456,6 +1456,7 @@ void oxpt_nrc_config_default(oxpt_nrc_config* cfg) {
     cfg->train_one_in = 16;
     cfg->max_train = 65536;
     cfg->train = 1;
+    cfg->train_suffix = 4;
 }
 
 }  // extern "C"
@@ -1478,16 +1479,18 @@ oxpt_status nrc_buffers(oxpt_ctx* c, oxpt_nrc* r, size_t q, size_t t, size_t slo
     size_t dummy = 0;
     if (!r->counts && (s = grow(c, &r->counts, &dummy, 2, 1, "cache counters"))) return s;
     if (q > r->q_cap) {
-        size_t c1 = 0, c2 = 0, c3 = 0;
+        size_t c1 = 0, c2 = 0, c3 = 0, c4 = 0;
         if ((s = grow(c, &r->q_in, &c1, q, 3, "cache queries"))) return s;
         if ((s = grow(c, &r->q_beta, &c2, q, 1, "cache queries"))) return s;
         if ((s = grow(c, &r->q_item, &c3, q, 1, "cache queries"))) return s;
+        if ((s = grow(c, &r->q_pred, &c4, q, 1, "cache queries"))) return s;
         r->q_cap = q;
     }
     if (t > r->t_cap) {
-        size_t c1 = 0, c2 = 0;
+        size_t c1 = 0, c2 = 0, c3 = 0;
         if ((s = grow(c, &r->t_in, &c1, t, 3, "cache training samples"))) return s;
         if ((s = grow(c, &r->t_target, &c2, t, 1, "cache training samples"))) return s;
+        if ((s = grow(c, &r->t_tail, &c3, t, 1, "cache training samples"))) return s;
         r->t_cap = t;
     }
     if (slots > r->s_cap) {
@@ -1520,13 +1523,16 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
     if ((s = ready(c))) return s;
     const uint64_t npix = (uint64_t)c->w * c->h;
     if (npix > c->wave_items) return fail(c, OXPT_E_LIMIT, "a cache frame must fit one launch (width x height <= wave_items)");
-    const uint32_t P = (uint32_t)std::min<uint64_t>(npix, c->wave_slots);
+    const uint32_t P = (uint32_t)npix;  // every path of the frame in flight at once
     const uint32_t max_train = std::max(cfg->max_train, 1u);
+    if (cfg->train_suffix && cfg->query_bounce + cfg->train_suffix < cfg->query_bounce)
+        return fail(c, OXPT_E_INVALID, "train_suffix too large");
     if ((s = nrc_buffers(c, r, npix, max_train, P))) return s;
     if ((s = oxd::nrc::ensure_scratch(r, max_train))) return s;
     if ((s = ensure_out(c, npix))) return s;
-    uint32_t saved_mode = c->mode;
+    uint32_t saved_mode = c->mode, saved_slots = c->wave_slots;
     c->mode = OXPT_MODE_WAVEFRONT_SPLIT;
+    c->wave_slots = std::max<uint32_t>(c->wave_slots, P);
     for (uint32_t i = 0; i < count && !s; i++) {
         cudaError_t ce = cudaMemsetAsync(r->counts, 0, 8, c->stream);
         if (ce) {
@@ -1559,6 +1565,8 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         nw.s_pre = r->s_pre;
         nw.s_beta = r->s_beta;
         nw.s_tidx = r->s_tidx;
+        nw.t_tail = r->t_tail;
+        nw.tail_k = cfg->train_suffix ? cfg->query_bounce + cfg->train_suffix : 0xffffffffu;
         if ((s = run_wave(c, ta, false, &nw))) break;
         // The cache's predictions complete the rendering paths.
         oxd::nrc::Args a = oxd::nrc::base_args(r);
@@ -1568,6 +1576,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         a.query_beta = r->q_beta;
         a.query_item = r->q_item;
         a.query_out = c->out;
+        a.pred = r->q_pred;
         if ((ce = oxd::nrc::launch_forward(a, c->sms, c->stream))) {
             s = cuda_fail(c, ce, "cache inference");
             break;
@@ -1589,6 +1598,9 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
             b.acts = r->acts;
             b.dy = r->dy;
             b.grad_scale = 0.0f;
+            if (!ce && cfg->train_suffix)
+                ce = oxd::nrc::launch_tail_targets(r->counts, max_train, (uint32_t)npix, r->t_tail, r->q_pred,
+                                                   r->t_target, c->stream);
             if (!ce) ce = oxd::nrc::launch_forward(b, c->sms, c->stream);
             if (!ce) ce = oxd::nrc::launch_backward(b, c->sms, c->stream);
             if (!ce) ce = oxd::nrc::adam_step(r, c->stream);
@@ -1600,6 +1612,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         }
     }
     c->mode = saved_mode;
+    c->wave_slots = saved_slots;
     if (s) return s;
     if (loss) {
         float l = 0.0f;

@@ -393,6 +393,29 @@ __global__ void nrc_adam(const __grid_constant__ Args a, AdamStep st) {
     publish_weight(a, i, w);
 }
 
+// Targets of training samples whose suffix ended into the cache: add the
+// cache's (non-negative) prediction there times the throughput ratio.
+__global__ void nrc_tail_targets(const uint32_t* counts, uint32_t t_cap, uint32_t q_cap, const uint4* tail,
+                                 const float4* pred, float4* target) {
+    uint32_t n = counts[1] < t_cap ? counts[1] : t_cap;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint4 t = tail[i];
+    if (t.x == 0xffffffffu || t.x >= q_cap) return;
+    float4 p = pred[t.x], g = target[i];
+    g.x += __uint_as_float(t.y) * fmaxf(p.x, 0.0f);
+    g.y += __uint_as_float(t.z) * fmaxf(p.y, 0.0f);
+    g.z += __uint_as_float(t.w) * fmaxf(p.z, 0.0f);
+    target[i] = g;
+}
+
+cudaError_t launch_tail_targets(const uint32_t* counts, uint32_t t_cap, uint32_t q_cap, const uint4* tail,
+                                const float4* pred, float4* target, cudaStream_t st) {
+    if (t_cap == 0) return cudaSuccess;
+    nrc_tail_targets<<<(t_cap + 255) / 256, 256, 0, st>>>(counts, t_cap, q_cap, tail, pred, target);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_forward(const Args& a, int sms, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {

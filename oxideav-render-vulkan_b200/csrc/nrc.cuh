@@ -69,6 +69,8 @@ struct AdamStep {
 cudaError_t launch_forward(const Args& a, int sms, cudaStream_t st);
 cudaError_t launch_backward(const Args& a, int sms, cudaStream_t st);
 cudaError_t launch_adam(const Args& a, const AdamStep& s, cudaStream_t st);
+cudaError_t launch_tail_targets(const uint32_t* counts, uint32_t t_cap, uint32_t q_cap, const uint4* tail,
+                                const float4* pred, float4* target, cudaStream_t st);
 
 }  // namespace nrc
 }  // namespace oxd

@@ -27,7 +27,9 @@ struct oxpt_nrc {
     unsigned long long* q_item = nullptr;
     size_t q_cap = 0;
     float4 *t_in = nullptr, *t_target = nullptr;
+    uint4* t_tail = nullptr;
     size_t t_cap = 0;
+    float4* q_pred = nullptr;
     float4 *s_pre = nullptr, *s_beta = nullptr;
     uint32_t* s_tidx = nullptr;
     size_t s_cap = 0;

@@ -283,6 +283,30 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
             save_state(a, i, pc, smp, ST_ENDING);
             continue;
         }
+        if (a.nrc.on && pc.k == a.nrc.tail_k && (smp.path_seed & a.nrc.train_mask) == 0u) {
+            // A training path's suffix ends here, into the cache.
+            float4 f[3];
+            nrc_features(s, vx, f);
+            uint32_t q = atomicAdd(&a.nrc.counts[0], 1u);
+            if (q < a.nrc.q_cap) {
+                a.nrc.q_in[3 * (size_t)q] = f[0];
+                a.nrc.q_in[3 * (size_t)q + 1] = f[1];
+                a.nrc.q_in[3 * (size_t)q + 2] = f[2];
+                a.nrc.q_beta[q] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, 0.0f);
+                a.nrc.q_item[q] = a.st.item[i];
+                uint32_t ti = a.nrc.s_tidx[i];
+                if (ti != NONE) {
+                    float4 b0 = a.nrc.s_beta[i];
+                    float rx = b0.x > 0.0f ? pc.beta.x / b0.x : 0.0f;
+                    float ry = b0.y > 0.0f ? pc.beta.y / b0.y : 0.0f;
+                    float rz = b0.z > 0.0f ? pc.beta.z / b0.z : 0.0f;
+                    a.nrc.t_tail[ti] = make_uint4(q, __float_as_uint(rx), __float_as_uint(ry), __float_as_uint(rz));
+                }
+            }
+            a.st.nee_n[i] = 0u;
+            save_state(a, i, pc, smp, ST_ENDING);
+            continue;
+        }
         if (a.nrc.on && pc.k == a.nrc.query_k) {
             float4 f[3];
             nrc_features(s, vx, f);
@@ -306,6 +330,7 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
                 a.nrc.t_in[3 * (size_t)ti + 1] = f[1];
                 a.nrc.t_in[3 * (size_t)ti + 2] = f[2];
                 a.nrc.t_target[ti] = make_float4(0.f, 0.f, 0.f, 0.f);
+                a.nrc.t_tail[ti] = make_uint4(NONE, 0u, 0u, 0u);
                 a.nrc.s_pre[i] = make_float4(pc.radiance.x, pc.radiance.y, pc.radiance.z, 0.0f);
                 a.nrc.s_beta[i] = make_float4(pc.beta.x, pc.beta.y, pc.beta.z, 0.0f);
                 a.nrc.s_tidx[i] = ti;

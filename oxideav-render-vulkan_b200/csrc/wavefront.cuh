@@ -44,8 +44,11 @@ struct BatchFrame {
 // seed & train_mask == 0) continue to the end and record, at that vertex,
 // the inputs and, when they finish, the radiance they gathered from there
 // on divided by their throughput there: the cache's target.
+// Training paths end into the cache too, at the vertex hit by ray tail_k
+// (0xffffffff: never): their target then adds the cache's prediction there
+// (scaled by the throughput ratio), filled in after inference.
 struct NrcWave {
-    uint32_t on, query_k, train_mask, q_cap, t_cap, pad0, pad1, pad2;
+    uint32_t on, query_k, train_mask, q_cap, t_cap, tail_k, pad1, pad2;
     uint32_t* counts;              // [0] queries, [1] training samples
     float4* q_in;                  // q_cap x 3 float4 inputs
     float4* q_beta;                // throughput at the query vertex
@@ -55,6 +58,7 @@ struct NrcWave {
     float4* s_pre;                 // per slot: radiance before the training vertex's reflected light
     float4* s_beta;                // per slot: throughput at the training vertex
     uint32_t* s_tidx;              // per slot: training sample index, or 0xffffffff
+    uint4* t_tail;                 // per training sample: tail query, throughput ratio (float bits)
 };
 
 struct WaveQueues {

@@ -163,7 +163,7 @@ def test_training_paths_are_the_plain_tracer(pkg):
     from oxideav_render_vulkan_b200.nrc import RadianceCache
     t = _tracer(pkg)
     cache = RadianceCache(t)
-    cache.configure(train_one_in=1, train=0, max_train=1 << 20)
+    cache.configure(train_one_in=1, train=0, max_train=1 << 20, train_suffix=0)
     cache.refine(2)
     plain = _tracer(pkg)
     plain.refine(2)
