@@ -76,6 +76,8 @@ def parse():
                          "full stream)")
     ap.add_argument("--frames", type=int, default=512, help="nrc workload: frames of 1 spp")
     ap.add_argument("--ref-spp", type=int, default=16384, help="nrc workload: spp of the plain reference")
+    ap.add_argument("--nrc-scene", default="large", choices=["large", "cornell"], help="nrc workload: scene")
+    ap.add_argument("--nrc-train-one-in", type=int, default=4, help="nrc workload: one training path in this many")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve", "nrc"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
@@ -475,13 +477,17 @@ def run_nrc(a):
     __graft_entry__.build()
     pkg = __graft_entry__.load_package()
     from oxideav_render_vulkan_b200.nrc import RadianceCache
-    scene = pkg.Scene.icosphere(freq=a.freq, seed=1, n_materials=64, n_textures=8, tex_size=a.tex, n_punctual=16,
-                                n_emissive=512, material_mix=1)
-    env = pkg.EnvironmentMap.sky(1024, 512, sun_dir=(0.3, 0.8, -0.5), sun_radiance=2000.0)
+    if a.nrc_scene == "cornell":
+        scene, env = pkg.Scene.cornell(), None
+    else:
+        scene = pkg.Scene.icosphere(freq=a.freq, seed=1, n_materials=64, n_textures=8, tex_size=a.tex,
+                                    n_punctual=16, n_emissive=512, material_mix=1)
+        env = pkg.EnvironmentMap.sky(1024, 512, sun_dir=(0.3, 0.8, -0.5), sun_radiance=2000.0)
 
     def tracer():
         t = pkg.GpuPathTracer(0)
-        t.set_environment(env)
+        if env is not None:
+            t.set_environment(env)
         t.sync(scene, pkg.RenderOptions(width=a.width, height=a.height, scene_camera=0,
                                         path_trace=pkg.PathTraceOptions(samples_per_pixel=a.ref_spp, max_bounces=12,
                                                                         rr_start=3)))
@@ -504,6 +510,11 @@ def run_nrc(a):
     checkpoints = [1 << k for k in range(20) if (1 << k) <= a.frames]
 
     def progress(t, step):
+        # one untimed frame first: allocations of the plan (and of the
+        # cache's buffers) are not part of the comparison
+        step(1)
+        t.finish()
+        t.reset()
         out, wall, frames = [], 0.0, 0
         for c in checkpoints:
             t0 = time.perf_counter()
@@ -523,6 +534,7 @@ def run_nrc(a):
     del plain
     nt = tracer()
     cache = RadianceCache(nt)
+    cache.configure(train_one_in=a.nrc_train_one_in)
     nrc_curve = progress(nt, lambda n: cache.refine(n))
     q, smp = cache.frame_counts()
 
@@ -542,11 +554,14 @@ def run_nrc(a):
     line = {"metric": "seconds to 35 dB PSNR", "value": tn, "unit": "s", "n_gpus": 1, "steps": a.frames,
             "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
             "data": "synthetic",
-            "config": {"workload": "radiance cache: large scene (20 x freq^2 triangles) with the mixed material model, "
-                                   f"{a.width}x{a.height}, 1 spp per frame, {a.frames} frames, 12 bounces",
+            "config": {"workload": ("radiance cache: procedural Cornell box" if a.nrc_scene == "cornell" else
+                                    "radiance cache: large scene (20 x freq^2 triangles) with the mixed material model")
+                                   + f", {a.width}x{a.height}, 1 spp per frame, {a.frames} frames, 12 bounces",
                        "reference": f"plain tracer {a.ref_spp} spp ({ref_s:.1f} s)",
                        "cache": "5 x 64 ReLU MLP, BF16 tcgen05, 12-frequency encoding, paths end after 2 bounces, "
-                                "1 in 16 paths trains, <= 65536 samples and one Adam step (lr 1e-2) per frame"},
+                                f"1 in {a.nrc_train_one_in} paths trains (suffix of 4 bounces into the cache), "
+                                "<= 65536 samples and one Adam step (lr 1e-2) per frame",
+                       "timing": "host wall clock with a device sync per checkpoint; one untimed frame first"},
             "plain_seconds_to_35db": tp, "ratio_to_plain": (tn / tp) if (tn and tp) else None,
             "plain_ms_per_frame": frame_ms(plain_curve), "cache_ms_per_frame": frame_ms(nrc_curve),
             "plain": plain_curve, "cache": nrc_curve,
