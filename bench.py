@@ -686,7 +686,7 @@ def main():
     # region / its summed CUDA-event time (kernel launches on the tracer's
     # stream), against the measured HBM copy bandwidth.
     peak, peak_kind = measured_peak()
-    kms, kn = (C.c_double * 8)(), (C.c_uint64 * 8)()
+    kms, kn = (C.c_double * 12)(), (C.c_uint64 * 12)()
     L.oxpt_diag_timing_kinds(pt.ctx, kms, kn)
     kernel_timing = "timed region"
     if pt.tuning().graphs:

@@ -69,8 +69,9 @@ oxpt_status oxpt_diag_timing(oxpt_ctx* ctx, double* trace_ms, uint64_t* trace_la
  * phase of each launch (the megakernel, or a whole wavefront run), 1 the
  * ordered reduce, 2 wavefront logic, 3 wavefront extension traversal, 4
  * wavefront shadow traversal, 5 split-wavefront shading, 6 split-wavefront
- * NEE. */
-oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* ctx, double ms[8], uint64_t n[8]);
+ * NEE, 7 radiance-cache inference, 8 cache training forward, 9 cache
+ * backward; 10, 11 unused. */
+oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* ctx, double ms[12], uint64_t n[12]);
 /* The last oxpt_diag_refine_counted totals split by ray kind: out[0..7] for
  * continuation rays and shading (wavefront logic + extension), out[8..15]
  * for shadow rays (wavefront shadow kernel); the megakernel reports all in

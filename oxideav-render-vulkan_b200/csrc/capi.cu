@@ -76,8 +76,8 @@ struct oxpt_ctx {
         int kind;
     };
     std::vector<Timed> timed;
-    double kind_ms[8] = {0}, last_ms[8] = {0};
-    uint64_t kind_n[8] = {0}, last_n[8] = {0};
+    double kind_ms[12] = {0}, last_ms[12] = {0};
+    uint64_t kind_n[12] = {0}, last_n[12] = {0};
     uint64_t split_counts[2 * oxd::C_N] = {0};
     // execution mode: megakernel or wavefront, and the wavefront's buffers
     uint32_t mode = OXPT_MODE_WAVEFRONT;
@@ -1108,16 +1108,16 @@ oxpt_status oxpt_diag_timing(oxpt_ctx* c, double* trace_ms, uint64_t* trace_n, d
     if (reduce_n) *reduce_n = c->kind_n[1];
     std::memcpy(c->last_ms, c->kind_ms, sizeof(c->last_ms));
     std::memcpy(c->last_n, c->kind_n, sizeof(c->last_n));
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < 12; k++) {
         c->kind_ms[k] = 0.0;
         c->kind_n[k] = 0;
     }
     return OXPT_OK;
 }
 
-oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* c, double ms[8], uint64_t n[8]) {
+oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* c, double ms[12], uint64_t n[12]) {
     if (!c || !ms || !n) return OXPT_E_INVALID;
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < 12; k++) {
         ms[k] = c->last_ms[k];
         n[k] = c->last_n[k];
     }
@@ -1507,6 +1507,27 @@ oxpt_status nrc_buffers(oxpt_ctx* c, oxpt_nrc* r, size_t q, size_t t, size_t slo
 
 extern "C" {
 
+}  // extern "C"
+
+// Per-launch event pair of kind `kind` around `launch` when timing is on.
+template <class F>
+static cudaError_t timed_launch(oxpt_ctx* c, int kind, F&& launch) {
+    oxpt_ctx::Timed t{nullptr, nullptr, kind};
+    if (c->timing) {
+        cudaEventCreate(&t.a);
+        cudaEventCreate(&t.b);
+        cudaEventRecord(t.a, c->stream);
+    }
+    cudaError_t e = launch();
+    if (c->timing) {
+        cudaEventRecord(t.b, c->stream);
+        c->timed.push_back(t);
+    }
+    return e;
+}
+
+extern "C" {
+
 oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t count, const oxpt_nrc_config* cfg,
                             float* loss) {
     if (!r || !c || !cfg) return fail(c, OXPT_E_INVALID, "null argument");
@@ -1577,7 +1598,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         a.query_item = r->q_item;
         a.query_out = c->out;
         a.pred = r->q_pred;
-        if ((ce = oxd::nrc::launch_forward(a, c->sms, c->stream))) {
+        if ((ce = timed_launch(c, 7, [&] { return oxd::nrc::launch_forward(a, c->sms, c->stream); }))) {
             s = cuda_fail(c, ce, "cache inference");
             break;
         }
@@ -1601,8 +1622,8 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
             if (!ce && cfg->train_suffix)
                 ce = oxd::nrc::launch_tail_targets(r->counts, max_train, (uint32_t)npix, r->t_tail, r->q_pred,
                                                    r->t_target, c->stream);
-            if (!ce) ce = oxd::nrc::launch_forward(b, c->sms, c->stream);
-            if (!ce) ce = oxd::nrc::launch_backward(b, c->sms, c->stream);
+            if (!ce) ce = timed_launch(c, 8, [&] { return oxd::nrc::launch_forward(b, c->sms, c->stream); });
+            if (!ce) ce = timed_launch(c, 9, [&] { return oxd::nrc::launch_backward(b, c->sms, c->stream); });
             if (!ce) ce = oxd::nrc::adam_step(r, c->stream);
             if (ce) {
                 s = cuda_fail(c, ce, "cache training");
