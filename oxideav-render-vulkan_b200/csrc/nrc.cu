@@ -21,8 +21,11 @@
 //                 gradient.
 //   nrc_backward  propagates the gradient down the layers with tcgen05
 //                 (delta_{l-1} = delta_l x W_l through W_l^T, masked by
-//                 ReLU) and accumulates the weight gradients delta^T x a
-//                 on the CUDA cores, one atomic add per weight per tile.
+//                 ReLU) and accumulates the weight gradients a^T x delta
+//                 with tcgen05 too, in TMEM across all of the CTA's tiles
+//                 (512 columns: one accumulator per layer); each CTA then
+//                 writes one row of partial sums and nrc_grad_reduce adds
+//                 the rows in CTA order (no atomics, deterministic).
 //   nrc_adam      Adam on the FP32 master weights; rewrites the BF16
 //                 operand copies (forward and transposed layouts).
 #include <cuda_bf16.h>
@@ -46,12 +49,12 @@ constexpr uint32_t FWD_H = FWD_A0 + TILE * IN * 2;  // 128 x 64 hidden
 constexpr uint32_t FWD_BAR = FWD_H + TILE * HID * 2;
 constexpr uint32_t FWD_SMEM = FWD_BAR + 64;
 
-constexpr uint32_t BWD_WT = 0;                            // transposed weights, layers 1..4
-constexpr uint32_t BWD_GCM = BWD_WT + WT_BYTES;           // gradient operand, 128 x 64 bf16
-constexpr uint32_t BWD_G = BWD_GCM + TILE * HID * 2;      // gradient rows, 128 x 64 fp32
-constexpr uint32_t BWD_ACT = BWD_G + TILE * HID * 4;      // layer input rows, 128 x 64 bf16
-constexpr uint32_t BWD_A0 = BWD_ACT + TILE * HID * 2;     // encoded inputs, 128 x 256 bf16
-constexpr uint32_t BWD_BAR = BWD_A0 + TILE * IN * 2;
+constexpr uint32_t BWD_WT = 0;                             // transposed weights, layers 1..4
+constexpr uint32_t BWD_GCM = BWD_WT + WT_BYTES;            // gradient operand: rows = samples, 128 x 64
+constexpr uint32_t BWD_GT = BWD_GCM + TILE * HID * 2;      // gradient^T operand: rows = outputs, 64 x 128
+constexpr uint32_t BWD_ACTT = BWD_GT + HID * TILE * 2;     // h^T operand: rows = features, 128 (64 used) x 128
+constexpr uint32_t BWD_A0T = BWD_ACTT + TILE * TILE * 2;   // encoded inputs^T: 2 x (128 features x 128)
+constexpr uint32_t BWD_BAR = BWD_A0T + 2 * TILE * TILE * 2;
 constexpr uint32_t BWD_SMEM = BWD_BAR + 64;
 
 constexpr uint32_t WAIT_LIMIT = 1u << 26;
@@ -247,112 +250,147 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
     if (t < 32) umma::tmem_free(tmem, 64);
 }
 
+// Writes column r (one sample) of a K-major core-matrix tile whose rows
+// are features and whose K dimension is the 128 samples of the tile.
+__device__ __forceinline__ void put_col(char* tile, uint32_t r, uint32_t rows, const float* f) {
+    for (uint32_t k = 0; k < rows; k++)
+        *reinterpret_cast<__nv_bfloat16*>(tile + cm_offset(k, r, TILE)) = __float2bfloat16_rn(f[k]);
+}
+
+// TMEM columns of the backward kernel: the gradient propagation product,
+// then each layer's weight-gradient accumulator (transposed: lane = input
+// feature, column = output), which lives across the CTA's tiles.
+constexpr uint32_t TC_D = 0;
+__host__ __device__ constexpr uint32_t tc_dw(int l) {
+    return l == 0 ? 64u : (l == 1 ? 192u : (l == 2 ? 256u : (l == 3 ? 320u : 384u)));
+}
+
 __global__ void __launch_bounds__(TILE, 1) nrc_backward(const __grid_constant__ Args a) {
     extern __shared__ __align__(1024) char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + BWD_BAR);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + BWD_BAR + 8);
-    float* G = reinterpret_cast<float*>(smem + BWD_G);                  // [128][64] fp32
-    uint16_t* ACT = reinterpret_cast<uint16_t*>(smem + BWD_ACT);        // [128][64] bf16
-    uint16_t* A0 = reinterpret_cast<uint16_t*>(smem + BWD_A0);          // [128][256] bf16
     const uint32_t t = threadIdx.x;
     for (uint32_t i = t; i < WT_BYTES / 16; i += TILE)
         reinterpret_cast<uint4*>(smem + BWD_WT)[i] = reinterpret_cast<const uint4*>(a.wt)[i];
     if (t == 0) umma::bar_init(bar, 1);
-    if (t < 32) umma::tmem_alloc(tslot, 64);
+    if (t < 32) umma::tmem_alloc(tslot, 512);
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t s_base = umma::smem_addr(smem), s_gcm = s_base + BWD_GCM;
+    const uint32_t sb = umma::smem_addr(smem);
     uint32_t phase = 0;
+    bool first = true;  // first tile of this CTA: the weight-gradient accumulators start at zero
+    bool ok = true;
     const uint32_t n = count_of(a);
     const uint32_t tiles = (n + TILE - 1) / TILE;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t s = tile * TILE + t;
         const bool live = s < n;
-        // Output gradient (N = 16) into G and its operand tile.
+        // Output gradient, N = 16: row t of the propagation operand, column t
+        // of the weight-gradient operand.
         float g[HID];
-        for (int c = 0; c < OUT_PAD; c++) g[c] = live ? a.dy[(size_t)s * OUT_PAD + c] : 0.0f;
-        for (int c = 0; c < OUT_PAD; c++) G[t * HID + c] = g[c];
+        for (int c = 0; c < HID; c++) g[c] = (live && c < (int)OUT_PAD) ? a.dy[(size_t)s * OUT_PAD + c] : 0.0f;
         put_row<OUT_PAD>(smem + BWD_GCM, t, g);
-        bool ok = true;
+        put_col(smem + BWD_GT, t, OUT_PAD, g);
         for (int l = LAYERS - 1; l >= 1 && ok; l--) {
-            const uint32_t N = l == LAYERS - 1 ? OUT_PAD : HID;  // width of the gradient G
-            // Input of layer l (h_{l-1}) into ACT.
+            const uint32_t N = l == LAYERS - 1 ? OUT_PAD : HID;
+            // h_{l-1}, the input of layer l, for this sample.
+            float h[HID];
             {
                 const uint4* src = reinterpret_cast<const uint4*>(a.acts + ((size_t)s * (LAYERS - 1) + (l - 1)) * HID);
-                uint4* dst = reinterpret_cast<uint4*>(ACT + t * HID);
-                for (int q = 0; q < HID / 8; q++) dst[q] = live ? src[q] : make_uint4(0, 0, 0, 0);
-            }
-            publish_smem();
-            // delta_{l-1} = G x W_l on the tensor cores (B = W_l^T, 64 x N).
-            if (t == 0) layer_mma(tmem, s_gcm, s_base + BWD_WT + WT_OFF(l), N, HID, bar);
-            // Meanwhile dW_l += G^T x ACT on the CUDA cores.
-            {
-                const uint32_t k = t % HID, half = t / HID;  // two threads per input column
-                const uint32_t n0 = half * (N / 2), n1 = n0 + N / 2;
-                float acc[HID / 2];
-                for (uint32_t i = 0; i < N / 2; i++) acc[i] = 0.0f;
-                for (uint32_t r = 0; r < TILE; r++) {
-                    float av = __uint_as_float((uint32_t)ACT[r * HID + k] << 16);
-                    if (av == 0.0f) continue;
-                    for (uint32_t nn = n0; nn < n1; nn++) acc[nn - n0] += G[r * HID + nn] * av;
+                for (int q = 0; q < HID / 8; q++) {
+                    uint4 v = live ? src[q] : make_uint4(0, 0, 0, 0);
+                    h[8 * q + 0] = bf16_lo(v.x); h[8 * q + 1] = bf16_hi(v.x);
+                    h[8 * q + 2] = bf16_lo(v.y); h[8 * q + 3] = bf16_hi(v.y);
+                    h[8 * q + 4] = bf16_lo(v.z); h[8 * q + 5] = bf16_hi(v.z);
+                    h[8 * q + 6] = bf16_lo(v.w); h[8 * q + 7] = bf16_hi(v.w);
                 }
-                for (uint32_t nn = n0; nn < n1; nn++)
-                    if (acc[nn - n0] != 0.0f) atomicAdd(a.grad + P_OFF(l) + nn * HID + k, acc[nn - n0]);
+            }
+            put_col(smem + BWD_ACTT, t, HID, h);
+            publish_smem();
+            if (t == 0) {
+                // delta_{l-1} = G x W_l (B = W_l^T), and dW_l^T += h_{l-1}^T x G.
+                const uint32_t sbo_g = (N / 8) * 128;
+                const uint32_t id = umma::idesc_bf16(TILE, HID);
+                for (uint32_t kk = 0; kk < N / 16; kk++)
+                    umma::mma_bf16(tmem + TC_D, umma::smem_desc(sb + BWD_GCM + kk * 256, 128, sbo_g),
+                                   umma::smem_desc(sb + BWD_WT + WT_OFF(l) + kk * 256, 128, sbo_g), id, kk > 0);
+                const uint32_t idw = umma::idesc_bf16(TILE, N), sbo_t = (TILE / 8) * 128;
+                for (uint32_t kk = 0; kk < TILE / 16; kk++)
+                    umma::mma_bf16(tmem + tc_dw(l), umma::smem_desc(sb + BWD_ACTT + kk * 256, 128, sbo_t),
+                                   umma::smem_desc(sb + BWD_GT + kk * 256, 128, sbo_t), idw, !first || kk > 0);
+                umma::commit(bar);
             }
             ok = await_mma(bar, &phase, a.err);
             if (!ok) break;
             float d[HID];
-            read_row(tmem, HID, d);
-            for (int k = 0; k < HID; k++) {
-                float h = __uint_as_float((uint32_t)ACT[t * HID + k] << 16);
-                d[k] = h > 0.0f ? d[k] : 0.0f;
-            }
+            read_row(tmem + TC_D, HID, d);
+            for (int k = 0; k < HID; k++) d[k] = h[k] > 0.0f ? d[k] : 0.0f;
             umma::fence_before_sync();
-            __syncthreads();  // G, ACT and D reads done
-            for (int k = 0; k < HID; k++) G[t * HID + k] = d[k];
+            __syncthreads();  // products read, operands free
             put_row<HID>(smem + BWD_GCM, t, d);
-            __syncthreads();
+            put_col(smem + BWD_GT, t, HID, d);
         }
         if (!ok) break;
-        // dW_0 += G^T x encoded inputs.
+        // dW_0^T += encoded inputs^T x delta_0, two 128-feature halves.
         {
             float f[IN];
             encode(a.in, s, n, f);
-            for (int k = 0; k < IN; k += 2)
-                reinterpret_cast<uint32_t*>(A0)[(t * IN + k) >> 1] = pack_bf16(f[k], f[k + 1]);
+            put_col(smem + BWD_A0T, t, TILE, f);
+            put_col(smem + BWD_A0T + TILE * TILE * 2, t, TILE, f + TILE);
         }
-        __syncthreads();
-        {
-            const uint32_t k = 2 * t;  // columns k, k + 1
-            for (uint32_t n0 = 0; n0 < HID; n0 += 16) {
-                float acc0[16], acc1[16];
-                for (int i = 0; i < 16; i++) acc0[i] = acc1[i] = 0.0f;
-                for (uint32_t r = 0; r < TILE; r++) {
-                    uint32_t pv = reinterpret_cast<const uint32_t*>(A0)[(r * IN + k) >> 1];
-                    float x0 = bf16_lo(pv), x1 = bf16_hi(pv);
-#pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        float gv = G[r * HID + n0 + i];
-                        acc0[i] += gv * x0;
-                        acc1[i] += gv * x1;
-                    }
-                }
-                for (int i = 0; i < 16; i++) {
-                    if (acc0[i] != 0.0f) atomicAdd(a.grad + P_OFF(0) + (n0 + i) * IN + k, acc0[i]);
-                    if (acc1[i] != 0.0f) atomicAdd(a.grad + P_OFF(0) + (n0 + i) * IN + k + 1, acc1[i]);
-                }
-            }
+        publish_smem();
+        if (t == 0) {
+            const uint32_t idw = umma::idesc_bf16(TILE, HID), sbo_t = (TILE / 8) * 128;
+            for (uint32_t half = 0; half < 2; half++)
+                for (uint32_t kk = 0; kk < TILE / 16; kk++)
+                    umma::mma_bf16(tmem + tc_dw(0) + half * HID,
+                                   umma::smem_desc(sb + BWD_A0T + half * TILE * TILE * 2 + kk * 256, 128, sbo_t),
+                                   umma::smem_desc(sb + BWD_GT + kk * 256, 128, sbo_t), idw, !first || kk > 0);
+            umma::commit(bar);
         }
+        ok = await_mma(bar, &phase, a.err);
+        first = false;
         umma::fence_before_sync();
         __syncthreads();
         umma::fence_after_sync();
     }
+    // This CTA's weight gradients, one row of partial sums per CTA.
+    if (ok && !first) {
+        float* part = a.grad_part + (size_t)blockIdx.x * PARAMS;
+        float v[HID];
+        for (uint32_t half = 0; half < 2; half++) {
+            read_row(tmem + tc_dw(0) + half * HID, HID, v);
+            const uint32_t f = half * TILE + t;
+            for (uint32_t o = 0; o < HID; o++) part[P_OFF(0) + o * IN + f] = v[o];
+        }
+        for (int l = 1; l < LAYERS; l++) {
+            const uint32_t N = l == LAYERS - 1 ? OUT_PAD : HID;
+            read_row(tmem + tc_dw(l), N, v);
+            if (t < HID)
+                for (uint32_t o = 0; o < N; o++) part[P_OFF(l) + o * HID + t] = v[o];
+        }
+    } else if (!first || !ok) {
+        // nothing traced, or gave up: no contribution
+    }
+    if (first) {  // no tile: an all-zero partial
+        float* part = a.grad_part + (size_t)blockIdx.x * PARAMS;
+        for (uint32_t i = t; i < PARAMS; i += TILE) part[i] = 0.0f;
+    }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    if (t < 32) umma::tmem_free(tmem, 64);
+    if (t < 32) umma::tmem_free(tmem, 512);
+}
+
+// grad[i] = sum over the backward CTAs' partial rows, in CTA order.
+__global__ void nrc_grad_reduce(const float* part, uint32_t rows, float* grad) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= PARAMS) return;
+    float acc = 0.0f;
+    for (uint32_t r = 0; r < rows; r++) acc += part[(size_t)r * PARAMS + i];
+    grad[i] = acc;
 }
 
 // Layer, row (output) and column (input) of parameter i.
@@ -437,10 +475,14 @@ cudaError_t launch_backward(const Args& a, int sms, cudaStream_t st) {
         if (e) return e;
         attr = true;
     }
-    uint32_t tiles = (a.n + TILE - 1) / TILE;
-    if (tiles == 0) return cudaSuccess;
-    uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
+    // The grid is the SM count (a partial-sum row per CTA; CTAs without a
+    // tile write zeros), so the reduce order does not depend on n.
+    if (a.n == 0) return cudaSuccess;
+    const uint32_t grid = (uint32_t)sms;
     nrc_backward<<<grid, TILE, BWD_SMEM, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e) return e;
+    nrc_grad_reduce<<<(PARAMS + 255) / 256, 256, 0, st>>>(a.grad_part, grid, a.grad);
     return cudaGetLastError();
 }
 

@@ -53,7 +53,8 @@ struct Args {
     float* dy;                    // training: n x 16 loss gradient w.r.t. outputs
     float* loss;                  // training: summed relative L2 loss
     float grad_scale;             // 1 / (3 n): the loss is a mean over samples and channels (0: from n)
-    float* grad;                  // PARAMS gradient accumulator
+    float* grad;                  // PARAMS gradient
+    float* grad_part;             // backward: one row of PARAMS partial sums per CTA (SM count rows)
     float* master;                // PARAMS FP32 weights
     float* m1;                    // Adam first moments
     float* m2;                    // Adam second moments

@@ -41,6 +41,7 @@ Args oxd::nrc::base_args(oxpt_nrc* c) {
     a.wf = c->wf;
     a.wt = c->wt;
     a.grad = c->grad;
+    a.grad_part = c->grad_part;
     a.master = c->master;
     a.m1 = c->m1;
     a.m2 = c->m2;
@@ -133,7 +134,8 @@ oxpt_status oxpt_nrc_create(oxpt_ctx* ctx, uint64_t seed, oxpt_nrc** out) {
               cudaMalloc((void**)&c->grad, PARAMS * 4) == cudaSuccess &&
               cudaMalloc((void**)&c->loss, 16) == cudaSuccess && cudaMalloc((void**)&c->wf, W_BYTES) == cudaSuccess &&
               cudaMalloc((void**)&c->wt, WT_BYTES) == cudaSuccess &&
-              cudaMalloc((void**)&c->err_dev, 4) == cudaSuccess;
+              cudaMalloc((void**)&c->err_dev, 4) == cudaSuccess &&
+              cudaMalloc((void**)&c->grad_part, (size_t)c->sms * PARAMS * 4) == cudaSuccess;
     if (!ok) {
         oxpt_nrc_destroy(c);
         return OXPT_E_NOMEM;
@@ -169,7 +171,7 @@ void oxpt_nrc_destroy(oxpt_nrc* c) {
         cudaStreamSynchronize(c->stream);
         cudaStreamDestroy(c->stream);
     }
-    void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->loss, c->wf, c->wt, c->err_dev,
+    void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->grad_part, c->loss, c->wf, c->wt, c->err_dev,
                     c->in, c->pred, c->target, c->acts, c->dy, c->counts, c->q_in, c->q_beta, c->q_item,
                     c->t_in, c->t_target, c->s_pre, c->s_beta, c->s_tidx, c->t_tail, c->q_pred};
     for (void* p : ptrs)

@@ -14,6 +14,7 @@ struct oxpt_nrc {
     cudaStream_t stream = nullptr;  // owned: host-buffer calls
     std::string err;
     float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *loss = nullptr;
+    float* grad_part = nullptr;  // SM count x PARAMS partial sums of the backward kernel
     uint16_t *wf = nullptr, *wt = nullptr;
     uint32_t* err_dev = nullptr;
     // scratch of the host-buffer calls
