@@ -182,6 +182,21 @@ oxpt_status oxpt_resolve(oxpt_ctx* ctx, const oxpt_resolve_params* params, int h
 
 /* Raw accumulator (w*h*4 floats: sum rgb over covered samples, covered
  * count). Blocking. */
+/*
+ * Present path (§ image() / draw_texture(), src/pathtrace.rs:687-725, as an
+ * asynchronous readback): resolves on the context's stream into a device
+ * image, then copies it to `host_out` on a separate copy stream, so the
+ * copy overlaps whatever is enqueued next on the context (the next refine
+ * does not wait for it). `host_out` must stay valid until
+ * oxpt_resolve_wait returns; pinned memory (oxpt_host_alloc) makes the copy
+ * truly asynchronous. A later oxpt_resolve_async waits on the device for
+ * the previous copy before reusing the image.
+ */
+oxpt_status oxpt_resolve_async(oxpt_ctx* ctx, const oxpt_resolve_params* params, int hdr, void* host_out);
+oxpt_status oxpt_resolve_wait(oxpt_ctx* ctx);
+/* Page-locked host memory for present buffers (NULL on failure). */
+void* oxpt_host_alloc(size_t bytes);
+void oxpt_host_free(void* p);
 oxpt_status oxpt_read_accum(oxpt_ctx* ctx, float* host_out);
 
 /* The accumulator itself as a device image (RGBA32F, read-write), for

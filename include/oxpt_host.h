@@ -233,6 +233,11 @@ oxpt_status oxpt_tracer_finish(oxpt_tracer* t);
 oxpt_status oxpt_tracer_image(oxpt_tracer* t, uint8_t* out);
 /* w*h*4 floats, scene-linear. */
 oxpt_status oxpt_tracer_hdr(oxpt_tracer* t, float* out);
+/* image() without waiting: the RGBA8 bytes land in `out` (keep it valid,
+ * preferably pinned) while later work proceeds; oxpt_tracer_present_wait
+ * returns once they have. (oxpt_resolve_async.) */
+oxpt_status oxpt_tracer_image_async(oxpt_tracer* t, uint8_t* out);
+oxpt_status oxpt_tracer_present_wait(oxpt_tracer* t);
 oxpt_status oxpt_tracer_draw_texture(oxpt_tracer* t, oxpt_devimage* out);
 oxpt_status oxpt_tracer_read_accum(oxpt_tracer* t, float* out);
 /* The flat buffers and Params of the current binding (valid until the next

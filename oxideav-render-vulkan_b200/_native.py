@@ -141,6 +141,10 @@ _SIGS = {
     "oxpt_finish": (cint, [vp]),
     "oxpt_resolve": (cint, [vp, C.POINTER(ResolveParams), cint, vp, C.POINTER(DevImage)]),
     "oxpt_read_accum": (cint, [vp, vp]),
+    "oxpt_resolve_async": (cint, [vp, C.POINTER(ResolveParams), cint, vp]),
+    "oxpt_resolve_wait": (cint, [vp]),
+    "oxpt_host_alloc": (vp, [sz]),
+    "oxpt_host_free": (None, [vp]),
     "oxpt_accum_view": (cint, [vp, C.POINTER(DevImage)]),
     "oxpt_dispatch_noalloc": (cint, [C.c_void_p, C.POINTER(Params), C.POINTER(Frame), vp, vp]),
     # oxpt_batch.h
@@ -223,6 +227,8 @@ _SIGS = {
     "oxpt_tracer_finish": (cint, [vp]),
     "oxpt_tracer_image": (cint, [vp, vp]),
     "oxpt_tracer_hdr": (cint, [vp, vp]),
+    "oxpt_tracer_image_async": (cint, [vp, vp]),
+    "oxpt_tracer_present_wait": (cint, [vp]),
     "oxpt_tracer_draw_texture": (cint, [vp, C.POINTER(DevImage)]),
     "oxpt_tracer_read_accum": (cint, [vp, vp]),
     "oxpt_tracer_prepared": (cint, [vp, C.POINTER(PreparedView)]),

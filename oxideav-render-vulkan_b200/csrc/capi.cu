@@ -47,6 +47,11 @@ struct oxpt_ctx {
     // scene buffers / tables borrowed from another context (oxpt_share_*)
     bool borrowed_scene = false, borrowed_tables = false;
     std::vector<uint32_t> table_head;  // host copy of the first table words (fixed tables)
+    // present path (oxpt_resolve_async): image buffer, copy stream, events
+    void* present = nullptr;
+    size_t present_bytes = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t resolved = nullptr, copied = nullptr;
     cudaEvent_t ready = nullptr;       // this context's stream position, for batches
     // stream marks (oxpt_mark): a ring of events
     std::vector<cudaEvent_t> marks;
@@ -542,6 +547,11 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
                     c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev};
     if (c->batch_done) cudaEventDestroy(c->batch_done);
+    if (c->copy) cudaStreamSynchronize(c->copy);
+    if (c->present) cudaFree(c->present);
+    if (c->resolved) cudaEventDestroy(c->resolved);
+    if (c->copied) cudaEventDestroy(c->copied);
+    if (c->copy) cudaStreamDestroy(c->copy);
     if (c->batch_copied) cudaEventDestroy(c->batch_copied);
     if (c->batch_host) cudaFreeHost(c->batch_host);
     if (c->ready) cudaEventDestroy(c->ready);
@@ -797,6 +807,63 @@ oxpt_status oxpt_resolve(oxpt_ctx* c, const oxpt_resolve_params* p, int hdr, voi
         CK(c, cudaStreamSynchronize(c->stream), "readback");
     }
     return OXPT_OK;
+}
+
+oxpt_status oxpt_resolve_async(oxpt_ctx* c, const oxpt_resolve_params* p, int hdr, void* host_out) {
+    if (!c || !p || !host_out) return fail(c, OXPT_E_INVALID, "null argument");
+    if (!c->accum) return fail(c, OXPT_E_INVALID, "no accumulator: call oxpt_resize first");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    size_t bytes = (size_t)c->w * c->h * (hdr ? 16 : 4);
+    if (!c->copy) CK(c, cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking), "copy stream");
+    if (!c->resolved) CK(c, cudaEventCreateWithFlags(&c->resolved, cudaEventDisableTiming), "present event");
+    if (!c->copied) CK(c, cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming), "present event");
+    if (bytes > c->present_bytes) {
+        CK(c, cudaStreamSynchronize(c->copy), "present buffer");
+        if ((s = realloc_dev(c, &c->present, bytes, "present buffer"))) {
+            c->present_bytes = 0;
+            return s;
+        }
+        c->present_bytes = bytes;
+    }
+    // The previous copy out of the buffer finishes before it is rewritten.
+    CK(c, cudaStreamWaitEvent(c->stream, c->copied, 0), "present order");
+    oxd::ResolveArgs ra;
+    ra.accum = c->accum;
+    ra.w = c->w;
+    ra.h = c->h;
+    ra.p = *p;
+    ra.hdr = hdr ? 1 : 0;
+    ra.out = c->present;
+    CK(c, oxd::launch_resolve(ra, c->stream), "resolve launch");
+    c->launches += 1;
+    CK(c, cudaEventRecord(c->resolved, c->stream), "present event");
+    CK(c, cudaStreamWaitEvent(c->copy, c->resolved, 0), "present order");
+    CK(c, cudaMemcpyAsync(host_out, c->present, bytes, cudaMemcpyDeviceToHost, c->copy), "present copy");
+    CK(c, cudaEventRecord(c->copied, c->copy), "present event");
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_resolve_wait(oxpt_ctx* c) {
+    if (!c) return OXPT_E_INVALID;
+    if (!c->copied) return OXPT_OK;
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaEventSynchronize(c->copied), "present wait");
+    return OXPT_OK;
+}
+
+void* oxpt_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void oxpt_host_free(void* p) {
+    if (p) cudaFreeHost(p);
 }
 
 oxpt_status oxpt_read_accum(oxpt_ctx* c, float* out) {

@@ -350,6 +350,13 @@ oxpt_status oxpt_tracer_set_camera(oxpt_tracer* t, const oxpt_camera* cam) {
 oxpt_status oxpt_tracer_finish(oxpt_tracer* t) { return t->check(oxpt_finish(t->ctx)); }
 oxpt_status oxpt_tracer_image(oxpt_tracer* t, uint8_t* out) { return t->resolve(false, out, nullptr); }
 oxpt_status oxpt_tracer_hdr(oxpt_tracer* t, float* out) { return t->resolve(true, out, nullptr); }
+oxpt_status oxpt_tracer_image_async(oxpt_tracer* t, uint8_t* out) {
+    if (!t || !out) return OXPT_E_INVALID;
+    if (!t->has_accum) return t->resolve(false, out, nullptr);  // never synced: background, synchronously
+    oxpt_resolve_params rp = t->resolve_params(false);
+    return t->check(oxpt_resolve_async(t->ctx, &rp, 0, out));
+}
+oxpt_status oxpt_tracer_present_wait(oxpt_tracer* t) { return t ? t->check(oxpt_resolve_wait(t->ctx)) : OXPT_E_INVALID; }
 oxpt_status oxpt_tracer_draw_texture(oxpt_tracer* t, oxpt_devimage* out) { return t->resolve(false, nullptr, out); }
 
 oxpt_status oxpt_tracer_read_accum(oxpt_tracer* t, float* out) {

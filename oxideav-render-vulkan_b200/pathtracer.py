@@ -273,6 +273,31 @@ class DeviceImage:
     format: str
 
 
+class PinnedImage:
+    """Page-locked RGBA8 host image (oxpt_host_alloc) for the present path."""
+
+    def __init__(self, h: int, w: int):
+        n = max(1, h * w * 4)
+        self.ptr = N.lib().oxpt_host_alloc(n)
+        if not self.ptr:
+            raise BackendError("cannot allocate pinned host memory")
+        self.array = np.ctypeslib.as_array(C.cast(self.ptr, C.POINTER(C.c_uint8)), shape=(h, w, 4))
+        self._tracer = None
+
+    def wait(self) -> np.ndarray:
+        if self._tracer is not None:
+            self._tracer.present_wait()
+        return self.array
+
+    def __del__(self):
+        p = getattr(self, "ptr", None)
+        if p:
+            if self._tracer is not None:
+                N.lib().oxpt_tracer_present_wait(self._tracer._h)
+            N.lib().oxpt_host_free(p)
+            self.ptr = None
+
+
 class GpuPathTracer:
     """Progressive CUDA path tracer with the reference's API and reset rules."""
 
@@ -398,6 +423,19 @@ class GpuPathTracer:
         out = np.empty((h, w, 4), dtype=np.uint8)
         self._check(N.lib().oxpt_tracer_image(self._h, out.ctypes.data))
         return out
+
+    def image_async(self) -> "PinnedImage":
+        """image() without waiting: returns a pinned buffer that holds the
+        RGBA8 image once .wait() returns; refines enqueued meanwhile overlap
+        the copy."""
+        w, h = self.size()
+        buf = PinnedImage(h, w)
+        self._check(N.lib().oxpt_tracer_image_async(self._h, buf.ptr))
+        buf._tracer = self
+        return buf
+
+    def present_wait(self):
+        self._check(N.lib().oxpt_tracer_present_wait(self._h))
 
     def hdr(self) -> np.ndarray:
         w, h = self.size()
