@@ -147,6 +147,12 @@ oxpt_status oxpt_diag_bvh4(const oxpt_ctx* ctx, uint32_t out[4]);
  * more than 16 triangles). Needs no GPU. */
 oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint32_t* out, size_t cap,
                                  size_t* words, uint32_t* root, uint32_t* stack_need);
+/* BVH of n triangles (tri_pos: 9 floats each) by the host builder
+ * (on_gpu = 0) or the GPU builder on `device` (on_gpu = 1): node words
+ * (8 per node, at most 2n nodes), leaf slot -> triangle, node count and
+ * depth. Both give the same words. */
+oxpt_status oxpt_diag_bvh_build(int device, const float* tri_pos, uint32_t n, int on_gpu, uint32_t* words,
+                                uint32_t* slots, uint32_t* node_count, uint32_t* depth);
 /* Wavefront bounces (logic + extend + shadow launches) run so far (waits
  * for the context's stream when graph-resident loops have run). */
 oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* ctx, uint64_t* out);

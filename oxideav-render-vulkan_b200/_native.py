@@ -162,6 +162,7 @@ _SIGS = {
     "oxpt_get_tuning": (cint, [vp, C.POINTER(Tuning)]),
     "oxpt_diag_wave_iterations": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_bvh4": (cint, [vp, C.POINTER(u32 * 4)]),
+    "oxpt_diag_bvh_build": (cint, [cint, vp, u32, cint, vp, vp, C.POINTER(u32), C.POINTER(u32)]),
     "oxpt_diag_graph_builds": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_bvh4_build": (cint, [vp, u32, vp, sz, C.POINTER(sz), C.POINTER(u32), C.POINTER(u32)]),
     "oxpt_diag_timing_kinds": (cint, [vp, vp, vp]),
@@ -222,6 +223,7 @@ _SIGS = {
     "oxpt_tracer_size": (None, [vp, C.POINTER(u32), C.POINTER(u32)]),
     "oxpt_tracer_sync": (cint, [vp, vp, C.POINTER(RenderOptions), C.POINTER(cint)]),
     "oxpt_tracer_refine": (cint, [vp, u32]),
+    "oxpt_tracer_set_gpu_build": (None, [vp, cint]),
     "oxpt_tracer_refine_rows": (cint, [vp, u32, u32, u32]),
     "oxpt_tracers_refine_batch": (cint, [C.POINTER(vp), u32, C.POINTER(u32), vp]),
     "oxpt_tracer_finish": (cint, [vp]),

@@ -9,6 +9,12 @@
 // is this project's own (Wald 2007 binning, 32 bins per axis, SAH with unit
 // traversal and intersection costs, leaves of at most 8 triangles). It
 // writes the same node format.
+//
+// The build is defined level by level so that the GPU builder
+// (csrc/bvh_build.cu) can produce the same words: the nodes of a level are
+// split in order, each split allocates its child pair next, partitions are
+// stable, and a triangle's box has its zeros made positive (so that min /
+// max over any order give the same bits).
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
@@ -64,97 +70,97 @@ struct Builder {
         w[7] = count;
     }
 
-    // Build node `n` over ids[begin, end). Explicit stack to bound recursion.
+    // Level-order build from the root over ids[begin0, end0).
     void build(uint32_t root_node, uint32_t begin0, uint32_t end0) {
         struct Job {
-            uint32_t node, begin, end, depth;
+            uint32_t node, begin, end;
         };
-        std::vector<Job> stack;
-        stack.push_back({root_node, begin0, end0, 1});
-        while (!stack.empty()) {
-            Job j = stack.back();
-            stack.pop_back();
-            max_depth = std::max(max_depth, j.depth);
-            Box bounds, cbounds;
-            for (uint32_t i = j.begin; i < j.end; i++) {
-                bounds.grow(tri_box[ids[i]]);
-                cbounds.grow(centroid[ids[i]]);
-            }
-            uint32_t count = j.end - j.begin;
-            if (count <= 1) {
-                set_node(j.node, bounds, j.begin, count);
-                continue;
-            }
-            // Binned SAH over the three axes.
-            float best_cost = FLT_MAX;
-            int best_axis = -1, best_split = -1;
-            for (int axis = 0; axis < 3; axis++) {
-                float lo = cbounds.lo[axis], hi = cbounds.hi[axis];
-                if (!(hi > lo)) continue;
-                float scale = BINS / (hi - lo);
-                Box bb[BINS];
-                uint32_t bc[BINS] = {0};
+        std::vector<Job> level{{root_node, begin0, end0}}, next;
+        while (!level.empty()) {
+            max_depth++;
+            next.clear();
+            for (const Job& j : level) {
+                Box bounds, cbounds;
                 for (uint32_t i = j.begin; i < j.end; i++) {
-                    int b = (int)((centroid[ids[i]][axis] - lo) * scale);
-                    b = std::min(std::max(b, 0), BINS - 1);
-                    bc[b]++;
-                    bb[b].grow(tri_box[ids[i]]);
+                    bounds.grow(tri_box[ids[i]]);
+                    cbounds.grow(centroid[ids[i]]);
                 }
-                float right_area[BINS];
-                uint32_t right_count[BINS];
-                Box acc;
-                uint32_t n = 0;
-                for (int b = BINS - 1; b > 0; b--) {
-                    acc.grow(bb[b]);
-                    n += bc[b];
-                    right_area[b] = acc.area();
-                    right_count[b] = n;
+                uint32_t count = j.end - j.begin;
+                if (count <= 1) {
+                    set_node(j.node, bounds, j.begin, count);
+                    continue;
                 }
-                Box lacc;
-                uint32_t ln = 0;
-                for (int b = 0; b < BINS - 1; b++) {
-                    lacc.grow(bb[b]);
-                    ln += bc[b];
-                    if (ln == 0 || right_count[b + 1] == 0) continue;
-                    float cost = lacc.area() * ln + right_area[b + 1] * right_count[b + 1];
-                    if (cost < best_cost) {
-                        best_cost = cost;
-                        best_axis = axis;
-                        best_split = b;
+                // Binned SAH over the three axes.
+                float best_cost = FLT_MAX;
+                int best_axis = -1, best_split = -1;
+                for (int axis = 0; axis < 3; axis++) {
+                    float lo = cbounds.lo[axis], hi = cbounds.hi[axis];
+                    if (!(hi > lo)) continue;
+                    float scale = BINS / (hi - lo);
+                    Box bb[BINS];
+                    uint32_t bc[BINS] = {0};
+                    for (uint32_t i = j.begin; i < j.end; i++) {
+                        int b = (int)((centroid[ids[i]][axis] - lo) * scale);
+                        b = std::min(std::max(b, 0), BINS - 1);
+                        bc[b]++;
+                        bb[b].grow(tri_box[ids[i]]);
+                    }
+                    float right_area[BINS];
+                    uint32_t right_count[BINS];
+                    Box acc;
+                    uint32_t n = 0;
+                    for (int b = BINS - 1; b > 0; b--) {
+                        acc.grow(bb[b]);
+                        n += bc[b];
+                        right_area[b] = acc.area();
+                        right_count[b] = n;
+                    }
+                    Box lacc;
+                    uint32_t ln = 0;
+                    for (int b = 0; b < BINS - 1; b++) {
+                        lacc.grow(bb[b]);
+                        ln += bc[b];
+                        if (ln == 0 || right_count[b + 1] == 0) continue;
+                        float cost = lacc.area() * ln + right_area[b + 1] * right_count[b + 1];
+                        if (cost < best_cost) {
+                            best_cost = cost;
+                            best_axis = axis;
+                            best_split = b;
+                        }
                     }
                 }
-            }
-            float parent_area = bounds.area();
-            float leaf_cost = (float)count;
-            float split_cost = parent_area > 0 ? 1.0f + best_cost / parent_area : FLT_MAX;
-            uint32_t mid;
-            if (best_axis < 0) {
-                // Coincident centroids: leaf if small, else split in half.
-                if (count <= MAX_LEAF) {
-                    set_node(j.node, bounds, j.begin, count);
-                    continue;
+                float parent_area = bounds.area();
+                float leaf_cost = (float)count;
+                float split_cost = parent_area > 0 ? 1.0f + best_cost / parent_area : FLT_MAX;
+                uint32_t mid;
+                if (best_axis < 0) {
+                    // Coincident centroids: leaf if small, else split in half.
+                    if (count <= MAX_LEAF) {
+                        set_node(j.node, bounds, j.begin, count);
+                        continue;
+                    }
+                    mid = j.begin + count / 2;
+                } else {
+                    if (count <= MAX_LEAF && leaf_cost <= split_cost) {
+                        set_node(j.node, bounds, j.begin, count);
+                        continue;
+                    }
+                    float lo = cbounds.lo[best_axis];
+                    float scale = BINS / (cbounds.hi[best_axis] - lo);
+                    auto it = std::stable_partition(ids.begin() + j.begin, ids.begin() + j.end, [&](uint32_t t) {
+                        int b = (int)((centroid[t][best_axis] - lo) * scale);
+                        b = std::min(std::max(b, 0), BINS - 1);
+                        return b <= best_split;
+                    });
+                    mid = (uint32_t)(it - ids.begin());
+                    if (mid == j.begin || mid == j.end) mid = j.begin + count / 2;
                 }
-                mid = j.begin + count / 2;
-            } else {
-                if (count <= MAX_LEAF && leaf_cost <= split_cost) {
-                    set_node(j.node, bounds, j.begin, count);
-                    continue;
-                }
-                float lo = cbounds.lo[best_axis];
-                float scale = BINS / (cbounds.hi[best_axis] - lo);
-                auto it = std::partition(ids.begin() + j.begin, ids.begin() + j.end, [&](uint32_t t) {
-                    int b = (int)((centroid[t][best_axis] - lo) * scale);
-                    b = std::min(std::max(b, 0), BINS - 1);
-                    return b <= best_split;
-                });
-                mid = (uint32_t)(it - ids.begin());
-                if (mid == j.begin || mid == j.end) mid = j.begin + count / 2;
+                uint32_t first = alloc_pair();
+                set_node(j.node, bounds, first, 0);
+                next.push_back({first, j.begin, mid});
+                next.push_back({first + 1, mid, j.end});
             }
-            uint32_t first = alloc_pair();
-            set_node(j.node, bounds, first, 0);
-            // Right pushed first so the left subtree is laid out first.
-            stack.push_back({first + 1, mid, j.end, j.depth + 1});
-            stack.push_back({first, j.begin, mid, j.depth + 1});
+            std::swap(level, next);
         }
     }
 };
@@ -171,8 +177,9 @@ BvhBuild build_bvh(const std::vector<float>& tri_pos) {
     b.ids.resize(n);
     for (size_t i = 0; i < n; i++) {
         Box bx;
-        for (int v = 0; v < 3; v++)
-            bx.grow(V3{tri_pos[i * 9 + v * 3], tri_pos[i * 9 + v * 3 + 1], tri_pos[i * 9 + v * 3 + 2]});
+        for (int v = 0; v < 3; v++)  // + 0.0f: -0 becomes +0
+            bx.grow(V3{tri_pos[i * 9 + v * 3] + 0.0f, tri_pos[i * 9 + v * 3 + 1] + 0.0f,
+                       tri_pos[i * 9 + v * 3 + 2] + 0.0f});
         b.tri_box[i] = bx;
         b.centroid[i] = (bx.lo + bx.hi) * 0.5f;
         b.ids[i] = (uint32_t)i;

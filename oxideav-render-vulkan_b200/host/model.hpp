@@ -131,7 +131,10 @@ struct SceneBuffers {
     uint32_t off_sobol = 0, off_sheen = 0, off_mat = 0, off_plights = 0, off_elights = 0;
     uint32_t bvh_depth = 0;
 };
-std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight);
+// `builder` (optional) replaces build_bvh, e.g. with the GPU build.
+std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
+                                           BvhBuild (*builder)(const std::vector<float>&, void*) = nullptr,
+                                           void* builder_arg = nullptr);
 
 // ensure_binding(): final tables (scene + env) and Params.
 void bind_params(const SceneBuffers& sb, const EnvWords* env, const ResolvedCamera& cam,

@@ -353,7 +353,8 @@ ResolvedCamera resolve_camera(const Framing& fr, const oxpt_render_options& o, u
 // ---------------------------------------------------------------------
 // upload (src/pathtrace.rs:970-1239).
 // ---------------------------------------------------------------------
-std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight) {
+std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
+                                           BvhBuild (*builder)(const std::vector<float>&, void*), void* builder_arg) {
     auto sb = std::make_unique<SceneBuffers>();
     // Materials: meshes without one use a trailing glTF default.
     std::vector<oxpt_material> materials = s.materials;
@@ -413,7 +414,7 @@ std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight)
     double total_power = 0.0;
     for (double p : power) total_power += p;
     // BVH.
-    BvhBuild bvh = build_bvh(pos);
+    BvhBuild bvh = builder ? builder(pos, builder_arg) : build_bvh(pos);
     sb->bvh_depth = bvh.depth;
     sb->node_count = (uint32_t)(bvh.node_words.size() / 8);
     sb->tri_base = sb->node_count * 2;

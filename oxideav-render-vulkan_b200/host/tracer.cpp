@@ -13,6 +13,7 @@
 #include "../../include/oxpt_batch.h"
 #include "../../include/oxpt_serve.h"
 #include "../../include/oxpt_nrc.h"
+#include "bvh_gpu.hpp"
 #include "model.hpp"
 
 namespace {
@@ -61,6 +62,7 @@ struct oxpt_tracer {
     // prepares itself (serving sessions); `cam` overrides the camera.
     const oxpt_tracer* owner = nullptr;
     std::optional<oxpt_camera> cam;
+    bool gpu_build = false;  // build the BVH on the context's GPU
     oxpt::Framing framing;
     std::optional<oxpt::Env> env;
     std::optional<oxpt::EnvWords> env_words;
@@ -87,8 +89,16 @@ struct oxpt_tracer {
         return OXPT_OK;
     }
 
+    static oxpt::BvhBuild device_build(const std::vector<float>& pos, void* arg) {
+        auto* t = static_cast<oxpt_tracer*>(arg);
+        oxpt::BvhBuild b;
+        std::string e;
+        if (oxpt::build_bvh_device(oxpt_ctx_device(t->ctx), pos, &b, &e)) return b;
+        return oxpt::build_bvh(pos);  // the device could not: the host builds the same tree
+    }
+
     oxpt_status upload(const oxpt_scene& s, float headlight) {
-        auto sb = oxpt::upload_scene(s, headlight);
+        auto sb = gpu_build ? oxpt::upload_scene(s, headlight, &device_build, this) : oxpt::upload_scene(s, headlight);
         oxpt_scene_desc d;
         d.geom = sb->geom.data();
         d.geom_words = sb->geom.size();
@@ -303,6 +313,12 @@ oxpt_status oxpt_tracer_refine_nrc(oxpt_tracer* t, oxpt_nrc* nrc, uint32_t frame
     if (st) return st;
     t->samples += frames;
     return OXPT_OK;
+}
+
+void oxpt_tracer_set_gpu_build(oxpt_tracer* t, int on) {
+    if (!t) return;
+    if ((on != 0) != t->gpu_build) t->dirty = true;  // the next sync prepares again
+    t->gpu_build = on != 0;
 }
 
 oxpt_status oxpt_tracer_new_view(const oxpt_tracer* owner, oxpt_tracer** out) {

@@ -382,6 +382,11 @@ class GpuPathTracer:
         N.lib().oxpt_device_summary(self.ctx, buf, 256)
         return buf.value.decode()
 
+    def set_gpu_build(self, on: bool = True):
+        """Build the BVH of the next preparation on this tracer's GPU (the
+        same tree as the host build)."""
+        N.lib().oxpt_tracer_set_gpu_build(self._h, int(bool(on)))
+
     def set_texture_resolver(self, resolver=None):
         N.lib().oxpt_tracer_set_texture_resolver(self._h)
 
