@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--ref-spp", type=int, default=16384, help="nrc workload: spp of the plain reference")
     ap.add_argument("--nrc-scene", default="large", choices=["large", "cornell"], help="nrc workload: scene")
     ap.add_argument("--nrc-train-one-in", type=int, default=4, help="nrc workload: one training path in this many")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve", "nrc"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve", "nrc", "prepare"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
     ap.add_argument("--scenes", type=int, default=64, help="batch workload: number of scenes")
@@ -366,6 +366,93 @@ def run_cornell(a):
     print(json.dumps(line), flush=True)
 
 
+def _leaf_depth_sum(geom, nodes):
+    """Sum over triangles of the depth of their leaf (root = 1): the levels
+    each triangle takes part in during a level-by-level build."""
+    w = geom[: nodes * 8].reshape(-1, 8)
+    first, count = w[:, 3].astype(np.int64), w[:, 7].astype(np.int64)
+    total, level, depth = 0, np.array([0], np.int64), 1
+    while level.size:
+        c = count[level]
+        total += int(c[c > 0].sum()) * depth
+        inner = level[c == 0]
+        level = np.concatenate([first[inner], first[inner] + 1])
+        depth += 1
+    return total
+
+
+def run_prepare(a):
+    """Scene preparation on the device (oxpt_build_scene behind
+    GpuPathTracer.sync with set_gpu_prepare): the large scene from host
+    memory to device-ready buffers, against the host preparation."""
+    import torch
+    torch.cuda.set_device(0)
+    __graft_entry__.build()
+    pkg = __graft_entry__.load_package()
+    scene, env = workload(pkg, a)
+    opts = options(pkg, a, spp=1)
+    tris = 20 * a.freq * a.freq
+    pt = pkg.GpuPathTracer(0)
+    pt.set_environment(env)
+    pt.set_gpu_prepare(True)
+    wall, phases = [], []
+    with Clocks(0) as clk:
+        for i in range(a.warmup + a.steps):
+            pt.invalidate_scene()
+            pt.finish()
+            t0 = time.perf_counter()
+            pt.sync(scene, opts)
+            pt.finish()
+            dt = time.perf_counter() - t0
+            if i >= a.warmup:
+                wall.append(dt)
+                phases.append(pt.prepare_timing())
+    prep = pt.prepared()
+    level_tris = _leaf_depth_sum(prep.geom, prep.node_count)
+    med = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
+    build_ms = med["bvh"] + med["flatten"]
+    e2e_s = statistics.median(wall)
+    # Source bytes that go up per step: positions, attribute streams, level-0 texels.
+    h2d = tris * (36 + 36 + 24)  # positions, normals, uv0 (the icosphere's streams)
+    h2d += 8 * a.tex * a.tex * 16  # level-0 texels of the 8 textures
+    d2h = prep.node_count * 32  # node words for the four-wide collapse
+    # Host preparation of the same scene (bounded sample: one run).
+    host = pkg.GpuPathTracer(0)
+    host.set_environment(env)
+    t0 = time.perf_counter()
+    host.sync(scene, opts)
+    host.finish()
+    host_s = time.perf_counter() - t0
+    hp = host.prepared()
+    same = (np.array_equal(hp.geom, prep.geom) and np.array_equal(hp.attrs.view(np.uint32), prep.attrs.view(np.uint32))
+            and np.array_equal(hp.atlas, prep.atlas) and np.array_equal(hp.tables, prep.tables))
+    peak, peak_kind = measured_peak()
+    # BVH roofline: per level every triangle still in an inner node reads its
+    # box and centroid (48 B) and its id (4 B) and writes its id (4 B).
+    alg = level_tris * 56
+    achieved = alg / (med["bvh"] * 1e-3) / 1e9
+    line = {"metric": "Mtriangles/s prepared", "value": tris / (build_ms * 1e-3) / 1e6, "unit": "Mtriangles/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * e2e_s,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"scene preparation of the single large scene ({tris} triangles, 8 x {a.tex}^2 "
+                                   "textures + mips, 64 materials, 512 emissive triangles)",
+                       "value": "BVH build + slot flattening on sources resident in HBM (CUDA events)",
+                       "e2e": "GpuPathTracer.sync from host memory to device-ready buffers (host wall clock): "
+                              "source upload, BVH, flattening, atlas, four-wide tree, tables",
+                       "l2": "sources and outputs (0.9 GB) larger than L2; no flush"},
+            "phases_ms": med, "identical_to_host": bool(same),
+            "e2e": {"value": tris / e2e_s / 1e6, "unit": "Mtriangles/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "BVH build (all levels)",
+                         "peak_kind": peak_kind},
+            "cpu_baseline": {"value": tris / host_s / 1e6, "unit": "Mtriangles/s", "cores": 1, "kind": "port",
+                             "sample": f"host preparation of the same scene, one run ({host_s:.1f} s): binned-SAH BVH, "
+                                       "slot flattening, mip chains and atlas on one thread, then the upload"},
+            "clocks": clk.summary(), "gpu_launches": int(med["launches"])}
+    print(json.dumps(line), flush=True)
+
+
 SERVE_RES = [(128, 128), (256, 256), (512, 512), (1280, 720), (1920, 1080)]
 SERVE_SPP = [4, 16, 64, 256, 1024]
 
@@ -579,6 +666,9 @@ def main():
         return
     if a.workload == "cornell":
         run_cornell(a)
+        return
+    if a.workload == "prepare":
+        run_prepare(a)
         return
     if a.impl == "reference":
         run_reference(a)

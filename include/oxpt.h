@@ -147,6 +147,59 @@ oxpt_status oxpt_device_summary(const oxpt_ctx* ctx, char* buf, size_t len);
  * tables with the environment words appended. */
 oxpt_status oxpt_upload_scene(oxpt_ctx* ctx, const oxpt_scene_desc* scene);
 oxpt_status oxpt_set_tables(oxpt_ctx* ctx, const uint32_t* words, size_t count);
+
+/*
+ * Scene preparation on the device: the buffers of oxpt_upload_scene built
+ * by the GPU from the scene's sources instead of by the host. Replaces the
+ * host passes of upload (src/pathtrace.rs:970-1239): the BVH the external
+ * TraceScene builds (binned SAH; the tree of the host builder, node for
+ * node), the leaf-slot flattening of triangles and push_attrs
+ * (:1274-1315), and the texel work of AtlasBuilder (:1482-1627: the mip
+ * chains, sRGB decode, f32_to_f16 into the shelf rectangles). The caller
+ * keeps the cheap host parts: materials, the emissive triangle list, and
+ * the atlas placement (rectangles per packed level). The device buffers
+ * equal, word for word, those oxpt_upload_scene takes from the host
+ * preparation of the same scene. Pointers are read during the call only.
+ */
+typedef struct oxpt_mesh_src {
+    uint32_t ntri;
+    uint32_t material;   /* material word of its triangles */
+    const float* pos;    /* 9 per triangle */
+    const float* nrm;    /* optional (NULL): 9 per triangle */
+    const float* tan;    /* optional: 12 per triangle */
+    const float* uv0;    /* optional: 6 per triangle */
+    const float* uv1;    /* optional: 6 per triangle */
+    const float* col;    /* optional: 12 per triangle (absent: 1.0) */
+} oxpt_mesh_src;
+
+typedef struct oxpt_chain_src {
+    uint32_t width, height;  /* level 0; each next level max(1, side / 2) down to 1 x 1 */
+    const float* rgba;       /* level-0 texels, RGBA, row-major */
+    uint32_t srgb_decode;    /* 1: decode RGB from sRGB before building the chain */
+    uint32_t skip;           /* leading levels left out of the atlas */
+    uint32_t n_rects;        /* packed levels: skip .. skip + n_rects - 1 */
+    const uint32_t* rects;   /* 4 words per packed level: layer, x, y, w | h << 16 */
+} oxpt_chain_src;
+
+typedef struct oxpt_scene_src {
+    const oxpt_mesh_src* meshes;
+    uint32_t n_meshes;        /* global triangle ids run through the meshes in order */
+    const uint32_t* light_tris;
+    uint32_t n_lights;        /* emissive triangles by global id; light index = position */
+    const oxpt_chain_src* chains;
+    uint32_t n_chains;
+    uint32_t atlas_side, atlas_layers;
+} oxpt_scene_src;
+
+/* light_slots (n_lights entries, may be NULL when n_lights is 0) receives
+ * the leaf slot of each light triangle (for the emissive records);
+ * out = {node_count, slot_count, bvh depth}. At least one triangle. */
+oxpt_status oxpt_build_scene(oxpt_ctx* ctx, const oxpt_scene_src* src, uint32_t* light_slots, uint32_t out[3]);
+/* Copies the context's device scene back in the layouts of
+ * oxpt_scene_desc: the whole geom buffer (node_count * 8 + slot_count * 12
+ * words for a device-built scene; the uploaded words otherwise), attrs
+ * (slot_count * 48 floats) and the atlas (side^2 * layers * 4 halfs). */
+oxpt_status oxpt_read_scene(oxpt_ctx* ctx, uint32_t* geom, float* attrs, uint16_t* atlas);
 /*
  * Borrow another context's device scene (geometry, attributes, atlas,
  * four-wide tree) or tables instead of uploading copies: contexts that

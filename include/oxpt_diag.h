@@ -139,6 +139,14 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);
  * (0: the scene keeps the binary walk for every ray), out[1] its nodes,
  * out[2] its root reference, out[3] the stack entries its walk needs. */
 oxpt_status oxpt_diag_bvh4(const oxpt_ctx* ctx, uint32_t out[4]);
+/* Timing of the context's last oxpt_build_scene, in milliseconds: device
+ * time (CUDA events) of [0] the source upload, [1] the BVH build, [2] the
+ * slot flattening, [3] the atlas (texel upload and mip chains, on a stream
+ * of its own that overlaps [0]-[2]); host wall time of [4] the whole call
+ * and [5] the upload of its four-wide tree (collapsed on the host while the
+ * atlas builds); [6] the number of
+ * kernels it launched; [7] unused (0). */
+oxpt_status oxpt_diag_scene_build(const oxpt_ctx* ctx, float ms[8]);
 /* Host-side collapse of binary node words (node i at words 8i..8i+7) into
  * the four-wide layout: 32 words per node, written to `out` when it has
  * room for them (`cap` words); *words = the words needed, *root = the root

@@ -216,10 +216,12 @@ void oxpt_tracer_size(const oxpt_tracer* t, uint32_t* w, uint32_t* h);
 oxpt_status oxpt_tracer_sync(oxpt_tracer* t, const oxpt_scene* scene,
                              const oxpt_render_options* opts, int* did_reset);
 oxpt_status oxpt_tracer_refine(oxpt_tracer* t, uint32_t samples);
-/* Build the BVH of the next preparation on the tracer's GPU (the same tree
- * as the host build, node for node; falls back to the host when the GPU
- * build fails). Changing it makes the next sync prepare again. */
-void oxpt_tracer_set_gpu_build(oxpt_tracer* t, int on);
+/* Prepare the scene on the tracer's GPU (oxpt_build_scene: the BVH, the
+ * leaf-slot flattening and the atlas texels; the same buffers as the host
+ * preparation, word for word). A tree whose levels are too wide for the
+ * device build is prepared by the host instead. Changing it makes the next
+ * sync prepare again. */
+void oxpt_tracer_set_gpu_prepare(oxpt_tracer* t, int on);
 /* refine() restricted to rows [y0, y0 + rows): the per-GPU share of a
  * frame split by row tiles across GPUs (sample indices and the samples()
  * count advance exactly as for refine). */

@@ -223,7 +223,10 @@ _SIGS = {
     "oxpt_tracer_size": (None, [vp, C.POINTER(u32), C.POINTER(u32)]),
     "oxpt_tracer_sync": (cint, [vp, vp, C.POINTER(RenderOptions), C.POINTER(cint)]),
     "oxpt_tracer_refine": (cint, [vp, u32]),
-    "oxpt_tracer_set_gpu_build": (None, [vp, cint]),
+    "oxpt_tracer_set_gpu_prepare": (None, [vp, cint]),
+    "oxpt_build_scene": (cint, [vp, vp, vp, vp]),
+    "oxpt_read_scene": (cint, [vp, vp, vp, vp]),
+    "oxpt_diag_scene_build": (cint, [vp, vp]),
     "oxpt_tracer_refine_rows": (cint, [vp, u32, u32, u32]),
     "oxpt_tracers_refine_batch": (cint, [C.POINTER(vp), u32, C.POINTER(u32), vp]),
     "oxpt_tracer_finish": (cint, [vp]),

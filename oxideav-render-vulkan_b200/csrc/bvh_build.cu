@@ -440,9 +440,8 @@ __global__ void emit(const Job* jobs, uint32_t K, const Decision* dec, const uin
 }  // namespace bvhb
 }  // namespace oxd
 
-namespace oxpt {
-
-using namespace oxd::bvhb;
+namespace oxd {
+namespace bvhb {
 
 #define BK(expr)                                                         \
     do {                                                                 \
@@ -454,40 +453,36 @@ using namespace oxd::bvhb;
         }                                                                \
     } while (0)
 
-bool build_bvh_device(int device, const std::vector<float>& tri_pos, BvhBuild* out, std::string* err) {
-    const uint32_t n = (uint32_t)(tri_pos.size() / 9);
-    *out = BvhBuild{};
+bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** words_out, uint32_t** slots_out,
+                     uint32_t* nodes_out, uint32_t* depth_out, std::string* err) {
+    *words_out = *slots_out = nullptr;
+    *nodes_out = *depth_out = 0;
     if (n == 0) return true;
     if (n > (1u << 30)) {
         if (err) *err = "bvh build: too many triangles";
         return false;
     }
     bool ok = true;
-    float* pos = nullptr;
     float4 *blo = nullptr, *bhi = nullptr, *cen = nullptr;
     uint32_t *ids = nullptr, *ids2 = nullptr, *words = nullptr, *excl = nullptr, *sums = nullptr, *total = nullptr;
+    uint32_t splits_host = 0;  // pageable: the copy completes before the sync returns
     Job *jobs = nullptr, *next = nullptr;
     Decision* dec = nullptr;
-    cudaStream_t st = nullptr;
     const size_t max_nodes = 2 * (size_t)n;
     const size_t max_jobs = (size_t)n;  // nodes of one level
     uint32_t K = 1, nodes = 1, levels = 0;
-    BK(cudaSetDevice(device));
-    BK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    BK(cudaMalloc((void**)&pos, tri_pos.size() * 4));
-    BK(cudaMalloc((void**)&blo, (size_t)n * 16));
-    BK(cudaMalloc((void**)&bhi, (size_t)n * 16));
-    BK(cudaMalloc((void**)&cen, (size_t)n * 16));
-    BK(cudaMalloc((void**)&ids, (size_t)n * 4));
-    BK(cudaMalloc((void**)&ids2, (size_t)n * 4));
-    BK(cudaMalloc((void**)&words, max_nodes * 32));
-    BK(cudaMalloc((void**)&jobs, max_jobs * sizeof(Job)));
-    BK(cudaMalloc((void**)&next, max_jobs * sizeof(Job)));
-    BK(cudaMalloc((void**)&dec, max_jobs * sizeof(Decision)));
-    BK(cudaMalloc((void**)&excl, max_jobs * 4));
-    BK(cudaMalloc((void**)&sums, 1024 * 4));
-    BK(cudaMalloc((void**)&total, 4));
-    BK(cudaMemcpyAsync(pos, tri_pos.data(), tri_pos.size() * 4, cudaMemcpyHostToDevice, st));
+    BK(cudaMallocAsync((void**)&blo, (size_t)n * 16, st));
+    BK(cudaMallocAsync((void**)&bhi, (size_t)n * 16, st));
+    BK(cudaMallocAsync((void**)&cen, (size_t)n * 16, st));
+    BK(cudaMallocAsync((void**)&ids, (size_t)n * 4, st));
+    BK(cudaMallocAsync((void**)&ids2, (size_t)n * 4, st));
+    BK(cudaMallocAsync((void**)&words, max_nodes * 32, st));
+    BK(cudaMallocAsync((void**)&jobs, max_jobs * sizeof(Job), st));
+    BK(cudaMallocAsync((void**)&next, max_jobs * sizeof(Job), st));
+    BK(cudaMallocAsync((void**)&dec, max_jobs * sizeof(Decision), st));
+    BK(cudaMallocAsync((void**)&excl, max_jobs * 4, st));
+    BK(cudaMallocAsync((void**)&sums, 1024 * 4, st));
+    BK(cudaMallocAsync((void**)&total, 4, st));
     tri_prep<<<(n + 255) / 256, 256, 0, st>>>(pos, n, blo, bhi, cen, ids);
     BK(cudaGetLastError());
     {
@@ -514,25 +509,62 @@ bool build_bvh_device(int device, const std::vector<float>& tri_pos, BvhBuild* o
         BK(cudaGetLastError());
         emit<<<(K + 127) / 128, 128, 0, st>>>(jobs, K, dec, excl, sums, nodes, words, next);
         BK(cudaGetLastError());
-        uint32_t splits = 0;
-        BK(cudaMemcpyAsync(&splits, total, 4, cudaMemcpyDeviceToHost, st));
+        BK(cudaMemcpyAsync(&splits_host, total, 4, cudaMemcpyDeviceToHost, st));
         BK(cudaStreamSynchronize(st));
-        nodes += 2 * splits;
-        K = 2 * splits;
+        nodes += 2 * splits_host;
+        K = 2 * splits_host;
         std::swap(jobs, next);
         std::swap(ids, ids2);
+    }
+    *words_out = words;
+    *slots_out = ids;
+    words = ids = nullptr;
+    *nodes_out = nodes;
+    *depth_out = levels;
+done:
+    void* ptrs[] = {blo, bhi, cen, ids, ids2, words, excl, sums, total, jobs, next, dec};
+    for (void* p : ptrs)
+        if (p) cudaFreeAsync(p, st);  // stream-ordered: no device-wide synchronisation
+    if (!ok) cudaStreamSynchronize(st);
+    return ok;
+}
+
+}  // namespace bvhb
+}  // namespace oxd
+
+namespace oxpt {
+
+bool build_bvh_device(int device, const std::vector<float>& tri_pos, BvhBuild* out, std::string* err) {
+    const uint32_t n = (uint32_t)(tri_pos.size() / 9);
+    *out = BvhBuild{};
+    if (n == 0) return true;
+    bool ok = true;
+    float* pos = nullptr;
+    uint32_t *words = nullptr, *slots = nullptr, nodes = 0, depth = 0;
+    cudaStream_t st = nullptr;
+    BK(cudaSetDevice(device));
+    BK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    BK(cudaMalloc((void**)&pos, tri_pos.size() * 4));
+    BK(cudaMemcpyAsync(pos, tri_pos.data(), tri_pos.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!oxd::bvhb::build_on_device(pos, n, st, &words, &slots, &nodes, &depth, err)) {
+        ok = false;
+        goto done;
     }
     out->node_words.resize((size_t)nodes * 8);
     out->slots.resize(n);
     BK(cudaMemcpyAsync(out->node_words.data(), words, (size_t)nodes * 32, cudaMemcpyDeviceToHost, st));
-    BK(cudaMemcpyAsync(out->slots.data(), ids, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    BK(cudaMemcpyAsync(out->slots.data(), slots, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
     BK(cudaStreamSynchronize(st));
-    out->depth = levels;
+    out->depth = depth;
 done:
-    void* ptrs[] = {pos, blo, bhi, cen, ids, ids2, words, excl, sums, total, jobs, next, dec};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
-    if (st) cudaStreamDestroy(st);
+    if (st) cudaStreamSynchronize(st);
+    if (pos) cudaFree(pos);
+    if (words) cudaFreeAsync(words, st);
+    if (slots) cudaFreeAsync(slots, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
     if (!ok) *out = BvhBuild{};
     return ok;
 }

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -27,6 +28,7 @@
 #include "nrc_state.hpp"
 #include "../host/batch.hpp"
 #include "../host/bvh4.hpp"
+#include "scene_prep.cuh"
 
 struct oxpt_ctx {
     int device = 0;
@@ -116,6 +118,7 @@ struct oxpt_ctx {
     std::vector<uint64_t> bgraph_key;
     uint64_t graph_builds = 0;
     unsigned long long* dev_tally = nullptr;  // graph loops: kernels launched, iterations
+    float build_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last oxpt_build_scene: phases, wall, tree, launches
 };
 
 namespace {
@@ -589,11 +592,9 @@ oxpt_status oxpt_device_summary(const oxpt_ctx* c, char* buf, size_t len) {
 
 // Collapse the uploaded binary tree into the four-wide any-hit tree; a
 // tree that does not collapse exactly keeps the binary walk.
-static oxpt_status upload_bvh4(oxpt_ctx* c, const oxpt_scene_desc* d) {
+static oxpt_status install_bvh4(oxpt_ctx* c, bool ok, const std::vector<uint32_t>& words, uint32_t root) {
     c->bvh4_built = false;
-    std::vector<uint32_t> words;
-    uint32_t root = 0xffffffffu;
-    if (!oxpt::build_bvh4(d->geom, d->node_count, &words, &root)) return realloc_dev(c, &c->bvh4, 0, "bvh4");
+    if (!ok) return realloc_dev(c, &c->bvh4, 0, "bvh4");
     oxpt_status s = realloc_dev(c, &c->bvh4, words.size() * 4, "four-wide tree");
     if (s) return s;
     if (!words.empty()) {
@@ -606,6 +607,13 @@ static oxpt_status upload_bvh4(oxpt_ctx* c, const oxpt_scene_desc* d) {
     c->bvh4_need = oxpt::bvh4_stack_need(words, root);
     c->bvh4_built = true;
     return OXPT_OK;
+}
+
+static oxpt_status upload_bvh4(oxpt_ctx* c, const uint32_t* node_words, uint32_t node_count) {
+    std::vector<uint32_t> words;
+    uint32_t root = 0xffffffffu;
+    bool ok = oxpt::build_bvh4(node_words, node_count, &words, &root);
+    return install_bvh4(c, ok, words, root);
 }
 
 oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
@@ -637,8 +645,62 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     c->node_count = d->node_count;
     c->bvh_depth = bvh_depth_of(d->geom, d->node_count);
     if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
-    if ((s = upload_bvh4(c, d))) return s;
+    if ((s = upload_bvh4(c, d->geom, d->node_count))) return s;
     c->has_scene = true;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* light_slots, uint32_t out[3]) {
+    if (!c || !src || !out) return fail(c, OXPT_E_INVALID, "null argument");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before scene build");
+    c->has_scene = false;
+    drop_borrowed_scene(c);
+    // The old scene's buffers go first: the build needs the room.
+    realloc_dev(c, &c->geom, 0, "geom buffer");
+    realloc_dev(c, &c->attrs, 0, "attribute buffer");
+    realloc_dev(c, &c->atlas, 0, "texture atlas");
+    realloc_dev(c, &c->bvh4, 0, "four-wide tree");
+    c->bvh4_built = false;
+    auto t0 = std::chrono::steady_clock::now();
+    oxd::prep::DeviceScene ds;
+    std::string e;
+    if ((s = oxd::prep::build_scene(*src, c->stream, &ds, light_slots, &e))) return fail(c, s, e);
+    auto t1 = std::chrono::steady_clock::now();
+    c->geom = ds.geom;
+    c->geom_vec4 = ds.geom_vec4;
+    c->attrs = ds.attrs;
+    c->slot_count = ds.slot_count;
+    c->atlas = ds.atlas;
+    c->side = src->atlas_side;
+    c->layers = src->atlas_layers;
+    c->node_count = ds.node_count;
+    c->bvh_depth = std::min(ds.depth, 65u);  // bvh_depth_of's cap
+    if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
+    if ((s = install_bvh4(c, ds.bvh4_ok, ds.bvh4_words, ds.bvh4_root))) return s;
+    auto t2 = std::chrono::steady_clock::now();
+    for (int k = 0; k < 4; k++) c->build_ms[k] = ds.phase_ms[k];
+    c->build_ms[4] = std::chrono::duration<float, std::milli>(t2 - t0).count();
+    c->build_ms[5] = std::chrono::duration<float, std::milli>(t2 - t1).count();
+    c->build_ms[6] = (float)ds.launches;
+    c->has_scene = true;
+    out[0] = ds.node_count;
+    out[1] = (uint32_t)ds.slot_count;
+    out[2] = ds.depth;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_read_scene(oxpt_ctx* c, uint32_t* geom, float* attrs, uint16_t* atlas) {
+    if (!c || !geom || !attrs || !atlas) return fail(c, OXPT_E_INVALID, "null argument");
+    if (!c->has_scene) return fail(c, OXPT_E_INVALID, "no scene");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "sync before scene readback");
+    CK(c, cudaMemcpy(geom, c->geom, c->geom_vec4 * 16, cudaMemcpyDeviceToHost), "geom readback");
+    CK(c, cudaMemcpy(attrs, c->attrs, c->slot_count * 48 * 4, cudaMemcpyDeviceToHost), "attribute readback");
+    CK(c, cudaMemcpy(atlas, c->atlas, (size_t)c->side * c->side * c->layers * 8, cudaMemcpyDeviceToHost),
+       "atlas readback");
     return OXPT_OK;
 }
 
@@ -1116,6 +1178,12 @@ oxpt_status oxpt_ctx_memory(const oxpt_ctx* c, uint64_t out[4]) {
 oxpt_status oxpt_diag_graph_builds(const oxpt_ctx* c, uint64_t* out) {
     if (!c || !out) return OXPT_E_INVALID;
     *out = c->graph_builds;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_scene_build(const oxpt_ctx* c, float ms[8]) {
+    if (!c || !ms) return OXPT_E_INVALID;
+    for (int k = 0; k < 8; k++) ms[k] = c->build_ms[k];
     return OXPT_OK;
 }
 

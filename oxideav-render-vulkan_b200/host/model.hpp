@@ -130,11 +130,18 @@ struct SceneBuffers {
     uint32_t n_punctual = 0, n_emissive = 0;
     uint32_t off_sobol = 0, off_sheen = 0, off_mat = 0, off_plights = 0, off_elights = 0;
     uint32_t bvh_depth = 0;
+    bool on_device = false;  // geom / attrs / atlas were built on the device
 };
-// `builder` (optional) replaces build_bvh, e.g. with the GPU build.
-std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
-                                           BvhBuild (*builder)(const std::vector<float>&, void*) = nullptr,
-                                           void* builder_arg = nullptr);
+// Builds geom / attrs / atlas on a device instead of the host
+// (oxpt_build_scene): gets the scene's sources, writes the leaf slot of
+// each light triangle and {node_count, slot_count, depth}.
+using DeviceFlatten = oxpt_status (*)(const oxpt_scene_src& src, uint32_t* light_slots, uint32_t out[3], void* arg);
+// With `device`, the BVH, slot flattening and atlas texels are built there
+// (SceneBuffers::on_device; geom / attrs / atlas stay empty on the host);
+// on its failure this returns null with *status set. Scenes without
+// triangles are always prepared on the host.
+std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight, DeviceFlatten device = nullptr,
+                                           void* device_arg = nullptr, oxpt_status* status = nullptr);
 
 // ensure_binding(): final tables (scene + env) and Params.
 void bind_params(const SceneBuffers& sb, const EnvWords* env, const ResolvedCamera& cam,

@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 
+#include "../csrc/f16pack.h"
 #include "model.hpp"
 
 namespace oxpt {
@@ -111,29 +112,7 @@ struct Placed {
 // f32 -> f16 (src/scene.rs:242-272): round to nearest even, overflow to
 // infinity, subnormals, NaN kept quiet.
 // ---------------------------------------------------------------------
-uint16_t f32_to_f16(float v) {
-    uint32_t bits = fbits(v);
-    uint16_t sign = (uint16_t)((bits >> 16) & 0x8000u);
-    int32_t exp = (int32_t)((bits >> 23) & 0xffu);
-    uint32_t mant = bits & 0x007fffffu;
-    if (exp == 0xff) return (uint16_t)(sign | 0x7c00u | (mant ? 0x200u : 0u));
-    int32_t e = exp - 127 + 15;
-    if (e >= 0x1f) return (uint16_t)(sign | 0x7c00u);
-    if (e <= 0) {
-        if (e < -10) return sign;
-        uint32_t m = mant | 0x00800000u;
-        uint32_t shift = (uint32_t)(14 - e);
-        uint32_t half = m >> shift;
-        uint32_t rem = m & ((1u << shift) - 1u);
-        uint32_t mid = 1u << (shift - 1u);
-        bool round = rem > mid || (rem == mid && (half & 1u));
-        return (uint16_t)(sign | (half + (round ? 1u : 0u)));
-    }
-    uint32_t half = ((uint32_t)e << 10) | (mant >> 13);
-    uint32_t rem = mant & 0x1fffu;
-    bool round = rem > 0x1000u || (rem == 0x1000u && (half & 1u));
-    return (uint16_t)(sign | (half + (round ? 1u : 0u)));
-}
+uint16_t f32_to_f16(float v) { return fm_f32_to_f16(v); }
 
 // ---------------------------------------------------------------------
 // Sobol' direction numbers for 4 dimensions x 32 bits, MSB-first (the
@@ -353,8 +332,25 @@ ResolvedCamera resolve_camera(const Framing& fr, const oxpt_render_options& o, u
 // ---------------------------------------------------------------------
 // upload (src/pathtrace.rs:970-1239).
 // ---------------------------------------------------------------------
-std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
-                                           BvhBuild (*builder)(const std::vector<float>&, void*), void* builder_arg) {
+namespace {
+
+// Level sizes of a mip chain: each level halves (at least 1) down to 1 x 1,
+// as Texture::mips builds them.
+std::vector<std::pair<uint32_t, uint32_t>> chain_dims(uint32_t w, uint32_t h) {
+    std::vector<std::pair<uint32_t, uint32_t>> d{{w, h}};
+    while (w > 1 || h > 1) {
+        w = std::max(1u, w / 2);
+        h = std::max(1u, h / 2);
+        d.push_back({w, h});
+    }
+    return d;
+}
+
+}  // namespace
+
+std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight, DeviceFlatten device,
+                                           void* device_arg, oxpt_status* status) {
+    if (status) *status = OXPT_OK;
     auto sb = std::make_unique<SceneBuffers>();
     // Materials: meshes without one use a trailing glTF default.
     std::vector<oxpt_material> materials = s.materials;
@@ -367,119 +363,56 @@ std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
             materials.push_back(d);
             break;
         }
-    // Triangle soup in global-id order.
+    auto mesh_mat = [&](const Mesh& m) {
+        return (m.material < 0 || (size_t)m.material >= s.materials.size()) ? (uint32_t)default_mat
+                                                                            : (uint32_t)m.material;
+    };
     size_t ntri = 0;
     for (auto& m : s.meshes) ntri += m.ntri;
-    std::vector<float> pos;
-    pos.reserve(ntri * 9);
-    struct Ref {
-        uint32_t mesh, tri;
-    };
-    std::vector<Ref> refs;
-    refs.reserve(ntri);
-    for (uint32_t mi = 0; mi < s.meshes.size(); mi++) {
-        auto& m = s.meshes[mi];
-        pos.insert(pos.end(), m.pos.begin(), m.pos.begin() + (size_t)m.ntri * 9);
-        for (uint32_t t = 0; t < m.ntri; t++) refs.push_back({mi, t});
-    }
-    auto mat_of = [&](uint32_t g) {
-        int32_t m = s.meshes[refs[g].mesh].material;
-        return (m < 0 || (size_t)m >= s.materials.size()) ? (uint32_t)default_mat : (uint32_t)m;
-    };
+    if (ntri == 0) device = nullptr;  // nothing to build on the device
     // Emissive lights: non-unlit triangles with a positive emissive factor
     // and area; pmf proportional to area x mean emissive factor (float64).
+    // Global ids run through the meshes in order.
     std::vector<uint32_t> light_tris;
     std::vector<double> power;
-    for (uint32_t g = 0; g < ntri; g++) {
-        const oxpt_material& m = materials[mat_of(g)];
-        if (m.unlit) continue;
-        if (!(m.emissive[0] > 0 || m.emissive[1] > 0 || m.emissive[2] > 0)) continue;
-        const float* p = &pos[(size_t)g * 9];
-        double e1[3], e2[3];
-        for (int k = 0; k < 3; k++) {
-            e1[k] = (double)p[3 + k] - p[k];
-            e2[k] = (double)p[6 + k] - p[k];
+    {
+        uint32_t g = 0;
+        for (auto& mesh : s.meshes) {
+            const oxpt_material& m = materials[mesh_mat(mesh)];
+            if (m.unlit || !(m.emissive[0] > 0 || m.emissive[1] > 0 || m.emissive[2] > 0)) {
+                g += mesh.ntri;
+                continue;
+            }
+            double le = (std::fmax(m.emissive[0], 0.0f) + std::fmax(m.emissive[1], 0.0f) +
+                         std::fmax(m.emissive[2], 0.0f)) / 3.0;
+            for (uint32_t t = 0; t < mesh.ntri; t++, g++) {
+                const float* p = &mesh.pos[(size_t)t * 9];
+                double e1[3], e2[3];
+                for (int k = 0; k < 3; k++) {
+                    e1[k] = (double)p[3 + k] - p[k];
+                    e2[k] = (double)p[6 + k] - p[k];
+                }
+                double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                       cz = e1[0] * e2[1] - e1[1] * e2[0];
+                double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+                if (!(area > 0.0) || !(le > 0.0)) continue;
+                light_tris.push_back(g);
+                power.push_back(area * le);
+            }
         }
-        double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
-               cz = e1[0] * e2[1] - e1[1] * e2[0];
-        double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
-        double le = (std::fmax(m.emissive[0], 0.0f) + std::fmax(m.emissive[1], 0.0f) +
-                     std::fmax(m.emissive[2], 0.0f)) / 3.0;
-        if (!(area > 0.0) || !(le > 0.0)) continue;
-        light_tris.push_back(g);
-        power.push_back(area * le);
     }
-    std::vector<uint32_t> lookup(ntri, NONE);
-    for (uint32_t li = 0; li < light_tris.size(); li++) lookup[light_tris[li]] = li;
     double total_power = 0.0;
     for (double p : power) total_power += p;
-    // BVH.
-    BvhBuild bvh = builder ? builder(pos, builder_arg) : build_bvh(pos);
-    sb->bvh_depth = bvh.depth;
-    sb->node_count = (uint32_t)(bvh.node_words.size() / 8);
-    sb->tri_base = sb->node_count * 2;
-    sb->slot_count = (uint32_t)bvh.slots.size();
-    std::vector<uint32_t> slot_of(ntri, NONE);
-    for (uint32_t sl = 0; sl < bvh.slots.size(); sl++) slot_of[bvh.slots[sl]] = sl;
-    auto& geom = sb->geom;
-    geom = std::move(bvh.node_words);
-    geom.reserve(geom.size() + (size_t)sb->slot_count * 12);
-    auto& attrs = sb->attrs;
-    attrs.reserve((size_t)sb->slot_count * 48);
-    for (uint32_t g : bvh.slots) {
-        const float* p = &pos[(size_t)g * 9];
-        uint32_t ws[3] = {g, lookup[g], mat_of(g)};
-        for (int v = 0; v < 3; v++) {
-            geom.push_back(fbits(p[v * 3]));
-            geom.push_back(fbits(p[v * 3 + 1]));
-            geom.push_back(fbits(p[v * 3 + 2]));
-            geom.push_back(ws[v]);
-        }
-        // push_attrs (src/pathtrace.rs:1274-1315).
-        const Mesh& m = s.meshes[refs[g].mesh];
-        uint32_t t = refs[g].tri;
-        bool normals = !m.nrm.empty(), tangents = !m.tan.empty(), colors = !m.col.empty();
-        bool uv0 = !m.uv0.empty(), uv1 = !m.uv1.empty();
-        uint32_t flags = (normals ? 1u : 0u) | (tangents ? 1u : 0u) << 1 | (colors ? 1u : 0u) << 2 |
-                         (uv0 ? 1u : 0u) << 3 | (uv1 ? 1u : 0u) << 4;
-        float flagf;
-        std::memcpy(&flagf, &flags, 4);
-        for (int v = 0; v < 3; v++) {
-            for (int k = 0; k < 3; k++) attrs.push_back(normals ? m.nrm[(size_t)t * 9 + v * 3 + k] : 0.0f);
-            attrs.push_back(v == 0 ? flagf : 0.0f);
-        }
-        for (int v = 0; v < 3; v++)
-            for (int k = 0; k < 4; k++) attrs.push_back(tangents ? m.tan[(size_t)t * 12 + v * 4 + k] : 0.0f);
-        for (int v = 0; v < 3; v++) {
-            attrs.push_back(uv0 ? m.uv0[(size_t)t * 6 + v * 2] : 0.0f);
-            attrs.push_back(uv0 ? m.uv0[(size_t)t * 6 + v * 2 + 1] : 0.0f);
-            attrs.push_back(uv1 ? m.uv1[(size_t)t * 6 + v * 2] : 0.0f);
-            attrs.push_back(uv1 ? m.uv1[(size_t)t * 6 + v * 2 + 1] : 0.0f);
-        }
-        for (int v = 0; v < 3; v++)
-            for (int k = 0; k < 4; k++) attrs.push_back(colors ? m.col[(size_t)t * 12 + v * 4 + k] : 1.0f);
-    }
-    if (geom.empty()) geom.resize(8, 0);
-    if (attrs.empty()) attrs.resize(48, 0.0f);
 
-    // ---- Tables.
-    auto& t = sb->tables;
-    sb->off_sobol = (uint32_t)t.size();
-    uint32_t dirs[128];
-    sobol_directions(dirs);
-    t.insert(t.end(), dirs, dirs + 128);
-    sb->off_sheen = (uint32_t)t.size();
-    const float* lut = sheen_albedo_lut();
-    for (int i = 0; i < 512; i++) t.push_back(fbits(lut[i]));
-    // Texture descriptors keyed by (texture, sRGB), in key order.
-    std::map<std::pair<int32_t, bool>, uint32_t> descs;
+    // Atlas placement: shelf-pack every kept level, tallest first
+    // (AtlasBuilder::pack, src/pathtrace.rs:1512-1592). Only level sizes
+    // are needed here; texels are written below (host) or on the device.
+    std::map<std::pair<int32_t, bool>, uint32_t> descs;  // texture descriptors keyed by (texture, sRGB)
     for (auto& m : materials)
         for (int sl = 0; sl < OXPT_SLOT_COUNT; sl++) {
             int32_t ti = m.tex[sl].texture;
             if (ti >= 0 && (size_t)ti < s.textures.size()) descs[{ti, slot_srgb(sl)}] = 0;
         }
-    // Atlas: shelf-pack every kept level, tallest first
-    // (AtlasBuilder::pack, src/pathtrace.rs:1512-1592).
     std::vector<std::pair<int32_t, bool>> chains;
     for (auto& kv : descs) chains.push_back(kv.first);
     uint32_t biggest = 1;
@@ -495,12 +428,15 @@ std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
     };
     std::vector<Item> items;
     std::vector<Placed> placed(chains.size());
+    std::vector<uint32_t> chain_levels(chains.size());
     for (uint32_t ci = 0; ci < chains.size(); ci++) {
-        const auto& mips = s.textures[chains[ci].first].mips(chains[ci].second);
+        const Texture& tx = s.textures[chains[ci].first];
+        auto dims = chain_dims(tx.w, tx.h);
+        chain_levels[ci] = (uint32_t)dims.size();
         uint32_t skip = 0;
-        while (skip < mips.size() && (mips[skip].w > side || mips[skip].h > side)) skip++;
+        while (skip < dims.size() && (dims[skip].first > side || dims[skip].second > side)) skip++;
         placed[ci].skip = skip;
-        for (uint32_t li = skip; li < mips.size(); li++) items.push_back({ci, li, mips[li].w, mips[li].h});
+        for (uint32_t li = skip; li < dims.size(); li++) items.push_back({ci, li, dims[li].first, dims[li].second});
     }
     std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
         if (a.h != b.h) return a.h > b.h;
@@ -533,26 +469,156 @@ std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
         if (a.ci != b.ci) return a.ci < b.ci;
         return a.li < b.li;
     });
+    for (auto& pl : rects) placed[pl.ci].rects.push_back(pl.r);
     sb->atlas_side = side;
     sb->atlas_layers = layers;
-    sb->atlas.assign((size_t)side * side * 4 * layers, 0);
-    for (auto& pl : rects) {
-        const auto& mips = s.textures[chains[pl.ci].first].mips(chains[pl.ci].second);
-        const Mip& m = mips[pl.li];
-        uint16_t* dst = &sb->atlas[(size_t)pl.r.layer * side * side * 4];
-        for (uint32_t row = 0; row < pl.r.h; row++)
-            for (uint32_t col = 0; col < pl.r.w; col++) {
-                const float* tx = &m.texels[((size_t)row * pl.r.w + col) * 4];
-                size_t at = (((size_t)(pl.r.y + row)) * side + pl.r.x + col) * 4;
-                for (int c = 0; c < 4; c++) dst[at + c] = f32_to_f16(tx[c]);
+
+    std::vector<uint32_t> light_slot(light_tris.size(), NONE);
+    if (device) {
+        // BVH, slot flattening and atlas texels on the device.
+        std::vector<oxpt_mesh_src> msrc;
+        msrc.reserve(s.meshes.size());
+        for (auto& m : s.meshes) {
+            oxpt_mesh_src d{};
+            d.ntri = m.ntri;
+            d.material = mesh_mat(m);
+            d.pos = m.pos.data();
+            d.nrm = m.nrm.empty() ? nullptr : m.nrm.data();
+            d.tan = m.tan.empty() ? nullptr : m.tan.data();
+            d.uv0 = m.uv0.empty() ? nullptr : m.uv0.data();
+            d.uv1 = m.uv1.empty() ? nullptr : m.uv1.data();
+            d.col = m.col.empty() ? nullptr : m.col.data();
+            msrc.push_back(d);
+        }
+        std::vector<std::vector<uint32_t>> rect_words(chains.size());
+        std::vector<oxpt_chain_src> csrc(chains.size());
+        for (uint32_t ci = 0; ci < chains.size(); ci++) {
+            const Texture& tx = s.textures[chains[ci].first];
+            for (auto& r : placed[ci].rects) rect_words[ci].insert(rect_words[ci].end(), {r.layer, r.x, r.y, r.w | (r.h << 16)});
+            oxpt_chain_src& c = csrc[ci];
+            c.width = tx.w;
+            c.height = tx.h;
+            c.rgba = tx.rgba.data();
+            c.srgb_decode = (chains[ci].second && tx.srgb_encoded) ? 1u : 0u;
+            c.skip = placed[ci].skip;
+            c.n_rects = (uint32_t)placed[ci].rects.size();
+            c.rects = rect_words[ci].data();
+        }
+        oxpt_scene_src src{};
+        src.meshes = msrc.data();
+        src.n_meshes = (uint32_t)msrc.size();
+        src.light_tris = light_tris.data();
+        src.n_lights = (uint32_t)light_tris.size();
+        src.chains = csrc.data();
+        src.n_chains = (uint32_t)csrc.size();
+        src.atlas_side = side;
+        src.atlas_layers = layers;
+        uint32_t out[3] = {0, 0, 0};
+        oxpt_status st = device(src, light_slot.data(), out, device_arg);
+        if (st) {
+            if (status) *status = st;
+            return nullptr;
+        }
+        sb->on_device = true;
+        sb->node_count = out[0];
+        sb->slot_count = out[1];
+        sb->bvh_depth = out[2];
+        sb->tri_base = sb->node_count * 2;
+    } else {
+        // Triangle soup in global-id order.
+        std::vector<float> pos;
+        pos.reserve(ntri * 9);
+        struct Ref {
+            uint32_t mesh, tri;
+        };
+        std::vector<Ref> refs;
+        refs.reserve(ntri);
+        for (uint32_t mi = 0; mi < s.meshes.size(); mi++) {
+            auto& m = s.meshes[mi];
+            pos.insert(pos.end(), m.pos.begin(), m.pos.begin() + (size_t)m.ntri * 9);
+            for (uint32_t t = 0; t < m.ntri; t++) refs.push_back({mi, t});
+        }
+        std::vector<uint32_t> lookup(ntri, NONE);
+        for (uint32_t li = 0; li < light_tris.size(); li++) lookup[light_tris[li]] = li;
+        // BVH.
+        BvhBuild bvh = build_bvh(pos);
+        sb->bvh_depth = bvh.depth;
+        sb->node_count = (uint32_t)(bvh.node_words.size() / 8);
+        sb->tri_base = sb->node_count * 2;
+        sb->slot_count = (uint32_t)bvh.slots.size();
+        for (uint32_t sl = 0; sl < bvh.slots.size(); sl++) {
+            uint32_t g = bvh.slots[sl];
+            if (lookup[g] != NONE) light_slot[lookup[g]] = sl;
+        }
+        auto& geom = sb->geom;
+        geom = std::move(bvh.node_words);
+        geom.reserve(geom.size() + (size_t)sb->slot_count * 12);
+        auto& attrs = sb->attrs;
+        attrs.reserve((size_t)sb->slot_count * 48);
+        for (uint32_t g : bvh.slots) {
+            const float* p = &pos[(size_t)g * 9];
+            const Mesh& m = s.meshes[refs[g].mesh];
+            uint32_t ws[3] = {g, lookup[g], mesh_mat(m)};
+            for (int v = 0; v < 3; v++) {
+                geom.push_back(fbits(p[v * 3]));
+                geom.push_back(fbits(p[v * 3 + 1]));
+                geom.push_back(fbits(p[v * 3 + 2]));
+                geom.push_back(ws[v]);
             }
-        placed[pl.ci].rects.push_back(pl.r);
+            // push_attrs (src/pathtrace.rs:1274-1315).
+            uint32_t t = refs[g].tri;
+            bool normals = !m.nrm.empty(), tangents = !m.tan.empty(), colors = !m.col.empty();
+            bool uv0 = !m.uv0.empty(), uv1 = !m.uv1.empty();
+            uint32_t flags = (normals ? 1u : 0u) | (tangents ? 1u : 0u) << 1 | (colors ? 1u : 0u) << 2 |
+                             (uv0 ? 1u : 0u) << 3 | (uv1 ? 1u : 0u) << 4;
+            float flagf;
+            std::memcpy(&flagf, &flags, 4);
+            for (int v = 0; v < 3; v++) {
+                for (int k = 0; k < 3; k++) attrs.push_back(normals ? m.nrm[(size_t)t * 9 + v * 3 + k] : 0.0f);
+                attrs.push_back(v == 0 ? flagf : 0.0f);
+            }
+            for (int v = 0; v < 3; v++)
+                for (int k = 0; k < 4; k++) attrs.push_back(tangents ? m.tan[(size_t)t * 12 + v * 4 + k] : 0.0f);
+            for (int v = 0; v < 3; v++) {
+                attrs.push_back(uv0 ? m.uv0[(size_t)t * 6 + v * 2] : 0.0f);
+                attrs.push_back(uv0 ? m.uv0[(size_t)t * 6 + v * 2 + 1] : 0.0f);
+                attrs.push_back(uv1 ? m.uv1[(size_t)t * 6 + v * 2] : 0.0f);
+                attrs.push_back(uv1 ? m.uv1[(size_t)t * 6 + v * 2 + 1] : 0.0f);
+            }
+            for (int v = 0; v < 3; v++)
+                for (int k = 0; k < 4; k++) attrs.push_back(colors ? m.col[(size_t)t * 12 + v * 4 + k] : 1.0f);
+        }
+        if (geom.empty()) geom.resize(8, 0);
+        if (attrs.empty()) attrs.resize(48, 0.0f);
+        // Atlas texels.
+        sb->atlas.assign((size_t)side * side * 4 * layers, 0);
+        for (auto& pl : rects) {
+            const auto& mips = s.textures[chains[pl.ci].first].mips(chains[pl.ci].second);
+            const Mip& m = mips[pl.li];
+            uint16_t* dst = &sb->atlas[(size_t)pl.r.layer * side * side * 4];
+            for (uint32_t row = 0; row < pl.r.h; row++)
+                for (uint32_t col = 0; col < pl.r.w; col++) {
+                    const float* tx = &m.texels[((size_t)row * pl.r.w + col) * 4];
+                    size_t at = (((size_t)(pl.r.y + row)) * side + pl.r.x + col) * 4;
+                    for (int c = 0; c < 4; c++) dst[at + c] = f32_to_f16(tx[c]);
+                }
+        }
     }
+
+    // ---- Tables.
+    auto& t = sb->tables;
+    sb->off_sobol = (uint32_t)t.size();
+    uint32_t dirs[128];
+    sobol_directions(dirs);
+    t.insert(t.end(), dirs, dirs + 128);
+    sb->off_sheen = (uint32_t)t.size();
+    const float* lut = sheen_albedo_lut();
+    for (int i = 0; i < 512; i++) t.push_back(fbits(lut[i]));
+    // Texture descriptors, in key order.
     for (uint32_t ci = 0; ci < chains.size(); ci++) {
         const Texture& tx = s.textures[chains[ci].first];
-        const auto& mips = tx.mips(chains[ci].second);
         descs[chains[ci]] = (uint32_t)t.size();
-        t.insert(t.end(), {(uint32_t)mips.size(), sampler_flags(tx.sampler), tx.w, tx.h,
+        t.insert(t.end(), {chain_levels[ci], sampler_flags(tx.sampler), tx.w, tx.h,
                            placed[ci].skip, (uint32_t)placed[ci].rects.size(), 0u, 0u});
         for (auto& r : placed[ci].rects) t.insert(t.end(), {r.layer, r.x, r.y, r.w | (r.h << 16)});
     }
@@ -607,7 +673,7 @@ std::unique_ptr<SceneBuffers> upload_scene(const oxpt_scene& s, float headlight,
         acc += power[li];
         float cdf = li + 1 == light_tris.size() ? 1.0f : (float)(acc / total_power);
         float pmf = (float)(power[li] / total_power);
-        t.insert(t.end(), {fbits(cdf), fbits(pmf), light_tris[li], slot_of[light_tris[li]]});
+        t.insert(t.end(), {fbits(cdf), fbits(pmf), light_tris[li], light_slot[li]});
     }
     sb->n_emissive = (uint32_t)light_tris.size();
     return sb;

@@ -9,16 +9,14 @@
 #include <cstring>
 #include <unordered_map>
 
+#include "../csrc/f16pack.h"
 #include "model.hpp"
 
 using namespace oxpt;
 
 namespace {
 
-float srgb_decode(float c) {
-    if (c <= 0.04045f) return c / 12.92f;
-    return std::pow((c + 0.055f) / 1.055f, 2.4f);
-}
+float srgb_decode(float c) { return fm_srgb_decode(c); }
 
 // splitmix64: seeded, platform-independent random numbers for the
 // procedural scenes.

@@ -13,7 +13,6 @@
 #include "../../include/oxpt_batch.h"
 #include "../../include/oxpt_serve.h"
 #include "../../include/oxpt_nrc.h"
-#include "bvh_gpu.hpp"
 #include "model.hpp"
 
 namespace {
@@ -62,7 +61,7 @@ struct oxpt_tracer {
     // prepares itself (serving sessions); `cam` overrides the camera.
     const oxpt_tracer* owner = nullptr;
     std::optional<oxpt_camera> cam;
-    bool gpu_build = false;  // build the BVH on the context's GPU
+    bool gpu_prepare = false;  // BVH, slot flattening and atlas built on the context's GPU
     oxpt::Framing framing;
     std::optional<oxpt::Env> env;
     std::optional<oxpt::EnvWords> env_words;
@@ -89,16 +88,25 @@ struct oxpt_tracer {
         return OXPT_OK;
     }
 
-    static oxpt::BvhBuild device_build(const std::vector<float>& pos, void* arg) {
+    static oxpt_status device_flatten(const oxpt_scene_src& src, uint32_t* light_slots, uint32_t out[3], void* arg) {
         auto* t = static_cast<oxpt_tracer*>(arg);
-        oxpt::BvhBuild b;
-        std::string e;
-        if (oxpt::build_bvh_device(oxpt_ctx_device(t->ctx), pos, &b, &e)) return b;
-        return oxpt::build_bvh(pos);  // the device could not: the host builds the same tree
+        return t->check(oxpt_build_scene(t->ctx, &src, light_slots, out));
     }
 
     oxpt_status upload(const oxpt_scene& s, float headlight) {
-        auto sb = gpu_build ? oxpt::upload_scene(s, headlight, &device_build, this) : oxpt::upload_scene(s, headlight);
+        if (gpu_prepare) {
+            oxpt_status st = OXPT_OK;
+            auto sb = oxpt::upload_scene(s, headlight, &device_flatten, this, &st);
+            if (sb) {
+                framing = oxpt::framing_of(s);
+                scene = std::move(sb);
+                return OXPT_OK;
+            }
+            // A tree the device scan cannot hold is built by the host below;
+            // any other failure is the device's and is reported.
+            if (st != OXPT_E_LIMIT) return st;
+        }
+        auto sb = oxpt::upload_scene(s, headlight);
         oxpt_scene_desc d;
         d.geom = sb->geom.data();
         d.geom_words = sb->geom.size();
@@ -315,10 +323,10 @@ oxpt_status oxpt_tracer_refine_nrc(oxpt_tracer* t, oxpt_nrc* nrc, uint32_t frame
     return OXPT_OK;
 }
 
-void oxpt_tracer_set_gpu_build(oxpt_tracer* t, int on) {
+void oxpt_tracer_set_gpu_prepare(oxpt_tracer* t, int on) {
     if (!t) return;
-    if ((on != 0) != t->gpu_build) t->dirty = true;  // the next sync prepares again
-    t->gpu_build = on != 0;
+    if ((on != 0) != t->gpu_prepare) t->dirty = true;  // the next sync prepares again
+    t->gpu_prepare = on != 0;
 }
 
 oxpt_status oxpt_tracer_new_view(const oxpt_tracer* owner, oxpt_tracer** out) {
@@ -385,6 +393,18 @@ oxpt_status oxpt_tracer_prepared(oxpt_tracer* t, oxpt_prepared_view* v) {
     if (!t->scene) return t->fail(OXPT_E_INVALID, "no scene: sync first");
     oxpt_status s = t->ensure_binding();
     if (s) return s;
+    if (t->scene->on_device && t->scene->geom.empty()) {
+        // Built on the device: read the buffers back once.
+        auto& sb = *t->scene;
+        sb.geom.resize((size_t)sb.node_count * 8 + (size_t)sb.slot_count * 12);
+        sb.attrs.resize((size_t)sb.slot_count * 48);
+        sb.atlas.resize((size_t)sb.atlas_side * sb.atlas_side * sb.atlas_layers * 4);
+        s = t->check(oxpt_read_scene(t->ctx, sb.geom.data(), sb.attrs.data(), sb.atlas.data()));
+        if (s) {
+            sb.geom.clear();
+            return s;
+        }
+    }
     std::memset(v, 0, sizeof(*v));
     v->geom = t->scene->geom.data();
     v->geom_words = t->scene->geom.size();

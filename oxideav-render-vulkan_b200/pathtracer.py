@@ -382,10 +382,22 @@ class GpuPathTracer:
         N.lib().oxpt_device_summary(self.ctx, buf, 256)
         return buf.value.decode()
 
-    def set_gpu_build(self, on: bool = True):
-        """Build the BVH of the next preparation on this tracer's GPU (the
-        same tree as the host build)."""
-        N.lib().oxpt_tracer_set_gpu_build(self._h, int(bool(on)))
+    def set_gpu_prepare(self, on: bool = True):
+        """Prepare the scene on this tracer's GPU: BVH, leaf-slot
+        flattening and atlas texels (the host preparation's buffers, word
+        for word). Takes effect at the next sync."""
+        N.lib().oxpt_tracer_set_gpu_prepare(self._h, int(bool(on)))
+
+    def prepare_timing(self) -> dict:
+        """Milliseconds of the last device preparation: device time of the
+        source upload, BVH build, slot flattening and atlas (its own stream,
+        overlapping the others), host wall time of the whole call and of the
+        four-wide tree, and the kernels it launched."""
+        ms = (C.c_float * 8)()
+        st = N.lib().oxpt_diag_scene_build(self.ctx, ms)
+        if st != N.OK:
+            _raise(st, N.lib().oxpt_last_error(self.ctx).decode())
+        return dict(zip(("upload", "bvh", "flatten", "atlas", "total", "tree4", "launches"), list(ms)))
 
     def set_texture_resolver(self, resolver=None):
         N.lib().oxpt_tracer_set_texture_resolver(self._h)

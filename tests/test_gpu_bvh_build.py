@@ -1,8 +1,8 @@
 """GPU BVH build (csrc/bvh_build.cu) against the host builder
 (host/bvh.cpp): the same node words, slot order, node count and depth on
 real and adversarial triangle sets (coincident centroids, flat sets,
-negative zeros, huge and tiny triangles), and a tracer that builds on the
-GPU prepares the same buffers and renders the same accumulator."""
+negative zeros, huge and tiny triangles). The tracer's device preparation
+is covered by test_gpu_scene_prep.py."""
 from __future__ import annotations
 
 import ctypes as C
@@ -10,7 +10,6 @@ import ctypes as C
 import numpy as np
 import pytest
 
-import scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -61,18 +60,3 @@ def test_gpu_build_matches_the_host_build(pkg, which):
     assert (gn, gd) == (hn, hd)
     assert np.array_equal(gs, hs)
     assert np.array_equal(gw, hw)
-
-
-def test_tracer_with_gpu_build_prepares_and_renders_the_same(pkg):
-    opts = pkg.RenderOptions(width=48, height=32, path_trace=pkg.PathTraceOptions(samples_per_pixel=4))
-    a, b = pkg.GpuPathTracer(0), pkg.GpuPathTracer(0)
-    b.set_gpu_build(True)
-    scene = scenes.materials_scene(pkg)
-    a.sync(scene, opts)
-    b.sync(scene, opts)
-    pa, pb = a.prepared(), b.prepared()
-    assert np.array_equal(pa.geom, pb.geom) and np.array_equal(pa.attrs, pb.attrs)
-    assert np.array_equal(pa.tables, pb.tables)
-    a.refine(4)
-    b.refine(4)
-    assert np.array_equal(a.read_accum().view(np.uint32), b.read_accum().view(np.uint32))
