@@ -155,6 +155,14 @@ oxpt_status oxpt_diag_scene_build(const oxpt_ctx* ctx, float ms[8]);
  * more than 16 triangles). Needs no GPU. */
 oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint32_t* out, size_t cap,
                                  size_t* words, uint32_t* root, uint32_t* stack_need);
+/* The same collapse on `device` (the path scene uploads take), plus the
+ * binary tree's depth counted on the device (*depth) and by the host walk
+ * (*host_depth; both 65 when deeper than 64 levels or malformed). Equal
+ * outputs to oxpt_diag_bvh4_build; OXPT_E_INVALID when it refuses the
+ * tree, OXPT_E_LIMIT when the device pass leaves it to the host. */
+oxpt_status oxpt_diag_bvh4_build_device(int device, const uint32_t* geom, uint32_t node_count, uint32_t* out,
+                                        size_t cap, size_t* words, uint32_t* root, uint32_t* stack_need,
+                                        uint32_t* depth, uint32_t* host_depth);
 /* BVH of n triangles (tri_pos: 9 floats each) by the host builder
  * (on_gpu = 0) or the GPU builder on `device` (on_gpu = 1): node words
  * (8 per node, at most 2n nodes), leaf slot -> triangle, node count and

@@ -227,6 +227,7 @@ _SIGS = {
     "oxpt_build_scene": (cint, [vp, vp, vp, vp]),
     "oxpt_read_scene": (cint, [vp, vp, vp, vp]),
     "oxpt_diag_scene_build": (cint, [vp, vp]),
+    "oxpt_diag_bvh4_build_device": (cint, [cint, vp, C.c_uint32, vp, sz, vp, vp, vp, vp, vp]),
     "oxpt_tracer_refine_rows": (cint, [vp, u32, u32, u32]),
     "oxpt_tracers_refine_batch": (cint, [C.POINTER(vp), u32, C.POINTER(u32), vp]),
     "oxpt_tracer_finish": (cint, [vp]),

@@ -119,6 +119,7 @@ struct oxpt_ctx {
     uint64_t graph_builds = 0;
     unsigned long long* dev_tally = nullptr;  // graph loops: kernels launched, iterations
     float build_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last oxpt_build_scene: phases, wall, tree, launches
+    size_t geom_cap = 0, attrs_cap = 0, atlas_cap = 0;  // bytes of the owned scene buffers
 };
 
 namespace {
@@ -162,9 +163,21 @@ bool bvh4_usable(const oxpt_ctx* c) {
     return c->bvh4_built && c->params.env[3] == c->node_count && c->bvh_depth <= 64 && c->bvh4_need <= 64;
 }
 
+// Keeps an owned scene buffer that already holds `bytes` (and is at most
+// twice that) instead of freeing and allocating it again: a re-upload of the
+// same scene then costs only its copies.
+template <class T>
+oxpt_status reserve_dev(oxpt_ctx* c, T** p, size_t* cap, size_t bytes, const char* what) {
+    if (*p && bytes > 0 && *cap >= bytes && *cap / 2 <= bytes) return OXPT_OK;
+    oxpt_status s = realloc_dev(c, p, bytes, what);
+    *cap = s ? 0 : bytes;
+    return s;
+}
+
 // A borrowed scene is not freed here: the lending context owns it.
 void drop_borrowed_scene(oxpt_ctx* c) {
     if (!c->borrowed_scene) return;
+    c->geom_cap = c->attrs_cap = c->atlas_cap = 0;
     c->geom = nullptr;
     c->attrs = nullptr;
     c->atlas = nullptr;
@@ -616,6 +629,32 @@ static oxpt_status upload_bvh4(oxpt_ctx* c, const uint32_t* node_words, uint32_t
     return install_bvh4(c, ok, words, root);
 }
 
+// The four-wide tree of the scene now in c->geom, collapsed on the device
+// (the host collapse's words); a tree too wide or deep for the device pass
+// is read back and collapsed on the host.
+static oxpt_status device_bvh4(oxpt_ctx* c) {
+    c->bvh4_built = false;
+    realloc_dev(c, &c->bvh4, 0, "four-wide tree");
+    uint32_t* out = nullptr;
+    uint32_t n4 = 0, root = 0xffffffffu, need = 1;
+    std::string e;
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(c->geom);
+    oxd::Collapse r = oxd::collapse4_device(words, c->node_count, c->stream, &out, &n4, &root, &need, &e);
+    if (r == oxd::Collapse::FAILED) return fail(c, OXPT_E_CUDA, e);
+    if (r == oxd::Collapse::REFUSED) return OXPT_OK;  // the binary walk serves every ray
+    if (r == oxd::Collapse::UNSUPPORTED) {
+        std::vector<uint32_t> host((size_t)c->node_count * 8);
+        CK(c, cudaMemcpy(host.data(), c->geom, host.size() * 4, cudaMemcpyDeviceToHost), "node readback");
+        return upload_bvh4(c, host.data(), c->node_count);
+    }
+    c->bvh4 = reinterpret_cast<float4*>(out);
+    c->bvh4_nodes = n4;
+    c->bvh4_root = root;
+    c->bvh4_need = need;
+    c->bvh4_built = true;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     if (!c || !d) return fail(c, OXPT_E_INVALID, "null argument");
     if (!d->geom || d->geom_words < 8 || d->geom_words % 4 != 0) return fail(c, OXPT_E_INVALID, "geom must hold at least one node (8 words), a multiple of 4 words");
@@ -631,9 +670,9 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     drop_borrowed_scene(c);
     size_t gbytes = d->geom_words * 4, abytes = d->attr_floats * 4;
     size_t tbytes = (size_t)d->atlas_side * d->atlas_side * d->atlas_layers * 8;
-    if ((s = realloc_dev(c, &c->geom, gbytes, "geom buffer"))) return s;
-    if ((s = realloc_dev(c, &c->attrs, abytes, "attribute buffer"))) return s;
-    if ((s = realloc_dev(c, &c->atlas, tbytes, "texture atlas"))) return s;
+    if ((s = reserve_dev(c, &c->geom, &c->geom_cap, gbytes, "geom buffer"))) return s;
+    if ((s = reserve_dev(c, &c->attrs, &c->attrs_cap, abytes, "attribute buffer"))) return s;
+    if ((s = reserve_dev(c, &c->atlas, &c->atlas_cap, tbytes, "texture atlas"))) return s;
     CK(c, cudaMemcpyAsync(c->geom, d->geom, gbytes, cudaMemcpyHostToDevice, c->stream), "geom upload");
     CK(c, cudaMemcpyAsync(c->attrs, d->attrs, abytes, cudaMemcpyHostToDevice, c->stream), "attr upload");
     CK(c, cudaMemcpyAsync(c->atlas, d->atlas, tbytes, cudaMemcpyHostToDevice, c->stream), "atlas upload");
@@ -643,9 +682,17 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     c->side = d->atlas_side;
     c->layers = d->atlas_layers;
     c->node_count = d->node_count;
-    c->bvh_depth = bvh_depth_of(d->geom, d->node_count);
+    {
+        // Depth and four-wide tree from the uploaded words, on the device.
+        std::string e;
+        uint32_t depth = 0;
+        if (!oxd::binary_depth_device(reinterpret_cast<const uint32_t*>(c->geom), d->node_count, c->stream, &depth,
+                                      &e))
+            return fail(c, OXPT_E_CUDA, e);
+        c->bvh_depth = depth;
+    }
     if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
-    if ((s = upload_bvh4(c, d->geom, d->node_count))) return s;
+    if ((s = device_bvh4(c))) return s;
     c->has_scene = true;
     return OXPT_OK;
 }
@@ -661,6 +708,7 @@ oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* l
     realloc_dev(c, &c->geom, 0, "geom buffer");
     realloc_dev(c, &c->attrs, 0, "attribute buffer");
     realloc_dev(c, &c->atlas, 0, "texture atlas");
+    c->geom_cap = c->attrs_cap = c->atlas_cap = 0;
     realloc_dev(c, &c->bvh4, 0, "four-wide tree");
     c->bvh4_built = false;
     auto t0 = std::chrono::steady_clock::now();
@@ -670,6 +718,9 @@ oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* l
     auto t1 = std::chrono::steady_clock::now();
     c->geom = ds.geom;
     c->geom_vec4 = ds.geom_vec4;
+    c->geom_cap = ds.geom_vec4 * 16;
+    c->attrs_cap = ds.slot_count * 192;
+    c->atlas_cap = (size_t)src->atlas_side * src->atlas_side * src->atlas_layers * 8;
     c->attrs = ds.attrs;
     c->slot_count = ds.slot_count;
     c->atlas = ds.atlas;
@@ -678,7 +729,7 @@ oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* l
     c->node_count = ds.node_count;
     c->bvh_depth = std::min(ds.depth, 65u);  // bvh_depth_of's cap
     if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
-    if ((s = install_bvh4(c, ds.bvh4_ok, ds.bvh4_words, ds.bvh4_root))) return s;
+    if ((s = device_bvh4(c))) return s;
     auto t2 = std::chrono::steady_clock::now();
     for (int k = 0; k < 4; k++) c->build_ms[k] = ds.phase_ms[k];
     c->build_ms[4] = std::chrono::duration<float, std::milli>(t2 - t0).count();
@@ -735,6 +786,7 @@ oxpt_status oxpt_share_scene(oxpt_ctx* c, const oxpt_ctx* owner) {
     void* own[] = {c->geom, c->attrs, c->atlas, c->bvh4};
     for (void* p : own)
         if (p) cudaFree(p);
+    c->geom_cap = c->attrs_cap = c->atlas_cap = 0;
     c->geom = owner->geom;
     c->geom_vec4 = owner->geom_vec4;
     c->attrs = owner->attrs;
@@ -1207,6 +1259,46 @@ oxpt_status oxpt_diag_bvh4_build(const uint32_t* geom, uint32_t node_count, uint
     *stack_need = oxpt::bvh4_stack_need(w, r);
     if (out && cap >= w.size()) std::memcpy(out, w.data(), w.size() * 4);
     return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_bvh4_build_device(int device, const uint32_t* geom, uint32_t node_count, uint32_t* out,
+                                        size_t cap, size_t* words, uint32_t* root, uint32_t* stack_need,
+                                        uint32_t* depth, uint32_t* host_depth) {
+    if ((node_count && !geom) || !words || !root || !stack_need || !depth || !host_depth) return OXPT_E_INVALID;
+    *host_depth = bvh_depth_of(geom, node_count);
+    if (cudaSetDevice(device) != cudaSuccess) return OXPT_E_NODEV;
+    cudaStream_t st = nullptr;
+    uint32_t *d = nullptr, *o = nullptr;
+    uint32_t n4 = 0, r = 0xffffffffu, need = 1;
+    oxpt_status res = OXPT_OK;
+    std::string e;
+    oxd::Collapse c4 = oxd::Collapse::FAILED;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return OXPT_E_CUDA;
+    if (cudaMalloc((void**)&d, std::max<size_t>((size_t)node_count * 32, 32)) != cudaSuccess ||
+        cudaMemcpy(d, geom, (size_t)node_count * 32, cudaMemcpyHostToDevice) != cudaSuccess) {
+        res = OXPT_E_CUDA;
+        goto done;
+    }
+    if (!oxd::binary_depth_device(d, node_count, st, depth, &e)) {
+        res = OXPT_E_CUDA;
+        goto done;
+    }
+    c4 = oxd::collapse4_device(d, node_count, st, &o, &n4, &r, &need, &e);
+    if (c4 == oxd::Collapse::FAILED) res = OXPT_E_CUDA;
+    else if (c4 == oxd::Collapse::REFUSED) res = OXPT_E_INVALID;
+    else if (c4 == oxd::Collapse::UNSUPPORTED) res = OXPT_E_LIMIT;
+    else {
+        *words = (size_t)n4 * 32;
+        *root = r;
+        *stack_need = need;
+        if (out && cap >= *words && n4 && cudaMemcpy(out, o, *words * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            res = OXPT_E_CUDA;
+    }
+done:
+    if (o) cudaFree(o);
+    if (d) cudaFree(d);
+    cudaStreamDestroy(st);
+    return res;
 }
 
 oxpt_status oxpt_diag_wave_iterations(const oxpt_ctx* c, uint64_t* out) {

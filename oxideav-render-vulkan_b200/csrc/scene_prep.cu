@@ -29,7 +29,6 @@
 #include <thread>
 #include <vector>
 
-#include "../host/bvh4.hpp"
 #include "f16pack.h"
 #include "scene_prep.cuh"
 
@@ -480,6 +479,7 @@ oxpt_status build_scene(const oxpt_scene_src& src, cudaStream_t st, DeviceScene*
     AtlasJob job;
     std::thread worker;
     bool working = false;
+    uint32_t bvh_launches = 0;
 
 #define PK(expr, what)                                            \
     do {                                                          \
@@ -567,7 +567,7 @@ oxpt_status build_scene(const oxpt_scene_src& src, cudaStream_t st, DeviceScene*
     }
     PK(cudaEventRecord(ev[1], st), "timing");
     // BVH (syncs the stream once per level).
-    if (!bvhb::build_on_device(pos, n, st, &words, &slots, &ds.node_count, &ds.depth, err)) {
+    if (!bvhb::build_on_device(pos, n, st, &words, &slots, &ds.node_count, &ds.depth, &bvh_launches, err)) {
         // A level wider than the scan is a size limit (the host builds such
         // trees); anything else is the device's failure.
         status = err->find("wider") != std::string::npos ? OXPT_E_LIMIT
@@ -593,12 +593,7 @@ oxpt_status build_scene(const oxpt_scene_src& src, cudaStream_t st, DeviceScene*
     PK(cudaEventRecord(ev[3], st), "timing");
     if (src.n_lights)
         PK(cudaMemcpyAsync(light_slots, lslots, (size_t)src.n_lights * 4, cudaMemcpyDeviceToHost, st), "light slots");
-    ds.node_words.resize((size_t)ds.node_count * 8);
-    PK(cudaMemcpyAsync(ds.node_words.data(), words, (size_t)ds.node_count * 32, cudaMemcpyDeviceToHost, st),
-       "node readback");
     PK(cudaStreamSynchronize(st), "scene build");
-    // The four-wide any-hit tree (host collapse) while the atlas finishes.
-    ds.bvh4_ok = oxpt::build_bvh4(ds.node_words.data(), ds.node_count, &ds.bvh4_words, &ds.bvh4_root);
     worker.join();
     working = false;
     if (job.e != cudaSuccess) {
@@ -610,8 +605,8 @@ oxpt_status build_scene(const oxpt_scene_src& src, cudaStream_t st, DeviceScene*
     cudaEventElapsedTime(&ds.phase_ms[1], ev[1], ev[2]);
     cudaEventElapsedTime(&ds.phase_ms[2], ev[2], ev[3]);
     if (cudaEventElapsedTime(&ds.phase_ms[3], job.begin, job.end) != cudaSuccess) ds.phase_ms[3] = 0.0f;
-    // tri_prep, five kernels per level, flattening (+ two for lights), mip levels
-    ds.launches = 1 + 5 * ds.depth + 1 + (src.n_lights ? 2 : 0) + job.launches;
+    // the BVH's, flattening (+ two for lights), mip levels
+    ds.launches = bvh_launches + 1 + (src.n_lights ? 2 : 0) + job.launches;
     (void)cudaGetLastError();
     cudaFreeAsync(words, st);
     cudaFreeAsync(slots, st);

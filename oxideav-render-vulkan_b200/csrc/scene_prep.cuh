@@ -20,9 +20,22 @@ namespace bvhb {
 // for other streams' work. False with *err when an allocation or launch fails or a
 // level is wider than the level scan handles.
 bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** words, uint32_t** slots,
-                     uint32_t* nodes, uint32_t* depth, std::string* err);
+                     uint32_t* nodes, uint32_t* depth, uint32_t* launches, std::string* err);
 
 }  // namespace bvhb
+
+// Four-wide any-hit tree collapsed on the device from binary node words in
+// device memory (bvh4_build.cu): the host collapse's words (host/bvh4.cpp),
+// node for node. BUILT: *out (cudaMalloc, n4 x 32 words; null when the
+// root is a leaf), *root_ref and *need are set. REFUSED: the host collapse
+// refuses the tree too (keep the binary walk). UNSUPPORTED: too wide or
+// deep for the device pass (collapse on the host). FAILED: a CUDA error.
+enum class Collapse { BUILT, REFUSED, UNSUPPORTED, FAILED };
+Collapse collapse4_device(const uint32_t* words, uint32_t nodes, cudaStream_t st, uint32_t** out, uint32_t* n4,
+                          uint32_t* root_ref, uint32_t* need, std::string* err);
+// Levels of the binary tree (65 when deeper than 64 or malformed), as the
+// host's depth walk counts them.
+bool binary_depth_device(const uint32_t* words, uint32_t nodes, cudaStream_t st, uint32_t* depth, std::string* err);
 
 namespace prep {
 
@@ -34,11 +47,7 @@ struct DeviceScene {
     size_t slot_count = 0;
     uint2* atlas = nullptr;   // side x side x layers RGBA16F texels
     uint32_t node_count = 0, depth = 0;
-    std::vector<uint32_t> node_words;  // host copy of the nodes
-    // four-wide any-hit tree collapsed from node_words (host/bvh4.cpp)
-    bool bvh4_ok = false;
-    std::vector<uint32_t> bvh4_words;
-    uint32_t bvh4_root = 0xffffffffu;
+
     // Device time of the phases (CUDA events): source upload, BVH, slot
     // flattening, atlas (texel upload + mip chains, on its own stream).
     float phase_ms[4] = {0, 0, 0, 0};

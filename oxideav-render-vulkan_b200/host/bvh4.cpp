@@ -51,11 +51,6 @@ inline bool inside(const BNode& c, const BNode& p) {
     return sane(c);
 }
 
-// Both children of inner node n lie in its box.
-inline bool children_inside(const uint32_t* g, const BNode& n) {
-    return sane(n) && inside(bnode(g, n.first), n) && inside(bnode(g, n.first + 1), n);
-}
-
 inline float area(const BNode& n) {
     float e0 = n.hi[0] - n.lo[0], e1 = n.hi[1] - n.lo[1], e2 = n.hi[2] - n.lo[2];
     return e0 * e1 + e1 * e2 + e2 * e0;
@@ -79,65 +74,82 @@ bool build_bvh4(const uint32_t* geom, uint32_t nodes, std::vector<uint32_t>* out
     };
     BNode root = bnode(geom, 0);
     if (root.count > 0) return leaf_ref(root, root_ref);
+    // Every 4-wide node stands for a distinct binary inner node, and a
+    // binary tree of `nodes` nodes has at most nodes / 2 inner ones.
+    const size_t cap = (size_t)nodes / 2 + 1;
+    out->resize(cap * 32);  // zero-filled: padding words and unused child boxes stay 0
+    uint32_t* o = out->data();
+    size_t used = 1;
     // Work list of (binary node, 4-wide node index to fill).
-    std::vector<std::pair<uint32_t, uint32_t>> work;
-    out->resize(32, 0);
+    struct Item {
+        uint32_t b, dst;
+    };
+    std::vector<Item> work;
+    work.reserve(256);
     work.push_back({0u, 0u});
     *root_ref = 0u;
     uint64_t guard = 0;
     while (!work.empty()) {
-        auto [b, dst] = work.back();
+        Item it = work.back();
         work.pop_back();
         if (++guard > nodes) return false;
-        BNode n = bnode(geom, b);
-        if (n.count > 0 || (uint64_t)n.first + 1 >= nodes || !children_inside(geom, n)) return false;
-        std::vector<uint32_t> kids = {n.first, n.first + 1};
-        while (kids.size() < 4) {
+        BNode n = bnode(geom, it.b);
+        if (n.count > 0 || (uint64_t)n.first + 1 >= nodes) return false;
+        uint32_t kid[4] = {n.first, n.first + 1, 0, 0};
+        BNode kn[4];
+        kn[0] = bnode(geom, kid[0]);
+        kn[1] = bnode(geom, kid[1]);
+        if (!sane(n) || !inside(kn[0], n) || !inside(kn[1], n)) return false;
+        int nk = 2;
+        while (nk < 4) {
+            // Open the inner child of largest area (the first on ties).
             int best = -1;
             float best_a = -1.0f;
-            for (int k = 0; k < (int)kids.size(); k++) {
-                BNode c = bnode(geom, kids[k]);
-                if (c.count == 0 && area(c) > best_a) {
-                    best_a = area(c);
+            for (int k = 0; k < nk; k++) {
+                if (kn[k].count != 0) continue;
+                float a = area(kn[k]);
+                if (a > best_a) {
+                    best_a = a;
                     best = k;
                 }
             }
             if (best < 0) break;
-            BNode c = bnode(geom, kids[best]);
-            if ((uint64_t)c.first + 1 >= nodes || !children_inside(geom, c)) return false;
-            kids[best] = c.first;
-            kids.insert(kids.begin() + best + 1, c.first + 1);
+            const BNode c = kn[best];
+            if ((uint64_t)c.first + 1 >= nodes) return false;
+            BNode c0 = bnode(geom, c.first), c1 = bnode(geom, c.first + 1);
+            if (!sane(c) || !inside(c0, c) || !inside(c1, c)) return false;
+            for (int k = nk; k > best + 1; k--) {
+                kid[k] = kid[k - 1];
+                kn[k] = kn[k - 1];
+            }
+            kid[best] = c.first;
+            kn[best] = c0;
+            kid[best + 1] = c.first + 1;
+            kn[best + 1] = c1;
+            nk++;
         }
-        float* f = reinterpret_cast<float*>(out->data() + (size_t)dst * 32);
-        uint32_t* r = out->data() + (size_t)dst * 32 + 24;
+        float* f = reinterpret_cast<float*>(o + (size_t)it.dst * 32);
+        uint32_t* r = o + (size_t)it.dst * 32 + 24;
         for (int k = 0; k < 4; k++) {
-            if (k >= (int)kids.size()) {
-                // Empty child: skipped by its reference (its box is unused).
-                for (int a = 0; a < 3; a++) {
-                    f[a * 4 + k] = 0.0f;
-                    f[12 + a * 4 + k] = 0.0f;
-                }
-                r[k] = BVH4_EMPTY;
+            if (k >= nk) {
+                r[k] = BVH4_EMPTY;  // empty child: skipped by its reference (its box is unused, 0)
                 continue;
             }
-            BNode c = bnode(geom, kids[k]);
             for (int a = 0; a < 3; a++) {
-                f[a * 4 + k] = c.lo[a];
-                f[12 + a * 4 + k] = c.hi[a];
+                f[a * 4 + k] = kn[k].lo[a];
+                f[12 + a * 4 + k] = kn[k].hi[a];
             }
-            if (c.count > 0) {
-                if (!leaf_ref(c, &r[k])) return false;
+            if (kn[k].count > 0) {
+                if (!leaf_ref(kn[k], &r[k])) return false;
             } else {
-                uint32_t idx = (uint32_t)(out->size() / 32);
-                out->resize(out->size() + 32, 0);
-                // The resize may move the buffer: recompute r.
-                r = out->data() + (size_t)dst * 32 + 24;
-                f = reinterpret_cast<float*>(out->data() + (size_t)dst * 32);
-                r[k] = idx;
-                work.push_back({kids[k], idx});
+                if (used >= cap) return false;
+                r[k] = (uint32_t)used;
+                work.push_back({kid[k], (uint32_t)used});
+                used++;
             }
         }
     }
+    out->resize(used * 32);
     return true;
 }
 

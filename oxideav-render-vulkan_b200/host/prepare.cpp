@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 
 #include "../csrc/f16pack.h"
 #include "model.hpp"
@@ -274,22 +275,60 @@ EnvWords env_words(const Env& env) {
 // Camera::resolve stand-in: the scene camera when asked for, otherwise a
 // 45-degree pinhole on +z framing the scene bounds.
 // ---------------------------------------------------------------------
+// Bounds of every vertex for camera framing. A coordinate replaces the
+// running bound only when strictly beyond it (NaN never does), so the
+// result is the first extreme value in vertex order; pieces of the vertex
+// list are bounded on several threads and combined in order by the same
+// rule, which gives the same bits as one sequential pass.
 Framing framing_of(const oxpt_scene& s) {
     Framing f;
     f.cameras = s.cameras;
-    V3 lo{1e30f, 1e30f, 1e30f}, hi{-1e30f, -1e30f, -1e30f};
-    bool any = false;
-    for (auto& m : s.meshes)
-        for (size_t i = 0; i + 2 < m.pos.size(); i += 3) {
-            V3 p{m.pos[i], m.pos[i + 1], m.pos[i + 2]};
-            lo = vmin(lo, p);
-            hi = vmax(hi, p);
-            any = true;
-        }
-    if (any) {
-        f.lo = lo;
-        f.hi = hi;
+    struct Piece {
+        const float* p;
+        size_t n;  // vertices
+        float lo[3], hi[3];
+    };
+    const size_t PIECE = 1u << 18;
+    std::vector<Piece> pieces;
+    for (auto& m : s.meshes) {
+        size_t nv = m.pos.size() / 3;
+        for (size_t v = 0; v < nv; v += PIECE)
+            pieces.push_back({m.pos.data() + v * 3, std::min(PIECE, nv - v), {}, {}});
     }
+    if (pieces.empty()) return f;
+    auto bound = [](Piece& pc) {
+        float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+        for (size_t i = 0; i < pc.n; i++)
+            for (int k = 0; k < 3; k++) {
+                float x = pc.p[i * 3 + k];
+                lo[k] = x < lo[k] ? x : lo[k];
+                hi[k] = x > hi[k] ? x : hi[k];
+            }
+        for (int k = 0; k < 3; k++) {
+            pc.lo[k] = lo[k];
+            pc.hi[k] = hi[k];
+        }
+    };
+    unsigned threads = std::max(1u, std::min<unsigned>(8u, std::thread::hardware_concurrency()));
+    threads = (unsigned)std::min<size_t>(threads, pieces.size());
+    if (threads <= 1) {
+        for (auto& pc : pieces) bound(pc);
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < threads; t++)
+            pool.emplace_back([&, t] {
+                for (size_t i = t; i < pieces.size(); i += threads) bound(pieces[i]);
+            });
+        for (auto& th : pool) th.join();
+    }
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (auto& pc : pieces)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = pc.lo[k] < lo[k] ? pc.lo[k] : lo[k];
+            hi[k] = pc.hi[k] > hi[k] ? pc.hi[k] : hi[k];
+        }
+    f.lo = V3{lo[0], lo[1], lo[2]};
+    f.hi = V3{hi[0], hi[1], hi[2]};
     return f;
 }
 
