@@ -415,7 +415,7 @@ def run_prepare(a):
     # Source bytes that go up per step: positions, attribute streams, level-0 texels.
     h2d = tris * (36 + 36 + 24)  # positions, normals, uv0 (the icosphere's streams)
     h2d += 8 * a.tex * a.tex * 16  # level-0 texels of the 8 textures
-    d2h = prep.node_count * 32  # node words for the four-wide collapse
+    d2h = 512 * 4  # leaf slots of the emissive triangles (the four-wide tree is collapsed on the device)
     # Host preparation of the same scene (bounded sample: one run).
     host = pkg.GpuPathTracer(0)
     host.set_environment(env)
