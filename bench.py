@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--ref-spp", type=int, default=16384, help="nrc workload: spp of the plain reference")
     ap.add_argument("--nrc-scene", default="large", choices=["large", "cornell"], help="nrc workload: scene")
     ap.add_argument("--nrc-train-one-in", type=int, default=4, help="nrc workload: one training path in this many")
+    ap.add_argument("--nrc-query-bounce", type=int, default=2, help="nrc workload: paths end into the cache at the "
+                    "vertex hit by this ray")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve", "nrc", "prepare"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
@@ -621,7 +623,7 @@ def run_nrc(a):
     del plain
     nt = tracer()
     cache = RadianceCache(nt)
-    cache.configure(train_one_in=a.nrc_train_one_in)
+    cache.configure(train_one_in=a.nrc_train_one_in, query_bounce=a.nrc_query_bounce)
     nrc_curve = progress(nt, lambda n: cache.refine(n))
     q, smp = cache.frame_counts()
 
@@ -645,7 +647,8 @@ def run_nrc(a):
                                     "radiance cache: large scene (20 x freq^2 triangles) with the mixed material model")
                                    + f", {a.width}x{a.height}, 1 spp per frame, {a.frames} frames, 12 bounces",
                        "reference": f"plain tracer {a.ref_spp} spp ({ref_s:.1f} s)",
-                       "cache": "5 x 64 ReLU MLP, BF16 tcgen05, 12-frequency encoding, paths end after 2 bounces, "
+                       "cache": "5 x 64 ReLU MLP, BF16 tcgen05, 12-frequency encoding, paths end into the cache at the "
+                                f"vertex hit by ray {a.nrc_query_bounce}, "
                                 f"1 in {a.nrc_train_one_in} paths trains (suffix of 4 bounces into the cache), "
                                 "<= 65536 samples and one Adam step (lr 1e-2) per frame",
                        "timing": "host wall clock with a device sync per checkpoint; one untimed frame first"},
