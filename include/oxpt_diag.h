@@ -98,7 +98,8 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *   shade_variant  wavefront logic kernel compiled for 2 / 3 / 4 resident
  *                  blocks per SM (0 / 1 / 2): registers against occupancy.
  *   trace_variant  wavefront traversal kernels for 6 / 8 / 10 blocks.
- *   nee_variant    split wavefront NEE kernel for 4 / 5 / 6 blocks.
+ *   nee_variant    split wavefront NEE kernel: job-major (0, 1, 2) or
+ *                  vertex-major (3, 4, 5) for 4 / 5 / 6 blocks.
  *   OXPT_MODE_WAVEFRONT_SPLIT: the wavefront with the shading of a bounce
  *                  in three kernels (path logic, surface shading, one thread
  *                  per NEE job); shade_variant then applies to the shading

@@ -91,7 +91,7 @@ struct oxpt_ctx {
     uint32_t wave_slots = 1u << 20;
     uint64_t wave_items = 1ull << 24;
     uint32_t check_every = 4;
-    uint32_t shade_variant = 1, trace_variant = 0, nee_variant = 1, stack = 0;
+    uint32_t shade_variant = 1, trace_variant = 0, nee_variant = 3, stack = 0;
     uint32_t bvh_depth = 0;
     // four-wide any-hit tree (host/bvh4.cpp), built on upload when exact
     float4* bvh4 = nullptr;
@@ -1131,8 +1131,8 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     c->max_paths = t->max_paths ? t->max_paths : (1ull << 22);
     c->wave_items = t->wave_items ? t->wave_items : (1ull << 24);
     c->check_every = t->check_every ? t->check_every : 4u;
-    if (t->shade_variant > 2 || t->trace_variant > 2 || t->nee_variant > 2)
-        return fail(c, OXPT_E_INVALID, "variants are 0, 1 or 2");
+    if (t->shade_variant > 2 || t->trace_variant > 2 || t->nee_variant > 5)
+        return fail(c, OXPT_E_INVALID, "shade / trace variants are 0, 1 or 2; NEE variants 0 to 5");
     if (t->stack && t->stack != 32 && t->stack != 64) return fail(c, OXPT_E_INVALID, "stack is 0, 32 or 64");
     if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
     if (t->shadow_walk > 1) return fail(c, OXPT_E_INVALID, "shadow_walk is 0 or 1");

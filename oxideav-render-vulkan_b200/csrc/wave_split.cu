@@ -386,8 +386,45 @@ __global__ void __launch_bounds__(128, MINB) split_nee(const __grid_constant__ W
     }
 }
 
+// The same NEE jobs vertex-major: one thread per vertex loads its record
+// once and runs every job in order, so the lanes of a warp still evaluate
+// the same light together while the vertex array is read once instead of
+// once per job. Each (vertex, job) computes what split_nee computes; only
+// the order of the shadow queue changes (warp-sized runs per light).
+template <bool COUNT, int MINB, bool BATCH>
+__global__ void __launch_bounds__(128, MINB) split_nee_v(const __grid_constant__ WaveArgs a) {
+    __shared__ float s_sheen[512];
+    {
+        const Scene& s0 = tables_of<BATCH>(a);
+        for (uint32_t i = threadIdx.x; i < 512u; i += blockDim.x) s_sheen[i] = tf(s0, s0.P.offs0[1] + i);
+    }
+    __syncthreads();
+    const uint32_t nv = *((volatile uint32_t*)&a.ctr[4]);
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        uint32_t slot = a.q.vslot[v];
+        const Scene& s = slot_scene<BATCH>(a, slot);
+        const uint32_t J = BATCH ? min(a.jobs, s.P.cfg[2] + 1u) : a.jobs;  // this scene's NEE jobs
+        Vertex vx;
+        PathCore pc;
+        uint32_t path_seed;
+        get_vertex(a, v, &vx, &pc, &path_seed);
+        for (uint32_t j = 0; j < J; j++) {
+            ShadowRay sr;
+            float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (nee_job(s, s_sheen, pc, vx, j, &sr)) {
+                pe = make_float4(sr.pending.x, sr.pending.y, sr.pending.z, 1.0f);
+                uint32_t q = append1(&a.ctr[1]);
+                a.q.sh_o[q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+                a.q.sh_d[q] = make_float4(sr.d.x, sr.d.y, sr.d.z, __uint_as_float(sr.skip));
+                a.q.sh_m[q] = make_uint4(slot, j, sr.rid, path_seed);
+            }
+            a.st.pend[(uint64_t)slot * a.jobs + j] = pe;
+        }
+    }
+}
+
 // Variants: shade kernel for 2 / 3 / 4 resident blocks per SM; the NEE
-// kernel for 4 / 5 / 6.
+// kernel job-major (0-2) or vertex-major (3-5) for 4 / 5 / 6.
 template <bool C, bool B>
 static void* shade_fn(int v) {
     if (v == 0) return (void*)split_shade<C, 2, B>;
@@ -398,7 +435,10 @@ template <bool C, bool B>
 static void* nee_fn(int v) {
     if (v == 0) return (void*)split_nee<C, 4, B>;
     if (v == 1) return (void*)split_nee<C, 5, B>;
-    return (void*)split_nee<C, 6, B>;
+    if (v == 2) return (void*)split_nee<C, 6, B>;
+    if (v == 3) return (void*)split_nee_v<C, 4, B>;
+    if (v == 4) return (void*)split_nee_v<C, 5, B>;
+    return (void*)split_nee_v<C, 6, B>;
 }
 
 static cudaError_t persistent(void* fn, const WaveArgs& a, int sms, cudaStream_t st) {
@@ -430,7 +470,7 @@ cudaError_t launch_split_shade(const WaveArgs& a, bool count, int variant, int s
 }
 
 cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st) {
-    variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
+    variant = variant < 0 ? 0 : (variant > 5 ? 5 : variant);
     if (a.nframes) return count ? cudaErrorInvalidValue : persistent(nee_fn<false, true>(variant), a, sms, st);
     return persistent(count ? nee_fn<true, false>(variant) : nee_fn<false, false>(variant), a, sms, st);
 }

@@ -32,7 +32,7 @@ class Plan:
     trace_variant: int = 0
     stack: int = 0
     wave_slots: int = 1 << 20
-    nee_variant: int = 0
+    nee_variant: int = 3
     shadow_walk: int = 0
     graphs: int = 0
     refill: int = 8
@@ -48,7 +48,7 @@ SPACE = {
     "trace_variant": [0, 1, 2],
     "stack": [0, 64],
     "wave_slots": [1 << 19, 1 << 20, 1 << 21],
-    "nee_variant": [0, 1, 2],
+    "nee_variant": [0, 1, 2, 3, 4, 5],
     "shadow_walk": [0, 1],
     "refill": [1, 8, 16, 32],
     "graphs": [0, 1],

@@ -57,6 +57,8 @@ def _alone(pkg, cases, chunks):
     dict(mode=0),                                     # a megakernel executor runs the split wavefront
     dict(mode=2, graphs=1),                           # one CUDA graph, device-side while loops
     dict(mode=1, graphs=1, wave_items=3000, wave_slots=700),
+    dict(mode=2, nee_variant=3, wave_items=3000, wave_slots=700),  # vertex-major NEE, per-scene job counts
+    dict(mode=2, nee_variant=5, graphs=1),
 ])
 def test_batch_matches_each_scene_alone(pkg, plan):
     cases = _cases(pkg)

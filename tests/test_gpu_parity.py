@@ -227,6 +227,24 @@ def test_both_execution_modes_bit_exact(pkg, oracle, mode, refill, which):
     assert np.array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
 
 
+@pytest.mark.parametrize("nee", [0, 2, 3, 4, 5])
+@pytest.mark.parametrize("which", ["materials", "layered"])
+def test_nee_kernel_orders_bit_exact(pkg, oracle, nee, which):
+    """The split plan's NEE kernel job-major (0-2) or vertex-major (3-5):
+    the same jobs in another order, the oracle's accumulator bit for bit."""
+    if which == "materials":
+        scene, env = scenes.materials_scene(pkg), None
+    else:
+        scene = pkg.Scene.icosphere(freq=16, seed=2, n_materials=12, n_textures=3, tex_size=64, n_punctual=3,
+                                    n_emissive=16, material_mix=1)
+        env = pkg.EnvironmentMap.sky(64, 32)
+    t = _tracer(pkg, scene, _opts(pkg, 40, 28, 6, bounces=10), env)
+    t.set_tuning(mode=2, nee_variant=nee, wave_slots=333, wave_items=2000)
+    t.refine(6)
+    cpu, _ = oracle.render(t.prepared(), 6)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
+
+
 @pytest.mark.parametrize("mode", [0, 1, 2])
 def test_traversal_counters_match_oracle(pkg, oracle, mode):
     opts = _opts(pkg, 48, 32, 4)
