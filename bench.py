@@ -78,8 +78,10 @@ def parse():
     ap.add_argument("--ref-spp", type=int, default=16384, help="nrc workload: spp of the plain reference")
     ap.add_argument("--nrc-scene", default="large", choices=["large", "cornell"], help="nrc workload: scene")
     ap.add_argument("--nrc-train-one-in", type=int, default=4, help="nrc workload: one training path in this many")
-    ap.add_argument("--nrc-query-bounce", type=int, default=2, help="nrc workload: paths end into the cache at the "
-                    "vertex hit by this ray")
+    ap.add_argument("--nrc-query-bounce", type=int, default=2, help="nrc workload: first bounce at which paths may "
+                    "end into the cache")
+    ap.add_argument("--nrc-spread", type=float, default=0.01, help="nrc workload: path-spread constant (0: every "
+                    "path ends at the query bounce)")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "cornell", "serve", "nrc", "prepare"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces)")
@@ -599,9 +601,15 @@ def run_nrc(a):
     checkpoints = [1 << k for k in range(20) if (1 << k) <= a.frames]
 
     def progress(t, step):
-        # one untimed frame first: allocations of the plan (and of the
-        # cache's buffers) are not part of the comparison
-        step(1)
+        # untimed first: one call of every chunk size the timed loop makes,
+        # so that allocations and the CUDA graph of each refine shape (and
+        # the cache's buffers) are not part of the comparison
+        sizes, done_ = [], 0
+        for c in checkpoints:
+            sizes.append(c - done_)
+            done_ = c
+        for n in sorted(set(sizes)):
+            step(n)
         t.finish()
         t.reset()
         out, wall, frames = [], 0.0, 0
@@ -623,7 +631,7 @@ def run_nrc(a):
     del plain
     nt = tracer()
     cache = RadianceCache(nt)
-    cache.configure(train_one_in=a.nrc_train_one_in, query_bounce=a.nrc_query_bounce)
+    cache.configure(train_one_in=a.nrc_train_one_in, query_bounce=a.nrc_query_bounce, spread=a.nrc_spread)
     nrc_curve = progress(nt, lambda n: cache.refine(n))
     q, smp = cache.frame_counts()
 
@@ -647,11 +655,12 @@ def run_nrc(a):
                                     "radiance cache: large scene (20 x freq^2 triangles) with the mixed material model")
                                    + f", {a.width}x{a.height}, 1 spp per frame, {a.frames} frames, 12 bounces",
                        "reference": f"plain tracer {a.ref_spp} spp ({ref_s:.1f} s)",
-                       "cache": "5 x 64 ReLU MLP, BF16 tcgen05, 12-frequency encoding, paths end into the cache at the "
-                                f"vertex hit by ray {a.nrc_query_bounce}, "
+                       "cache": "5 x 64 ReLU MLP, BF16 tcgen05, 12-frequency encoding, paths end into the cache from "
+                                f"bounce {a.nrc_query_bounce} when the path spread exceeds {a.nrc_spread} x the "
+                                "primary vertex's, "
                                 f"1 in {a.nrc_train_one_in} paths trains (suffix of 4 bounces into the cache), "
                                 "<= 65536 samples and one Adam step (lr 1e-2) per frame",
-                       "timing": "host wall clock with a device sync per checkpoint; one untimed frame first"},
+                       "timing": "host wall clock with a device sync per checkpoint; one untimed call of every chunk size first"},
             "plain_seconds_to_35db": tp, "ratio_to_plain": (tn / tp) if (tn and tp) else None,
             "plain_ms_per_frame": frame_ms(plain_curve), "cache_ms_per_frame": frame_ms(nrc_curve),
             "plain": plain_curve, "cache": nrc_curve,

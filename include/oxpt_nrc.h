@@ -77,9 +77,14 @@ typedef struct oxpt_nrc_config {
     uint32_t train;
     uint32_t train_suffix;  /* training paths end into the cache this many bounces after the
                                query vertex (self-training); 0 = they run to the end */
-    uint32_t reserved[2];
+    float spread;           /* path-spread heuristic (Mueller et al. 2021): a path ends into the
+                               cache at the first vertex at or after query_bounce where
+                               (sum over its bounces of sqrt(t^2 / (pdf |cos|)))^2 exceeds
+                               spread x the primary vertex's t^2 / (4 pi |cos|); 0 = exactly
+                               at query_bounce */
+    uint32_t reserved;
 } oxpt_nrc_config;
-void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1, 4 */
+void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1, 4, 0.01 */
 
 /* `count` cache frames with sample indices first_sample.. on `ctx`'s
  * accumulator; *loss (optional, waits for the GPU) = the last frame's mean

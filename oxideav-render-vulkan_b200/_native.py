@@ -54,7 +54,7 @@ class BatchFrame(C.Structure):
 
 class NrcConfig(C.Structure):
     _fields_ = [("enabled", u32), ("query_bounce", u32), ("train_one_in", u32), ("max_train", u32),
-                ("train", u32), ("train_suffix", u32), ("reserved", u32 * 2)]
+                ("train", u32), ("train_suffix", u32), ("spread", C.c_float), ("reserved", u32)]
 
 
 class DevImage(C.Structure):

@@ -1684,6 +1684,7 @@ void oxpt_nrc_config_default(oxpt_nrc_config* cfg) {
     cfg->max_train = 65536;
     cfg->train = 1;
     cfg->train_suffix = 4;
+    cfg->spread = 0.01f;
 }
 
 }  // extern "C"
@@ -1721,10 +1722,12 @@ oxpt_status nrc_buffers(oxpt_ctx* c, oxpt_nrc* r, size_t q, size_t t, size_t slo
         r->t_cap = t;
     }
     if (slots > r->s_cap) {
-        size_t c1 = 0, c2 = 0, c3 = 0;
+        size_t c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;
         if ((s = grow(c, &r->s_pre, &c1, slots, 1, "cache slot state"))) return s;
         if ((s = grow(c, &r->s_beta, &c2, slots, 1, "cache slot state"))) return s;
         if ((s = grow(c, &r->s_tidx, &c3, slots, 1, "cache slot state"))) return s;
+        if ((s = grow(c, &r->s_spread, &c4, slots, 1, "cache slot state"))) return s;
+        if ((s = grow(c, &r->s_tail, &c5, slots, 1, "cache slot state"))) return s;
         r->s_cap = slots;
     }
     return OXPT_OK;
@@ -1773,8 +1776,9 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
     if (npix > c->wave_items) return fail(c, OXPT_E_LIMIT, "a cache frame must fit one launch (width x height <= wave_items)");
     const uint32_t P = (uint32_t)npix;  // every path of the frame in flight at once
     const uint32_t max_train = std::max(cfg->max_train, 1u);
-    if (cfg->train_suffix && cfg->query_bounce + cfg->train_suffix < cfg->query_bounce)
-        return fail(c, OXPT_E_INVALID, "train_suffix too large");
+    if (cfg->train_suffix > 64) return fail(c, OXPT_E_INVALID, "train_suffix above 64");
+    if (!(cfg->spread >= 0.0f) || !std::isfinite(cfg->spread))
+        return fail(c, OXPT_E_INVALID, "spread must be finite and not negative");
     if ((s = nrc_buffers(c, r, npix, max_train, P))) return s;
     if ((s = oxd::nrc::ensure_scratch(r, max_train))) return s;
     if ((s = ensure_out(c, npix))) return s;
@@ -1814,7 +1818,10 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         nw.s_beta = r->s_beta;
         nw.s_tidx = r->s_tidx;
         nw.t_tail = r->t_tail;
-        nw.tail_k = cfg->train_suffix ? cfg->query_bounce + cfg->train_suffix : 0xffffffffu;
+        nw.suffix = cfg->train_suffix;
+        nw.spread = cfg->spread;
+        nw.s_spread = r->s_spread;
+        nw.s_tail = r->s_tail;
         if ((s = run_wave(c, ta, false, &nw))) break;
         // The cache's predictions complete the rendering paths.
         oxd::nrc::Args a = oxd::nrc::base_args(r);

@@ -173,7 +173,8 @@ void oxpt_nrc_destroy(oxpt_nrc* c) {
     }
     void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->grad_part, c->loss, c->wf, c->wt, c->err_dev,
                     c->in, c->pred, c->target, c->acts, c->dy, c->counts, c->q_in, c->q_beta, c->q_item,
-                    c->t_in, c->t_target, c->s_pre, c->s_beta, c->s_tidx, c->t_tail, c->q_pred};
+                    c->t_in, c->t_target, c->s_pre, c->s_beta, c->s_tidx, c->t_tail, c->q_pred,
+                    c->s_spread, c->s_tail};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;

@@ -33,6 +33,8 @@ struct oxpt_nrc {
     float4* q_pred = nullptr;
     float4 *s_pre = nullptr, *s_beta = nullptr;
     uint32_t* s_tidx = nullptr;
+    float2* s_spread = nullptr;
+    uint32_t* s_tail = nullptr;
     size_t s_cap = 0;
     float lr = 1e-2f, b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
     uint64_t step = 0;

@@ -244,7 +244,10 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
         f3 o = start_path(s, s_sobol, q - yy * s.P.dims[0], y0 + yy, first + it, &smp, &pc);
         a.st.item[i] = item;
         if (BATCH) a.st.frame[i] = f;
-        if (a.nrc.on) a.nrc.s_tidx[i] = NONE;
+        if (a.nrc.on) {
+            a.nrc.s_tidx[i] = NONE;
+            a.nrc.s_tail[i] = NONE;
+        }
         save_state(a, i, pc, smp, ST_TRACING);
         a.st.org[i] = make_float4(o.x, o.y, o.z, 0.0f);
         a.q.ext[append1(&a.ctr[0])] = i;
@@ -283,7 +286,19 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
             save_state(a, i, pc, smp, ST_ENDING);
             continue;
         }
-        if (a.nrc.on && pc.k == a.nrc.tail_k && (smp.path_seed & a.nrc.train_mask) == 0u) {
+        bool spread_ok = true;
+        if (a.nrc.on) {
+            // Path spread (Mueller et al. 2021): a0 = t^2 / (4 pi |cos|) at the
+            // primary vertex, then the sum of sqrt(t^2 / (pdf |cos|)) over bounces.
+            const float cosv = fabsf(dot(vx.ng, pc.d));
+            float2 sp = pc.k == 0u ? make_float2(0.0f, 0.0f) : a.nrc.s_spread[i];
+            if (pc.k == 0u) sp.x = hit.t * hit.t / (4.0f * PI * fmaxf(cosv, 1e-6f));
+            else if (pc.prev_pdf > 0.0f && cosv > 0.0f) sp.y += sqrtf(hit.t * hit.t / (pc.prev_pdf * cosv));
+            a.nrc.s_spread[i] = sp;
+            spread_ok = a.nrc.spread <= 0.0f || sp.y * sp.y > a.nrc.spread * sp.x;
+        }
+        const uint32_t tail = a.nrc.on ? a.nrc.s_tail[i] : NONE;
+        if (a.nrc.on && tail == pc.k && (smp.path_seed & a.nrc.train_mask) == 0u) {
             // A training path's suffix ends here, into the cache.
             float4 f[3];
             nrc_features(s, vx, f);
@@ -307,7 +322,7 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
             save_state(a, i, pc, smp, ST_ENDING);
             continue;
         }
-        if (a.nrc.on && pc.k == a.nrc.query_k) {
+        if (a.nrc.on && pc.k >= a.nrc.query_k && tail == NONE && spread_ok) {
             float4 f[3];
             nrc_features(s, vx, f);
             if ((smp.path_seed & a.nrc.train_mask) != 0u) {
@@ -324,6 +339,7 @@ __global__ void __launch_bounds__(128, MINB) split_shade(const __grid_constant__
                 save_state(a, i, pc, smp, ST_ENDING);
                 continue;
             }
+            a.nrc.s_tail[i] = a.nrc.suffix ? pc.k + a.nrc.suffix : 0xfffffffeu;
             uint32_t ti = atomicAdd(&a.nrc.counts[1], 1u);
             if (ti < a.nrc.t_cap) {
                 a.nrc.t_in[3 * (size_t)ti] = f[0];

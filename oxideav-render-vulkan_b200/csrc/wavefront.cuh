@@ -39,16 +39,19 @@ struct BatchFrame {
 };
 
 // Radiance-cache frame (split plan only; `on` = 0 otherwise): paths that
-// are not training paths end at the vertex hit by ray `query_k` with a
-// cache query (features, throughput, result index); training paths (path
-// seed & train_mask == 0) continue to the end and record, at that vertex,
-// the inputs and, when they finish, the radiance they gathered from there
-// on divided by their throughput there: the cache's target.
-// Training paths end into the cache too, at the vertex hit by ray tail_k
-// (0xffffffff: never): their target then adds the cache's prediction there
-// (scaled by the throughput ratio), filled in after inference.
+// are not training paths end with a cache query (features, throughput,
+// result index) at their first vertex at or after bounce `query_k` whose
+// path spread passes the heuristic (`spread` = 0: exactly at query_k);
+// training paths (path seed & train_mask == 0) record, at that vertex, the
+// inputs and, when they finish, the radiance they gathered from there on
+// divided by their throughput there: the cache's target. A training path
+// ends into the cache `suffix` bounces later (0: never): its target then
+// adds the cache's prediction there (scaled by the throughput ratio),
+// filled in after inference.
 struct NrcWave {
-    uint32_t on, query_k, train_mask, q_cap, t_cap, tail_k, pad1, pad2;
+    uint32_t on, query_k, train_mask, q_cap, t_cap, suffix;
+    float spread;                  // path-spread constant (0: end exactly at query_k)
+    uint32_t pad;
     uint32_t* counts;              // [0] queries, [1] training samples
     float4* q_in;                  // q_cap x 3 float4 inputs
     float4* q_beta;                // throughput at the query vertex
@@ -59,6 +62,10 @@ struct NrcWave {
     float4* s_beta;                // per slot: throughput at the training vertex
     uint32_t* s_tidx;              // per slot: training sample index, or 0xffffffff
     uint4* t_tail;                 // per training sample: tail query, throughput ratio (float bits)
+    float2* s_spread;              // per slot: primary spread a0, sum of sqrt(t^2 / (pdf |cos|))
+    uint32_t* s_tail;              // per slot: bounce where a training path's suffix ends, or
+                                   // 0xfffffffe after its training vertex without a suffix, or
+                                   // 0xffffffff before it
 };
 
 struct WaveQueues {

@@ -43,7 +43,7 @@ class RadianceCache:
 
     def configure(self, **kw):
         for k, v in kw.items():
-            setattr(self.cfg, k, int(v))
+            setattr(self.cfg, k, float(v) if k == "spread" else int(v))
 
     def weights(self) -> np.ndarray:
         w = np.zeros(N.NRC_PARAMS, np.float32)

@@ -143,7 +143,7 @@ def test_zero_cache_ends_paths_exactly_at_the_query_bounce(pkg, oracle):
     t = _tracer(pkg)
     cache = RadianceCache(t)
     cache.set_weights(np.zeros(nrc.PARAMS, np.float32))
-    cache.configure(train_one_in=1 << 31, train=0)
+    cache.configure(train_one_in=1 << 31, train=0, spread=0)
     cache.refine(3)
     assert t.samples() == 3
     got = t.read_accum()
@@ -170,6 +170,46 @@ def test_training_paths_are_the_plain_tracer(pkg):
     assert np.array_equal(t.read_accum().view(np.uint32), plain.read_accum().view(np.uint32))
     q, s = cache.frame_counts()
     assert q == 0 and s > 100
+
+
+def test_path_spread_decides_where_paths_end(pkg):
+    """The path-spread heuristic: a spread no path reaches ends no path
+    (the frames are the plain tracer's, bit for bit); the default ends
+    fewer paths at the first eligible bounce than the fixed cut does (the
+    glossy ones go on) but still most of them."""
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+
+    def counts(spread):
+        t = _tracer(pkg)
+        cache = RadianceCache(t)
+        cache.set_weights(np.zeros(nrc.PARAMS, np.float32))
+        cache.configure(train_one_in=1 << 31, train=0, spread=spread)
+        cache.refine(2)
+        return t, cache.frame_counts()[0]
+
+    never, q_never = counts(1e30)
+    plain = _tracer(pkg)
+    plain.refine(2)
+    assert q_never == 0
+    assert np.array_equal(never.read_accum().view(np.uint32), plain.read_accum().view(np.uint32))
+    _, q_fixed = counts(0.0)
+    _, q_default = counts(0.01)
+    assert 0 < q_default <= q_fixed, (q_default, q_fixed)
+
+
+def test_path_spread_training_paths_record_once(pkg):
+    """With the default spread every training path records at most one
+    vertex, and all-training frames are still the plain tracer's."""
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg)
+    cache = RadianceCache(t)
+    cache.configure(train_one_in=1, train=0, max_train=1 << 20, train_suffix=0)
+    cache.refine(1)
+    q, samples = cache.frame_counts()
+    plain = _tracer(pkg)
+    plain.refine(1)
+    assert q == 0 and 0 < samples <= 96 * 64
+    assert np.array_equal(t.read_accum().view(np.uint32), plain.read_accum().view(np.uint32))
 
 
 def _mean_image(t):
