@@ -600,16 +600,17 @@ def run_nrc(a):
 
     checkpoints = [1 << k for k in range(20) if (1 << k) <= a.frames]
 
-    def progress(t, step):
+    def progress(t, step, warm=None):
         # untimed first: one call of every chunk size the timed loop makes,
         # so that allocations and the CUDA graph of each refine shape (and
-        # the cache's buffers) are not part of the comparison
+        # the cache's buffers) are not part of the comparison; the cache
+        # warms up without training, so it starts the timed loop untrained
         sizes, done_ = [], 0
         for c in checkpoints:
             sizes.append(c - done_)
             done_ = c
         for n in sorted(set(sizes)):
-            step(n)
+            (warm or step)(n)
         t.finish()
         t.reset()
         out, wall, frames = [], 0.0, 0
@@ -632,7 +633,12 @@ def run_nrc(a):
     nt = tracer()
     cache = RadianceCache(nt)
     cache.configure(train_one_in=a.nrc_train_one_in, query_bounce=a.nrc_query_bounce, spread=a.nrc_spread)
-    nrc_curve = progress(nt, lambda n: cache.refine(n))
+    def untrained(n):
+        cache.configure(train=0)
+        cache.refine(n)
+        cache.configure(train=1)
+
+    nrc_curve = progress(nt, lambda n: cache.refine(n), untrained)
     q, smp = cache.frame_counts()
 
     def time_to(curve, db):
