@@ -422,6 +422,7 @@ def run_prepare(a):
     d2h = 512 * 4  # leaf slots of the emissive triangles (the four-wide tree is collapsed on the device)
     # Host preparation of the same scene (bounded sample: one run).
     host = pkg.GpuPathTracer(0)
+    host.set_gpu_prepare(False)
     host.set_environment(env)
     t0 = time.perf_counter()
     host.sync(scene, opts)

@@ -61,7 +61,7 @@ struct oxpt_tracer {
     // prepares itself (serving sessions); `cam` overrides the camera.
     const oxpt_tracer* owner = nullptr;
     std::optional<oxpt_camera> cam;
-    bool gpu_prepare = false;  // BVH, slot flattening and atlas built on the context's GPU
+    bool gpu_prepare = true;  // BVH, slot flattening and atlas built on the context's GPU
     oxpt::Framing framing;
     std::optional<oxpt::Env> env;
     std::optional<oxpt::EnvWords> env_words;
@@ -94,19 +94,21 @@ struct oxpt_tracer {
     }
 
     oxpt_status upload(const oxpt_scene& s, float headlight) {
+        std::unique_ptr<oxpt::SceneBuffers> sb;
         if (gpu_prepare) {
             oxpt_status st = OXPT_OK;
-            auto sb = oxpt::upload_scene(s, headlight, &device_flatten, this, &st);
-            if (sb) {
+            sb = oxpt::upload_scene(s, headlight, &device_flatten, this, &st);
+            if (sb && sb->on_device) {
                 framing = oxpt::framing_of(s);
                 scene = std::move(sb);
                 return OXPT_OK;
             }
-            // A tree the device scan cannot hold is built by the host below;
-            // any other failure is the device's and is reported.
-            if (st != OXPT_E_LIMIT) return st;
+            // A scene without triangles comes back prepared on the host and
+            // is uploaded below; a tree the device scan cannot hold is built
+            // by the host; any other failure is the device's and is reported.
+            if (!sb && st != OXPT_E_LIMIT) return st;
         }
-        auto sb = oxpt::upload_scene(s, headlight);
+        if (!sb) sb = oxpt::upload_scene(s, headlight);
         oxpt_scene_desc d;
         d.geom = sb->geom.data();
         d.geom_words = sb->geom.size();

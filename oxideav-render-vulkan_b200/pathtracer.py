@@ -383,9 +383,10 @@ class GpuPathTracer:
         return buf.value.decode()
 
     def set_gpu_prepare(self, on: bool = True):
-        """Prepare the scene on this tracer's GPU: BVH, leaf-slot
-        flattening and atlas texels (the host preparation's buffers, word
-        for word). Takes effect at the next sync."""
+        """Prepare the scene on this tracer's GPU (the default): BVH,
+        leaf-slot flattening and atlas texels, the host preparation's
+        buffers word for word; False prepares on the host. Takes effect at
+        the next sync."""
         N.lib().oxpt_tracer_set_gpu_prepare(self._h, int(bool(on)))
 
     def prepare_timing(self) -> dict:

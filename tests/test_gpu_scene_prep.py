@@ -64,6 +64,7 @@ def _scenes(pkg):
 def _pair(pkg, scene, w=64, h=48, spp=2):
     opts = pkg.RenderOptions(width=w, height=h, path_trace=pkg.PathTraceOptions(samples_per_pixel=spp))
     a, b = pkg.GpuPathTracer(0), pkg.GpuPathTracer(0)
+    a.set_gpu_prepare(False)  # the host preparation
     b.set_gpu_prepare(True)
     a.sync(scene, opts)
     b.sync(scene, opts)
