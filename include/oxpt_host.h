@@ -219,9 +219,9 @@ oxpt_status oxpt_tracer_refine(oxpt_tracer* t, uint32_t samples);
 /* Prepare the scene on the tracer's GPU (oxpt_build_scene: the BVH, the
  * leaf-slot flattening and the atlas texels; the same buffers as the host
  * preparation, word for word). On by default; 0 selects the host
- * preparation. A tree whose levels are too wide for the device build is
- * prepared by the host instead. Changing it makes the next sync prepare
- * again. */
+ * preparation. Sources beyond the device build's limits (more than 2^30
+ * triangles, textures wider than 65535) are prepared by the host instead.
+ * Changing it makes the next sync prepare again. */
 void oxpt_tracer_set_gpu_prepare(oxpt_tracer* t, int on);
 /* refine() restricted to rows [y0, y0 + rows): the per-GPU share of a
  * frame split by row tiles across GPUs (sample indices and the samples()

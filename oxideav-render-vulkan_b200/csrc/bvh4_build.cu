@@ -17,8 +17,7 @@
 //           gets index u_x + j and starts numbering at
 //           u_x + m_x + sum of D over the kids after j; the node's words
 //           and the stack bound (max over nodes of acc + kids) are written.
-// A level wider than the scan or a tree deeper than 64 four-wide levels is
-// left to the host collapse.
+// A tree deeper than 64 four-wide levels is left to the host collapse.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -33,7 +32,6 @@ namespace bvh4b {
 
 constexpr uint32_t NONE = 0xffffffffu;
 constexpr uint32_t LEAF = 0x80000000u;
-constexpr uint32_t SCAN_MAX = 1024u * 1024u;
 
 struct Item {
     uint32_t b;             // binary node this 4-wide node stands for
@@ -148,7 +146,9 @@ __global__ void expand(Item* items, uint32_t s, uint32_t e, const uint32_t* w, u
     counts[i - s] = m;
 }
 
-// Exclusive scan of up to SCAN_MAX counts: per-block scans, then block offsets.
+// Exclusive scan of the counts: per-block scans, then block offsets (for more
+// than 1024 blocks the block sums are scanned the same way and their
+// offsets added back).
 __global__ void scan_blocks(uint32_t* v, uint32_t K, uint32_t* block_sums) {
     __shared__ uint32_t s[1024];
     uint32_t i = blockIdx.x * 1024 + threadIdx.x;
@@ -163,6 +163,11 @@ __global__ void scan_blocks(uint32_t* v, uint32_t K, uint32_t* block_sums) {
     }
     if (i < K) v[i] = s[threadIdx.x] - x;
     if (threadIdx.x == 1023) block_sums[blockIdx.x] = s[1023];
+}
+
+__global__ void add_offsets(uint32_t* v, uint32_t K, const uint32_t* offs) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < K) v[i] += offs[i / 1024];
 }
 
 __global__ void scan_sums(uint32_t* block_sums, uint32_t nb, uint32_t* total) {
@@ -302,7 +307,7 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
     uint32_t root_words[8];
     Collapse res = Collapse::BUILT;
     Item* items = nullptr;
-    uint32_t *counts = nullptr, *sums = nullptr, *ctr = nullptr;
+    uint32_t *counts = nullptr, *sums = nullptr, *sums2 = nullptr, *ctr = nullptr;
     std::vector<uint32_t> level_start;
     uint32_t h[2] = {0, 0};
     const uint32_t cap = nodes / 2 + 1;
@@ -319,8 +324,9 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
     }
     *root_ref = 0;
     CK4(cudaMallocAsync((void**)&items, (size_t)cap * sizeof(Item), st));
-    CK4(cudaMallocAsync((void**)&counts, (size_t)std::min(cap, SCAN_MAX) * 4, st));
-    CK4(cudaMallocAsync((void**)&sums, 1024 * 4, st));
+    CK4(cudaMallocAsync((void**)&counts, (size_t)cap * 4, st));
+    CK4(cudaMallocAsync((void**)&sums, (size_t)blocks(cap, 1024) * 4, st));
+    CK4(cudaMallocAsync((void**)&sums2, 1024 * 4, st));
     CK4(cudaMallocAsync((void**)&ctr, 8, st));  // total, bad
     {
         Item root{};
@@ -334,13 +340,21 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
     level_start = {0u, 1u};
     for (;;) {
         uint32_t s = level_start[level_start.size() - 2], e = level_start.back(), K = e - s;
-        if (K > SCAN_MAX || level_start.size() > 66) {
+        if (level_start.size() > 66) {
             res = Collapse::UNSUPPORTED;
             goto done;
         }
         expand<<<blocks(K, 128), 128, 0, st>>>(items, s, e, w, nodes, counts, ctr + 1);
-        scan_blocks<<<blocks(K, 1024), 1024, 0, st>>>(counts, K, sums);
-        scan_sums<<<1, 1024, 0, st>>>(sums, blocks(K, 1024), ctr);
+        const uint32_t nb = blocks(K, 1024);
+        scan_blocks<<<nb, 1024, 0, st>>>(counts, K, sums);
+        if (nb <= 1024) {
+            scan_sums<<<1, 1024, 0, st>>>(sums, nb, ctr);
+        } else {  // K <= cap <= 2^29 + 1, so one more level of blocks suffices
+            const uint32_t nb2 = blocks(nb, 1024);
+            scan_blocks<<<nb2, 1024, 0, st>>>(sums, nb, sums2);
+            scan_sums<<<1, 1024, 0, st>>>(sums2, nb2, ctr);
+            add_offsets<<<blocks(nb, 256), 256, 0, st>>>(sums, nb, sums2);
+        }
         link<<<blocks(K, 128), 128, 0, st>>>(items, s, e, counts, sums, w, cap);
         CK4(cudaGetLastError());
         CK4(cudaMemcpyAsync(h, ctr, 8, cudaMemcpyDeviceToHost, st));
@@ -373,7 +387,7 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
     CK4(cudaStreamSynchronize(st));
     *need = h[0];
 done:
-    for (void* p : {(void*)items, (void*)counts, (void*)sums, (void*)ctr})
+    for (void* p : {(void*)items, (void*)counts, (void*)sums, (void*)sums2, (void*)ctr})
         if (p) cudaFreeAsync(p, st);
     if (res != Collapse::BUILT) {
         cudaStreamSynchronize(st);

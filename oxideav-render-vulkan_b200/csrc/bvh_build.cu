@@ -850,6 +850,29 @@ __device__ __forceinline__ void classify(const Lists& l, uint32_t idx, uint32_t 
     else if (count > SMALL_MAX) l.medium[atomicAdd(&l.counts[0], 1u)] = idx;
 }
 
+// Wide levels (more than 1024 blocks of 1024): the block sums are scanned
+// in place by blocks of 1024 as well, and those blocks' offsets added back.
+__global__ void scan_u32(uint32_t* v, uint32_t K, uint32_t* block_sums) {
+    __shared__ uint32_t s[1024];
+    uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+    uint32_t x = i < K ? v[i] : 0u;
+    s[threadIdx.x] = x;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        uint32_t y = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
+        __syncthreads();
+        s[threadIdx.x] += y;
+        __syncthreads();
+    }
+    if (i < K) v[i] = s[threadIdx.x] - x;
+    if (threadIdx.x == 1023) block_sums[blockIdx.x] = s[1023];
+}
+
+__global__ void add_offsets(uint32_t* v, uint32_t K, const uint32_t* offs) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < K) v[i] += offs[i / 1024];
+}
+
 __global__ void emit(const Job* jobs, uint32_t K, const Decision* dec, const uint32_t* excl, const uint32_t* block_sums,
                      uint32_t nodes_before, uint32_t* words, Job* next, Lists lists) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -905,6 +928,7 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
     bool ok = true;
     float4 *blo = nullptr, *bhi = nullptr, *cen = nullptr;
     uint32_t *ids = nullptr, *ids2 = nullptr, *words = nullptr, *excl = nullptr, *sums = nullptr, *ctr = nullptr;
+    uint32_t* sums2 = nullptr;  // block offsets of the block sums (levels wider than 1024 x 1024)
     uint32_t *l_medium = nullptr, *l_large = nullptr, *l_huge = nullptr, *chunk_left = nullptr, *total_chunks = nullptr;
     HugeNode* hn = nullptr;
     HugeAcc* acc = nullptr;
@@ -926,7 +950,8 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
     BK(cudaMallocAsync((void**)&next, max_jobs * sizeof(Job), st));
     BK(cudaMallocAsync((void**)&dec, max_jobs * sizeof(Decision), st));
     BK(cudaMallocAsync((void**)&excl, max_jobs * 4, st));
-    BK(cudaMallocAsync((void**)&sums, 1024 * 4, st));
+    BK(cudaMallocAsync((void**)&sums, ((max_jobs + 1023) / 1024) * 4, st));
+    BK(cudaMallocAsync((void**)&sums2, 1024 * 4, st));
     BK(cudaMallocAsync((void**)&ctr, 4 * 4, st));
     BK(cudaMallocAsync((void**)&l_medium, max_jobs * 4, st));
     BK(cudaMallocAsync((void**)&l_large, max_large * 4, st));
@@ -949,11 +974,6 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
         BK(cudaMemsetAsync(l, 0, 4, st));
     }
     while (K > 0) {
-        if (K > 1024u * 1024u) {
-            if (err) *err = "bvh build: a level wider than the scan supports";
-            ok = false;
-            goto done;
-        }
         levels++;
         Tri tr{blo, bhi, cen};
         decide_small<<<(K + 127) / 128, 128, 0, st>>>(jobs, K, tr, ids, ids2, dec);
@@ -984,7 +1004,15 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
         uint32_t nb = (K + 1023) / 1024;
         scan_blocks<<<nb, 1024, 0, st>>>(dec, K, excl, sums);
         BK(cudaGetLastError());
-        scan_sums<<<1, 1024, 0, st>>>(sums, nb, ctr);
+        if (nb <= 1024) {
+            scan_sums<<<1, 1024, 0, st>>>(sums, nb, ctr);
+        } else {  // K <= n <= 2^30, so nb <= 2^20 and one more level suffices
+            uint32_t nb2 = (nb + 1023) / 1024;
+            scan_u32<<<nb2, 1024, 0, st>>>(sums, nb, sums2);
+            scan_sums<<<1, 1024, 0, st>>>(sums2, nb2, ctr);
+            add_offsets<<<(nb + 255) / 256, 256, 0, st>>>(sums, nb, sums2);
+            launches += 3;
+        }
         BK(cudaGetLastError());
         BK(cudaMemsetAsync(ctr + 1, 0, 12, st));
         emit<<<(K + 127) / 128, 128, 0, st>>>(jobs, K, dec, excl, sums, nodes, words, next,
@@ -1008,7 +1036,7 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
     *depth_out = levels;
     if (launches_out) *launches_out = launches;
 done:
-    void* ptrs[] = {blo, bhi, cen, ids, ids2, words, excl, sums, ctr, jobs, next, dec,
+    void* ptrs[] = {blo, bhi, cen, ids, ids2, words, excl, sums, sums2, ctr, jobs, next, dec,
                     l_medium, l_large, l_huge, hn, acc, chunk_left, total_chunks};
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, st);  // stream-ordered: no device-wide synchronisation

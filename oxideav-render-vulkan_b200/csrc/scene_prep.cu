@@ -568,11 +568,7 @@ oxpt_status build_scene(const oxpt_scene_src& src, cudaStream_t st, DeviceScene*
     PK(cudaEventRecord(ev[1], st), "timing");
     // BVH (syncs the stream once per level).
     if (!bvhb::build_on_device(pos, n, st, &words, &slots, &ds.node_count, &ds.depth, &bvh_launches, err)) {
-        // A level wider than the scan is a size limit (the host builds such
-        // trees); anything else is the device's failure.
-        status = err->find("wider") != std::string::npos ? OXPT_E_LIMIT
-                 : err->find("out of memory") != std::string::npos ? OXPT_E_NOMEM
-                                                                   : OXPT_E_CUDA;
+        status = err->find("out of memory") != std::string::npos ? OXPT_E_NOMEM : OXPT_E_CUDA;
         goto fail_status;
     }
     PK(cudaEventRecord(ev[2], st), "timing");

@@ -17,8 +17,8 @@ namespace bvhb {
 // and *slots (leaf slot -> triangle, n entries) are stream-ordered device
 // allocations (cudaMallocAsync on st) that the caller frees with
 // cudaFreeAsync. Scratch is stream-ordered too, so the build never waits
-// for other streams' work. False with *err when an allocation or launch fails or a
-// level is wider than the level scan handles.
+// for other streams' work. False with *err when an allocation or launch
+// fails.
 bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** words, uint32_t** slots,
                      uint32_t* nodes, uint32_t* depth, uint32_t* launches, std::string* err);
 
@@ -28,8 +28,8 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
 // device memory (bvh4_build.cu): the host collapse's words (host/bvh4.cpp),
 // node for node. BUILT: *out (cudaMalloc, n4 x 32 words; null when the
 // root is a leaf), *root_ref and *need are set. REFUSED: the host collapse
-// refuses the tree too (keep the binary walk). UNSUPPORTED: too wide or
-// deep for the device pass (collapse on the host). FAILED: a CUDA error.
+// refuses the tree too (keep the binary walk). UNSUPPORTED: deeper than
+// 64 four-wide levels (collapse on the host). FAILED: a CUDA error.
 enum class Collapse { BUILT, REFUSED, UNSUPPORTED, FAILED };
 Collapse collapse4_device(const uint32_t* words, uint32_t nodes, cudaStream_t st, uint32_t** out, uint32_t* n4,
                           uint32_t* root_ref, uint32_t* need, std::string* err);

@@ -104,8 +104,9 @@ struct oxpt_tracer {
                 return OXPT_OK;
             }
             // A scene without triangles comes back prepared on the host and
-            // is uploaded below; a tree the device scan cannot hold is built
-            // by the host; any other failure is the device's and is reported.
+            // is uploaded below; sources beyond the device build's limits
+            // (OXPT_E_LIMIT) are prepared by the host; any other failure is
+            // the device's and is reported.
             if (!sb && st != OXPT_E_LIMIT) return st;
         }
         if (!sb) sb = oxpt::upload_scene(s, headlight);
