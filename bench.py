@@ -729,7 +729,7 @@ def main():
         pt.set_tuning(**kw)
     elif not a.no_tune:
         from oxideav_render_vulkan_b200 import tuner
-        tuner.tune(pt, spp=min(a.spp, 4), repeats=1, log=tune_log)
+        tuner.tune(pt, spp=min(a.spp, 4), repeats=3, log=tune_log)  # best of three per trial: steadier picks
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):
