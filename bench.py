@@ -24,7 +24,9 @@ The JSON line also carries:
                the measured HBM copy bandwidth;
   cpu_baseline the CPU oracle (the same estimator, C++, all host threads) on
                a bounded sample of the same frame (N = 1, rank 0 only).
-`--impl reference` times that CPU implementation alone.
+`--impl reference` times that CPU implementation alone: the reference's own
+CPU tracer is an external Rust crate that cannot be built without a Rust
+toolchain, so its C++ restatement stands in for it.
 """
 from __future__ import annotations
 
