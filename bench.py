@@ -341,7 +341,7 @@ def run_cornell(a):
     tune_log = []
     plan = None
     if not a.no_tune:
-        plan = tuner.tune(pt, spp=min(spp, 16), repeats=1, log=tune_log)
+        plan = tuner.tune(pt, spp=spp, repeats=3, log=tune_log)  # the measured frame itself: 13 ms a trial
 
     def measure(with_image):
         ms = []

@@ -47,7 +47,7 @@ SPACE = {
     "shade_variant": [0, 1, 2],
     "trace_variant": [0, 1, 2],
     "stack": [0, 64],
-    "wave_slots": [1 << 19, 1 << 20, 1 << 21],
+    "wave_slots": [1 << 19, 1 << 20, 1 << 21, 1 << 22],
     "nee_variant": [0, 1, 2, 3, 4, 5],
     "shadow_walk": [0, 1],
     "refill": [1, 8, 16, 32],
