@@ -69,6 +69,7 @@ def parse():
                     help="execution plan; auto = the library default")
     ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--wave-items", type=int, default=0, help="wavefront paths per launch round (0: the plan's)")
     ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
                     help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
     ap.add_argument("--requests", type=int, default=300, help="serve workload: requests in the stream")
@@ -732,6 +733,8 @@ def main():
     elif not a.no_tune:
         from oxideav_render_vulkan_b200 import tuner
         tuner.tune(pt, spp=min(a.spp, 4), repeats=3, log=tune_log)  # best of three per trial: steadier picks
+    if a.wave_items:
+        pt.set_tuning(wave_items=a.wave_items)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):

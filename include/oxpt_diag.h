@@ -93,7 +93,9 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *                  shading launch and two traversal launches per bounce.
  *   threads, blocks_per_sm, max_paths   megakernel launch shape.
  *   wave_slots     paths in flight (wavefront); wave_items its paths per
- *                  launch; check_every its bounces between completion
+ *                  launch round (0 = 2^27: a 1080p frame of 64 spp in one
+ *                  round; the result buffer holds 16 bytes per path of a
+ *                  round); check_every its bounces between completion
  *                  checks.
  *   shade_variant  wavefront logic kernel compiled for 2 / 3 / 4 resident
  *                  blocks per SM (0 / 1 / 2): registers against occupancy.

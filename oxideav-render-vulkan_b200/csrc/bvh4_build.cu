@@ -25,6 +25,7 @@
 #include <string>
 #include <vector>
 
+#include "pool.cuh"
 #include "scene_prep.cuh"
 
 namespace oxd {
@@ -294,10 +295,9 @@ unsigned blocks(uint32_t n, unsigned t) { return (n + t - 1) / t; }
         }                                                                      \
     } while (0)
 
-Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, uint32_t** out, uint32_t* n4,
+Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, uint32_t** out, size_t* out_cap, uint32_t* n4,
                           uint32_t* root_ref, uint32_t* need, std::string* err) {
     using namespace bvh4b;
-    *out = nullptr;
     *n4 = 0;
     *need = 1;
     if (nodes == 0) {
@@ -323,11 +323,11 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
         return Collapse::BUILT;
     }
     *root_ref = 0;
-    CK4(cudaMallocAsync((void**)&items, (size_t)cap * sizeof(Item), st));
-    CK4(cudaMallocAsync((void**)&counts, (size_t)cap * 4, st));
-    CK4(cudaMallocAsync((void**)&sums, (size_t)blocks(cap, 1024) * 4, st));
-    CK4(cudaMallocAsync((void**)&sums2, 1024 * 4, st));
-    CK4(cudaMallocAsync((void**)&ctr, 8, st));  // total, bad
+    CK4(scratch_alloc((void**)&items, (size_t)cap * sizeof(Item), st));
+    CK4(scratch_alloc((void**)&counts, (size_t)cap * 4, st));
+    CK4(scratch_alloc((void**)&sums, (size_t)blocks(cap, 1024) * 4, st));
+    CK4(scratch_alloc((void**)&sums2, 1024 * 4, st));
+    CK4(scratch_alloc((void**)&ctr, 8, st));  // total, bad
     {
         Item root{};
         root.b = 0;
@@ -376,7 +376,13 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
         sizes<<<blocks(e - s, 128), 128, 0, st>>>(items, s, e);
     }
     CK4(cudaGetLastError());
-    CK4(cudaMalloc((void**)out, (size_t)*n4 * 128));
+    if (!*out || *out_cap < (size_t)*n4 * 128) {  // the caller's buffer, when it is large enough
+        if (*out) cudaFree(*out);
+        *out = nullptr;
+        *out_cap = 0;
+        CK4(cudaMalloc((void**)out, (size_t)*n4 * 128));
+        *out_cap = (size_t)*n4 * 128;
+    }
     CK4(cudaMemsetAsync(ctr, 0, 4, st));
     for (size_t l = 0; l + 1 < level_start.size(); l++) {
         uint32_t s = level_start[l], e = level_start[l + 1];
@@ -391,8 +397,6 @@ done:
         if (p) cudaFreeAsync(p, st);
     if (res != Collapse::BUILT) {
         cudaStreamSynchronize(st);
-        if (*out) cudaFree(*out);
-        *out = nullptr;
         *n4 = 0;
     }
     return res;
@@ -416,9 +420,9 @@ bool binary_depth_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, uin
     uint32_t *a = nullptr, *b = nullptr, *ctr = nullptr;
     uint32_t h[2] = {0, 0}, K = 1, levels = 0;
     const uint32_t cap = nodes + 2;
-    CKD(cudaMallocAsync((void**)&a, (size_t)cap * 4, st));
-    CKD(cudaMallocAsync((void**)&b, (size_t)cap * 4, st));
-    CKD(cudaMallocAsync((void**)&ctr, 8, st));
+    CKD(scratch_alloc((void**)&a, (size_t)cap * 4, st));
+    CKD(scratch_alloc((void**)&b, (size_t)cap * 4, st));
+    CKD(scratch_alloc((void**)&ctr, 8, st));
     CKD(cudaMemsetAsync(a, 0, 4, st));  // the root
     CKD(cudaMemsetAsync(ctr, 0, 8, st));
     {

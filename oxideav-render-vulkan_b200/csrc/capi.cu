@@ -89,7 +89,7 @@ struct oxpt_ctx {
     // execution mode: megakernel or wavefront, and the wavefront's buffers
     uint32_t mode = OXPT_MODE_WAVEFRONT;
     uint32_t wave_slots = 1u << 20;
-    uint64_t wave_items = 1ull << 24;
+    uint64_t wave_items = oxd::DEFAULT_WAVE_ITEMS;
     uint32_t check_every = 4;
     uint32_t shade_variant = 1, trace_variant = 0, nee_variant = 3, stack = 0;
     uint32_t bvh_depth = 0;
@@ -120,6 +120,7 @@ struct oxpt_ctx {
     unsigned long long* dev_tally = nullptr;  // graph loops: kernels launched, iterations
     float build_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last oxpt_build_scene: phases, wall, tree, launches
     size_t geom_cap = 0, attrs_cap = 0, atlas_cap = 0;  // bytes of the owned scene buffers
+    size_t bvh4_cap = 0, tables_cap = 0;
 };
 
 namespace {
@@ -178,6 +179,7 @@ oxpt_status reserve_dev(oxpt_ctx* c, T** p, size_t* cap, size_t bytes, const cha
 void drop_borrowed_scene(oxpt_ctx* c) {
     if (!c->borrowed_scene) return;
     c->geom_cap = c->attrs_cap = c->atlas_cap = 0;
+    c->bvh4_cap = 0;
     c->geom = nullptr;
     c->attrs = nullptr;
     c->atlas = nullptr;
@@ -607,8 +609,8 @@ oxpt_status oxpt_device_summary(const oxpt_ctx* c, char* buf, size_t len) {
 // tree that does not collapse exactly keeps the binary walk.
 static oxpt_status install_bvh4(oxpt_ctx* c, bool ok, const std::vector<uint32_t>& words, uint32_t root) {
     c->bvh4_built = false;
-    if (!ok) return realloc_dev(c, &c->bvh4, 0, "bvh4");
-    oxpt_status s = realloc_dev(c, &c->bvh4, words.size() * 4, "four-wide tree");
+    if (!ok) return OXPT_OK;  // the binary walk serves every ray
+    oxpt_status s = reserve_dev(c, &c->bvh4, &c->bvh4_cap, words.size() * 4, "four-wide tree");
     if (s) return s;
     if (!words.empty()) {
         CK(c, cudaMemcpyAsync(c->bvh4, words.data(), words.size() * 4, cudaMemcpyHostToDevice, c->stream),
@@ -634,12 +636,12 @@ static oxpt_status upload_bvh4(oxpt_ctx* c, const uint32_t* node_words, uint32_t
 // is read back and collapsed on the host.
 static oxpt_status device_bvh4(oxpt_ctx* c) {
     c->bvh4_built = false;
-    realloc_dev(c, &c->bvh4, 0, "four-wide tree");
-    uint32_t* out = nullptr;
+    uint32_t* out = reinterpret_cast<uint32_t*>(c->bvh4);  // reused when large enough
     uint32_t n4 = 0, root = 0xffffffffu, need = 1;
     std::string e;
     const uint32_t* words = reinterpret_cast<const uint32_t*>(c->geom);
-    oxd::Collapse r = oxd::collapse4_device(words, c->node_count, c->stream, &out, &n4, &root, &need, &e);
+    oxd::Collapse r = oxd::collapse4_device(words, c->node_count, c->stream, &out, &c->bvh4_cap, &n4, &root, &need, &e);
+    c->bvh4 = reinterpret_cast<float4*>(out);
     if (r == oxd::Collapse::FAILED) return fail(c, OXPT_E_CUDA, e);
     if (r == oxd::Collapse::REFUSED) return OXPT_OK;  // the binary walk serves every ray
     if (r == oxd::Collapse::UNSUPPORTED) {
@@ -647,7 +649,6 @@ static oxpt_status device_bvh4(oxpt_ctx* c) {
         CK(c, cudaMemcpy(host.data(), c->geom, host.size() * 4, cudaMemcpyDeviceToHost), "node readback");
         return upload_bvh4(c, host.data(), c->node_count);
     }
-    c->bvh4 = reinterpret_cast<float4*>(out);
     c->bvh4_nodes = n4;
     c->bvh4_root = root;
     c->bvh4_need = need;
@@ -710,6 +711,7 @@ oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* l
     realloc_dev(c, &c->atlas, 0, "texture atlas");
     c->geom_cap = c->attrs_cap = c->atlas_cap = 0;
     realloc_dev(c, &c->bvh4, 0, "four-wide tree");
+    c->bvh4_cap = 0;
     c->bvh4_built = false;
     auto t0 = std::chrono::steady_clock::now();
     oxd::prep::DeviceScene ds;
@@ -763,9 +765,10 @@ oxpt_status oxpt_set_tables(oxpt_ctx* c, const uint32_t* words, size_t count) {
     c->has_tables = false;
     if (c->borrowed_tables) {
         c->tables = nullptr;
+        c->tables_cap = 0;
         c->borrowed_tables = false;
     }
-    if ((s = realloc_dev(c, &c->tables, count * 4, "tables"))) return s;
+    if ((s = reserve_dev(c, &c->tables, &c->tables_cap, count * 4, "tables"))) return s;
     CK(c, cudaMemcpyAsync(c->tables, words, count * 4, cudaMemcpyHostToDevice, c->stream), "tables upload");
     c->table_head.assign(words, words + std::min<size_t>(count, 4096));
     CK(c, cudaStreamSynchronize(c->stream), "tables upload");
@@ -787,6 +790,7 @@ oxpt_status oxpt_share_scene(oxpt_ctx* c, const oxpt_ctx* owner) {
     for (void* p : own)
         if (p) cudaFree(p);
     c->geom_cap = c->attrs_cap = c->atlas_cap = 0;
+    c->bvh4_cap = 0;
     c->geom = owner->geom;
     c->geom_vec4 = owner->geom_vec4;
     c->attrs = owner->attrs;
@@ -817,6 +821,7 @@ oxpt_status oxpt_share_tables(oxpt_ctx* c, const oxpt_ctx* owner) {
     CK(c, cudaStreamSynchronize(owner->stream), "sync before sharing");
     if (c->borrowed_tables) c->tables = nullptr;
     else if (c->tables) cudaFree(c->tables);
+    c->tables_cap = 0;
     c->tables = owner->tables;
     c->table_words = owner->table_words;
     c->table_head = owner->table_head;
@@ -1114,7 +1119,7 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* c, uint32_t threads, uint32_t blocks_
     c->threads = threads ? threads : oxd::TRACE_THREADS;
     c->blocks_per_sm = blocks_per_sm;
     c->max_paths = max_paths ? max_paths : (1ull << 22);
-    c->wave_items = max_paths ? max_paths : (1ull << 24);
+    c->wave_items = max_paths ? max_paths : oxd::DEFAULT_WAVE_ITEMS;
     return OXPT_OK;
 }
 
@@ -1129,7 +1134,7 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     c->blocks_per_sm = t->blocks_per_sm;
     c->wave_slots = t->wave_slots ? t->wave_slots : (1u << 20);
     c->max_paths = t->max_paths ? t->max_paths : (1ull << 22);
-    c->wave_items = t->wave_items ? t->wave_items : (1ull << 24);
+    c->wave_items = t->wave_items ? t->wave_items : oxd::DEFAULT_WAVE_ITEMS;
     c->check_every = t->check_every ? t->check_every : 4u;
     if (t->shade_variant > 2 || t->trace_variant > 2 || t->nee_variant > 5)
         return fail(c, OXPT_E_INVALID, "shade / trace variants are 0, 1 or 2; NEE variants 0 to 5");
@@ -1270,6 +1275,7 @@ oxpt_status oxpt_diag_bvh4_build_device(int device, const uint32_t* geom, uint32
     cudaStream_t st = nullptr;
     uint32_t *d = nullptr, *o = nullptr;
     uint32_t n4 = 0, r = 0xffffffffu, need = 1;
+    size_t ocap = 0;
     oxpt_status res = OXPT_OK;
     std::string e;
     oxd::Collapse c4 = oxd::Collapse::FAILED;
@@ -1283,7 +1289,7 @@ oxpt_status oxpt_diag_bvh4_build_device(int device, const uint32_t* geom, uint32
         res = OXPT_E_CUDA;
         goto done;
     }
-    c4 = oxd::collapse4_device(d, node_count, st, &o, &n4, &r, &need, &e);
+    c4 = oxd::collapse4_device(d, node_count, st, &o, &ocap, &n4, &r, &need, &e);
     if (c4 == oxd::Collapse::FAILED) res = OXPT_E_CUDA;
     else if (c4 == oxd::Collapse::REFUSED) res = OXPT_E_INVALID;
     else if (c4 == oxd::Collapse::UNSUPPORTED) res = OXPT_E_LIMIT;

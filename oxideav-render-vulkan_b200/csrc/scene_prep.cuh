@@ -15,8 +15,8 @@ namespace bvhb {
 // Binned-SAH BVH over n triangles whose positions (9 floats each) are in
 // device memory, built on stream st. On success *words (nodes x 8 words)
 // and *slots (leaf slot -> triangle, n entries) are stream-ordered device
-// allocations (cudaMallocAsync on st) that the caller frees with
-// cudaFreeAsync. Scratch is stream-ordered too, so the build never waits
+// allocations (the library's scratch pool, pool.cuh) that the caller frees
+// with cudaFreeAsync. Scratch is stream-ordered too, so the build never waits
 // for other streams' work. False with *err when an allocation or launch
 // fails.
 bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** words, uint32_t** slots,
@@ -26,12 +26,14 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
 
 // Four-wide any-hit tree collapsed on the device from binary node words in
 // device memory (bvh4_build.cu): the host collapse's words (host/bvh4.cpp),
-// node for node. BUILT: *out (cudaMalloc, n4 x 32 words; null when the
-// root is a leaf), *root_ref and *need are set. REFUSED: the host collapse
+// node for node. BUILT: *out holds n4 x 32 words (the caller's buffer of
+// *out_cap bytes when large enough, else a new cudaMalloc that replaces
+// it; untouched when the root is a leaf), *root_ref and *need are set. REFUSED: the host collapse
 // refuses the tree too (keep the binary walk). UNSUPPORTED: deeper than
 // 64 four-wide levels (collapse on the host). FAILED: a CUDA error.
 enum class Collapse { BUILT, REFUSED, UNSUPPORTED, FAILED };
-Collapse collapse4_device(const uint32_t* words, uint32_t nodes, cudaStream_t st, uint32_t** out, uint32_t* n4,
+Collapse collapse4_device(const uint32_t* words, uint32_t nodes, cudaStream_t st, uint32_t** out, size_t* out_cap,
+                          uint32_t* n4,
                           uint32_t* root_ref, uint32_t* need, std::string* err);
 // Levels of the binary tree (65 when deeper than 64 or malformed), as the
 // host's depth walk counts them.

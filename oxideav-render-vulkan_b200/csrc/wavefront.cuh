@@ -38,6 +38,12 @@ struct BatchFrame {
     uint32_t first, y0, npix, pad;
 };
 
+// Default paths per wavefront launch round: a 1920x1080 frame of 64 spp
+// (133 M paths) in one round, so its regeneration tail comes once instead
+// of once per round; the per-path result buffer holds one round (16 bytes a
+// path, at most 2 GiB, less for smaller refines).
+constexpr uint64_t DEFAULT_WAVE_ITEMS = 1ull << 27;
+
 // Radiance-cache frame (split plan only; `on` = 0 otherwise): paths that
 // are not training paths end with a cache query (features, throughput,
 // result index) at their first vertex at or after bounce `query_k` whose
