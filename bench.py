@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--wave-items", type=int, default=0, help="wavefront paths per launch round (0: the plan's)")
+    ap.add_argument("--nee-variant", type=int, default=-1, help="serve workload: the executor's NEE kernel "
+                    "(-1: the serving executor's default, job-major)")
     ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
                     help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
     ap.add_argument("--requests", type=int, default=300, help="serve workload: requests in the stream")
@@ -523,6 +525,8 @@ def run_serve(a):
     check = set(int(x) for x in np.random.default_rng(9).choice(a.requests, size=4, replace=False))
     ex = serve.GpuExecutor(pkg, owners, options, keep=lambda o: o.rid in check)
     ex.exe.set_tuning(mode=2, graphs=1)
+    if a.nee_variant >= 0:
+        ex.exe.set_tuning(nee_variant=a.nee_variant)
     budget = 150 << 30
     served = serve.Server(ex, budget, tick_paths=1 << 24).run(reqs)
     ex2 = serve.GpuExecutor(pkg, owners, options)
