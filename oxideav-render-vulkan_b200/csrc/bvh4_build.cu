@@ -25,7 +25,6 @@
 #include <string>
 #include <vector>
 
-#include "pool.cuh"
 #include "scene_prep.cuh"
 
 namespace oxd {
@@ -323,11 +322,11 @@ Collapse collapse4_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, ui
         return Collapse::BUILT;
     }
     *root_ref = 0;
-    CK4(scratch_alloc((void**)&items, (size_t)cap * sizeof(Item), st));
-    CK4(scratch_alloc((void**)&counts, (size_t)cap * 4, st));
-    CK4(scratch_alloc((void**)&sums, (size_t)blocks(cap, 1024) * 4, st));
-    CK4(scratch_alloc((void**)&sums2, 1024 * 4, st));
-    CK4(scratch_alloc((void**)&ctr, 8, st));  // total, bad
+    CK4(cudaMallocAsync((void**)&items, (size_t)cap * sizeof(Item), st));
+    CK4(cudaMallocAsync((void**)&counts, (size_t)cap * 4, st));
+    CK4(cudaMallocAsync((void**)&sums, (size_t)blocks(cap, 1024) * 4, st));
+    CK4(cudaMallocAsync((void**)&sums2, 1024 * 4, st));
+    CK4(cudaMallocAsync((void**)&ctr, 8, st));  // total, bad
     {
         Item root{};
         root.b = 0;
@@ -420,9 +419,9 @@ bool binary_depth_device(const uint32_t* w, uint32_t nodes, cudaStream_t st, uin
     uint32_t *a = nullptr, *b = nullptr, *ctr = nullptr;
     uint32_t h[2] = {0, 0}, K = 1, levels = 0;
     const uint32_t cap = nodes + 2;
-    CKD(scratch_alloc((void**)&a, (size_t)cap * 4, st));
-    CKD(scratch_alloc((void**)&b, (size_t)cap * 4, st));
-    CKD(scratch_alloc((void**)&ctr, 8, st));
+    CKD(cudaMallocAsync((void**)&a, (size_t)cap * 4, st));
+    CKD(cudaMallocAsync((void**)&b, (size_t)cap * 4, st));
+    CKD(cudaMallocAsync((void**)&ctr, 8, st));
     CKD(cudaMemsetAsync(a, 0, 4, st));  // the root
     CKD(cudaMemsetAsync(ctr, 0, 8, st));
     {

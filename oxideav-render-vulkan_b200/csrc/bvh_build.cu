@@ -27,7 +27,6 @@
 
 #include "../../include/oxpt_diag.h"
 #include "../host/bvh_gpu.hpp"
-#include "pool.cuh"
 
 namespace oxd {
 namespace bvhb {
@@ -941,26 +940,26 @@ bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** w
     const size_t max_large = n / LARGE + 2, max_huge = n / HUGE_N + 2, max_chunks = n / CHUNK + max_huge + 1;
     uint32_t K = 1, nodes = 1, levels = 0, launches = 0;
     uint32_t M = 0, Lg = 0, H = 0;  // this level's medium / large / huge nodes
-    BK(scratch_alloc((void**)&blo, (size_t)n * 16, st));
-    BK(scratch_alloc((void**)&bhi, (size_t)n * 16, st));
-    BK(scratch_alloc((void**)&cen, (size_t)n * 16, st));
-    BK(scratch_alloc((void**)&ids, (size_t)n * 4, st));
-    BK(scratch_alloc((void**)&ids2, (size_t)n * 4, st));
-    BK(scratch_alloc((void**)&words, max_nodes * 32, st));
-    BK(scratch_alloc((void**)&jobs, max_jobs * sizeof(Job), st));
-    BK(scratch_alloc((void**)&next, max_jobs * sizeof(Job), st));
-    BK(scratch_alloc((void**)&dec, max_jobs * sizeof(Decision), st));
-    BK(scratch_alloc((void**)&excl, max_jobs * 4, st));
-    BK(scratch_alloc((void**)&sums, ((max_jobs + 1023) / 1024) * 4, st));
-    BK(scratch_alloc((void**)&sums2, 1024 * 4, st));
-    BK(scratch_alloc((void**)&ctr, 4 * 4, st));
-    BK(scratch_alloc((void**)&l_medium, max_jobs * 4, st));
-    BK(scratch_alloc((void**)&l_large, max_large * 4, st));
-    BK(scratch_alloc((void**)&l_huge, max_huge * 4, st));
-    BK(scratch_alloc((void**)&hn, max_huge * sizeof(HugeNode), st));
-    BK(scratch_alloc((void**)&acc, max_huge * sizeof(HugeAcc), st));
-    BK(scratch_alloc((void**)&chunk_left, max_chunks * 4, st));
-    BK(scratch_alloc((void**)&total_chunks, 4, st));
+    BK(cudaMallocAsync((void**)&blo, (size_t)n * 16, st));
+    BK(cudaMallocAsync((void**)&bhi, (size_t)n * 16, st));
+    BK(cudaMallocAsync((void**)&cen, (size_t)n * 16, st));
+    BK(cudaMallocAsync((void**)&ids, (size_t)n * 4, st));
+    BK(cudaMallocAsync((void**)&ids2, (size_t)n * 4, st));
+    BK(cudaMallocAsync((void**)&words, max_nodes * 32, st));
+    BK(cudaMallocAsync((void**)&jobs, max_jobs * sizeof(Job), st));
+    BK(cudaMallocAsync((void**)&next, max_jobs * sizeof(Job), st));
+    BK(cudaMallocAsync((void**)&dec, max_jobs * sizeof(Decision), st));
+    BK(cudaMallocAsync((void**)&excl, max_jobs * 4, st));
+    BK(cudaMallocAsync((void**)&sums, ((max_jobs + 1023) / 1024) * 4, st));
+    BK(cudaMallocAsync((void**)&sums2, 1024 * 4, st));
+    BK(cudaMallocAsync((void**)&ctr, 4 * 4, st));
+    BK(cudaMallocAsync((void**)&l_medium, max_jobs * 4, st));
+    BK(cudaMallocAsync((void**)&l_large, max_large * 4, st));
+    BK(cudaMallocAsync((void**)&l_huge, max_huge * 4, st));
+    BK(cudaMallocAsync((void**)&hn, max_huge * sizeof(HugeNode), st));
+    BK(cudaMallocAsync((void**)&acc, max_huge * sizeof(HugeAcc), st));
+    BK(cudaMallocAsync((void**)&chunk_left, max_chunks * 4, st));
+    BK(cudaMallocAsync((void**)&total_chunks, 4, st));
     tri_prep<<<(n + 255) / 256, 256, 0, st>>>(pos, n, blo, bhi, cen, ids);
     BK(cudaGetLastError());
     launches++;

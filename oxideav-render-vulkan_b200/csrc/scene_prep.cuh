@@ -15,8 +15,8 @@ namespace bvhb {
 // Binned-SAH BVH over n triangles whose positions (9 floats each) are in
 // device memory, built on stream st. On success *words (nodes x 8 words)
 // and *slots (leaf slot -> triangle, n entries) are stream-ordered device
-// allocations (the library's scratch pool, pool.cuh) that the caller frees
-// with cudaFreeAsync. Scratch is stream-ordered too, so the build never waits
+// allocations (cudaMallocAsync on st) that the caller frees with
+// cudaFreeAsync. Scratch is stream-ordered too, so the build never waits
 // for other streams' work. False with *err when an allocation or launch
 // fails.
 bool build_on_device(const float* pos, uint32_t n, cudaStream_t st, uint32_t** words, uint32_t** slots,
