@@ -149,6 +149,26 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* ctx, const oxpt_scene_desc* scene);
 oxpt_status oxpt_set_tables(oxpt_ctx* ctx, const uint32_t* words, size_t count);
 
 /*
+ * The next scene and its tables (oxpt_upload_scene + oxpt_set_tables in one
+ * call) uploaded while work already queued on the context keeps tracing the
+ * current scene: the reference's upload (src/pathtrace.rs:970-1239) waits
+ * for the device, this does not. The context keeps a second set of scene
+ * buffers; the copies and the upload's tree passes run on a stream of
+ * their own, after the last work that traced that set. The call returns
+ * once the host buffers have been read (pinned host memory makes the copies
+ * asynchronous DMA); the next oxpt_refine / oxpt_dispatch on the context
+ * waits for the upload on the device and traces the new scene. Params for
+ * the new scene may be set before that call. oxpt_upload_scene,
+ * oxpt_set_tables and oxpt_build_scene first make a staged scene current.
+ * Not for contexts that lend their scene to others (oxpt_share_scene) or
+ * borrow one, nor for contexts traced by another context's batches
+ * (oxpt_refine_batch with a different executor): those must use
+ * oxpt_upload_scene. No reference counterpart.
+ */
+oxpt_status oxpt_stage_scene(oxpt_ctx* ctx, const oxpt_scene_desc* scene, const uint32_t* tables,
+                             size_t table_words);
+
+/*
  * Scene preparation on the device: the buffers of oxpt_upload_scene built
  * by the GPU from the scene's sources instead of by the host. Replaces the
  * host passes of upload (src/pathtrace.rs:970-1239): the BVH the external
@@ -283,7 +303,11 @@ oxpt_status oxpt_accum_view(oxpt_ctx* ctx, oxpt_devimage* out);
  * array, which keeps the previous call's contents: calls whose work
  * overlaps on the GPU (different streams, or different host threads on the
  * same device) race on it and must be ordered by the caller. A malformed
- * BVH is cut short on the device, not reported.
+ * BVH is cut short on the device and not reported (the call has no place to
+ * return the device's error word without a readback): pass scenes that this
+ * library prepared (oxpt_build_scene, the host preparation) or that the
+ * caller has checked. After a device reset (cudaDeviceReset, or a reset of
+ * the primary context) the next call looks the array's address up again.
  */
 #define OXPT_NOALLOC_MAX_PATHS (1u << 18)
 typedef struct oxpt_device_scene {

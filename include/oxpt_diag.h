@@ -84,6 +84,13 @@ oxpt_status oxpt_diag_counters_split(const oxpt_ctx* ctx, uint64_t out[16]);
 oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t blocks_per_sm,
                                  uint64_t max_paths_per_launch);
 
+/* Traversal kernels of trace_variant 3-5: walk-stack entries per lane kept
+ * in shared memory (default all the kernel's columns: 8 for binary walks,
+ * 16 for four-wide ones); deeper entries live in local memory. Smaller
+ * values only move entries to local memory (results are unchanged), which
+ * lets tests exercise that path on shallow trees. */
+oxpt_status oxpt_diag_set_walk_shared(oxpt_ctx* ctx, uint32_t entries);
+
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left
  * at the defaults. Every plan produces bit-identical accumulators; only
@@ -99,7 +106,9 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  *                  checks.
  *   shade_variant  wavefront logic kernel compiled for 2 / 3 / 4 resident
  *                  blocks per SM (0 / 1 / 2): registers against occupancy.
- *   trace_variant  wavefront traversal kernels for 6 / 8 / 10 blocks.
+ *   trace_variant  wavefront traversal kernels for 6 / 8 / 10 blocks; 3-5:
+ *                  shared-memory short stacks and staged top nodes, for
+ *                  8 / 10 / 12 blocks.
  *   nee_variant    split wavefront NEE kernel: job-major (0, 1, 2) or
  *                  vertex-major (3, 4, 5) for 4 / 5 / 6 blocks.
  *   OXPT_MODE_WAVEFRONT_SPLIT: the wavefront with the shading of a bounce

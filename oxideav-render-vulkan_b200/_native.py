@@ -10,6 +10,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboxpt.so"
+HOST_LIB_PATH = HERE / "liboxpt_host.so"  # scene building and preparation only, no CUDA
 
 u8, u16, u32, u64, i32, f32 = C.c_uint8, C.c_uint16, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
 vp, sz, cint = C.c_void_p, C.c_size_t, C.c_int
@@ -131,6 +132,7 @@ _SIGS = {
     "oxpt_device_summary": (cint, [vp, C.c_char_p, sz]),
     "oxpt_upload_scene": (cint, [vp, C.POINTER(SceneDesc)]),
     "oxpt_set_tables": (cint, [vp, vp, sz]),
+    "oxpt_stage_scene": (cint, [vp, C.POINTER(SceneDesc), vp, sz]),
     "oxpt_share_scene": (cint, [vp, vp]),
     "oxpt_share_tables": (cint, [vp, vp]),
     "oxpt_set_params": (cint, [vp, C.POINTER(Params)]),
@@ -156,6 +158,7 @@ _SIGS = {
     "oxpt_diag_math": (cint, [vp, cint, sz, vp, vp, vp]),
     "oxpt_diag_refine_counted": (cint, [vp, u32, u32, vp]),
     "oxpt_diag_set_launch": (cint, [vp, u32, u32, u64]),
+    "oxpt_diag_set_walk_shared": (cint, [vp, u32]),
     "oxpt_diag_launch_count": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_set_timing": (cint, [vp, cint]),
     "oxpt_set_tuning": (cint, [vp, C.POINTER(Tuning)]),
@@ -245,18 +248,34 @@ _SIGS = {
 }
 
 _lib = None
+_host_only = False
+
+
+def select_host_only():
+    """Make lib() load liboxpt_host.so instead: scene building and
+    preparation on the CPU, with no CUDA library mapped into the process.
+    Tracer calls are then unavailable (their symbols are absent). Must be
+    called before the first lib()."""
+    global _host_only
+    if _lib is not None and not _host_only:
+        raise RuntimeError("liboxpt.so is already loaded in this process")
+    _host_only = True
 
 
 def lib() -> C.CDLL:
-    """The loaded liboxpt.so (raises if it has not been built)."""
+    """The loaded liboxpt.so (raises if it has not been built), or
+    liboxpt_host.so after select_host_only()."""
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
+        path = HOST_LIB_PATH if _host_only else LIB_PATH
+        if not path.exists():
             raise RuntimeError(
-                f"{LIB_PATH} is missing: build it with oxideav-render-vulkan_b200/build.py "
+                f"{path} is missing: build it with oxideav-render-vulkan_b200/build.py "
                 "(there is no CPU fallback for the path tracer)")
-        L = C.CDLL(str(LIB_PATH))
+        L = C.CDLL(str(path))
         for name, (res, args) in _SIGS.items():
+            if _host_only and not hasattr(L, name):
+                continue
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args

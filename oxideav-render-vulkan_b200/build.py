@@ -19,6 +19,10 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 LIB = HERE / "liboxpt.so"
+# Scene building and preparation alone (no CUDA): what a process that only
+# prepares scenes on the CPU loads (the benchmark's CPU reference arm).
+HOST_LIB = HERE / "liboxpt_host.so"
+HOST_ONLY = ("prepare", "scene", "bvh", "bvh4", "batch")
 BUILD = ROOT / "_build" / "oxpt"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -87,6 +91,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         tmp = LIB.with_suffix(".so.tmp")
         _run([nv, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"])
         os.replace(tmp, LIB)
+    host_objs = [BUILD / (n + ".cpp.o") for n in HOST_ONLY]
+    if not HOST_LIB.exists() or any(o.stat().st_mtime > HOST_LIB.stat().st_mtime for o in host_objs):
+        tmp = HOST_LIB.with_suffix(".so.tmp")
+        _run(["g++", "-shared", "-o", str(tmp), *map(str, host_objs), "-lpthread"])
+        os.replace(tmp, HOST_LIB)
     if verbose:
         for log in logs:
             if log.strip():

@@ -30,6 +30,28 @@
 #include "../host/bvh4.hpp"
 #include "scene_prep.cuh"
 
+// A scene's device buffers and what the context knows of them. The
+// context traces its current set (the oxpt_ctx fields of the same names);
+// oxpt_stage_scene fills a second set while queued work still traces the
+// current one, and the next trace call swaps them.
+struct SceneSet {
+    float4* geom = nullptr;
+    size_t geom_vec4 = 0, geom_cap = 0;
+    float4* attrs = nullptr;
+    size_t slot_count = 0, attrs_cap = 0;
+    uint2* atlas = nullptr;
+    uint32_t side = 1, layers = 1;
+    size_t atlas_cap = 0;
+    uint32_t node_count = 0, bvh_depth = 0;
+    float4* bvh4 = nullptr;
+    size_t bvh4_cap = 0;
+    bool bvh4_built = false;
+    uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
+    uint32_t* tables = nullptr;
+    size_t table_words = 0, tables_cap = 0;
+    std::vector<uint32_t> table_head;
+};
+
 struct oxpt_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -99,6 +121,7 @@ struct oxpt_ctx {
     uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
     uint32_t shadow_walk = 0;
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
+    uint32_t walk_lim = 0xffffffffu;  // traversal variants 3-5: shared stack entries per lane (diagnostic)
     void* wave_mem = nullptr;
     size_t wave_bytes = 0;
     uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
@@ -121,6 +144,12 @@ struct oxpt_ctx {
     float build_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last oxpt_build_scene: phases, wall, tree, launches
     size_t geom_cap = 0, attrs_cap = 0, atlas_cap = 0;  // bytes of the owned scene buffers
     size_t bvh4_cap = 0, tables_cap = 0;
+    // oxpt_stage_scene: the second buffer set, its upload stream and events
+    SceneSet back;
+    bool staged = false;          // `back` holds a scene not yet traced
+    bool back_free_valid = false;  // back_free marks the back set's last use
+    cudaStream_t upload = nullptr;
+    cudaEvent_t staged_ready = nullptr, back_free = nullptr;
 };
 
 namespace {
@@ -214,7 +243,52 @@ oxpt_status set_device(oxpt_ctx* c) {
     return OXPT_OK;
 }
 
+void swap_scene(oxpt_ctx* c) {
+    SceneSet& b = c->back;
+    std::swap(c->geom, b.geom);
+    std::swap(c->geom_vec4, b.geom_vec4);
+    std::swap(c->geom_cap, b.geom_cap);
+    std::swap(c->attrs, b.attrs);
+    std::swap(c->slot_count, b.slot_count);
+    std::swap(c->attrs_cap, b.attrs_cap);
+    std::swap(c->atlas, b.atlas);
+    std::swap(c->side, b.side);
+    std::swap(c->layers, b.layers);
+    std::swap(c->atlas_cap, b.atlas_cap);
+    std::swap(c->node_count, b.node_count);
+    std::swap(c->bvh_depth, b.bvh_depth);
+    std::swap(c->bvh4, b.bvh4);
+    std::swap(c->bvh4_cap, b.bvh4_cap);
+    std::swap(c->bvh4_built, b.bvh4_built);
+    std::swap(c->bvh4_nodes, b.bvh4_nodes);
+    std::swap(c->bvh4_root, b.bvh4_root);
+    std::swap(c->bvh4_need, b.bvh4_need);
+    std::swap(c->tables, b.tables);
+    std::swap(c->table_words, b.table_words);
+    std::swap(c->tables_cap, b.tables_cap);
+    std::swap(c->table_head, b.table_head);
+}
+
+// Makes a staged scene current: work enqueued from here on waits for its
+// upload on the device and traces it; everything enqueued before traced
+// the previous set, whose last use the back_free event marks.
+oxpt_status activate_staged(oxpt_ctx* c) {
+    if (!c->staged) return OXPT_OK;
+    CK(c, cudaSetDevice(c->device), "cudaSetDevice");
+    CK(c, cudaStreamWaitEvent(c->stream, c->staged_ready, 0), "staged scene order");
+    swap_scene(c);
+    c->staged = false;
+    c->has_scene = true;
+    c->has_tables = true;
+    if (c->stack == 32 && c->bvh_depth > 32) c->stack = 0;
+    CK(c, cudaEventRecord(c->back_free, c->stream), "staged scene order");
+    c->back_free_valid = true;
+    return OXPT_OK;
+}
+
 oxpt_status ready(oxpt_ctx* c) {
+    oxpt_status s = activate_staged(c);
+    if (s) return s;
     if (!c->has_scene || !c->has_tables || !c->has_params) return fail(c, OXPT_E_INVALID, "scene, tables and params must be set first");
     if (!c->accum) return fail(c, OXPT_E_INVALID, "no accumulator: call oxpt_resize first");
     if (c->params.dims[0] != c->w || c->params.dims[1] != c->h)
@@ -357,6 +431,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const ox
     wa.frames = nullptr;
     wa.nframes = 0;
     wa.nrc = nrc ? *nrc : oxd::NrcWave{};
+    wa.walk_lim = c->walk_lim;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
     bool four = c->shadow_walk == 0 && bvh4_usable(c);
@@ -562,8 +637,13 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
     }
     drop_borrowed_scene(c);
     if (c->borrowed_tables) c->tables = nullptr;
+    if (c->upload) cudaStreamSynchronize(c->upload);
     void* ptrs[] = {c->geom, c->attrs, c->atlas, c->tables, c->accum, c->img8, c->img32, c->out, c->dev_err,
-                    c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev};
+                    c->dev_counters, c->wave_mem, c->bvh4, c->batch_dev, c->back.geom, c->back.attrs,
+                    c->back.atlas, c->back.bvh4, c->back.tables};
+    if (c->upload) cudaStreamDestroy(c->upload);
+    if (c->staged_ready) cudaEventDestroy(c->staged_ready);
+    if (c->back_free) cudaEventDestroy(c->back_free);
     if (c->batch_done) cudaEventDestroy(c->batch_done);
     if (c->copy) cudaStreamSynchronize(c->copy);
     if (c->present) cudaFree(c->present);
@@ -658,6 +738,7 @@ static oxpt_status device_bvh4(oxpt_ctx* c) {
 
 oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     if (!c || !d) return fail(c, OXPT_E_INVALID, "null argument");
+    if (oxpt_status sa = activate_staged(c)) return sa;
     if (!d->geom || d->geom_words < 8 || d->geom_words % 4 != 0) return fail(c, OXPT_E_INVALID, "geom must hold at least one node (8 words), a multiple of 4 words");
     if (!d->attrs || d->attr_floats < 48 || d->attr_floats % 48 != 0) return fail(c, OXPT_E_INVALID, "attrs must be 48 floats per slot");
     if ((size_t)d->node_count * 8 + (size_t)d->slot_count * 12 > d->geom_words) return fail(c, OXPT_E_INVALID, "geom smaller than nodes + triangles");
@@ -698,8 +779,77 @@ oxpt_status oxpt_upload_scene(oxpt_ctx* c, const oxpt_scene_desc* d) {
     return OXPT_OK;
 }
 
+// The staged upload: the scene's buffers and tables go into the context's
+// second buffer set on its upload stream, after the work that last traced
+// that set; the tree passes of an upload (depth, four-wide collapse) run
+// there too. The host waits for those, not for the context's stream, so
+// the copies overlap whatever is already queued there.
+oxpt_status oxpt_stage_scene(oxpt_ctx* c, const oxpt_scene_desc* d, const uint32_t* tables, size_t table_words) {
+    if (!c || !d) return fail(c, OXPT_E_INVALID, "null argument");
+    if (!tables || table_words == 0) return fail(c, OXPT_E_INVALID, "empty tables");
+    if (!d->geom || d->geom_words < 8 || d->geom_words % 4 != 0) return fail(c, OXPT_E_INVALID, "geom must hold at least one node (8 words), a multiple of 4 words");
+    if (!d->attrs || d->attr_floats < 48 || d->attr_floats % 48 != 0) return fail(c, OXPT_E_INVALID, "attrs must be 48 floats per slot");
+    if ((size_t)d->node_count * 8 + (size_t)d->slot_count * 12 > d->geom_words) return fail(c, OXPT_E_INVALID, "geom smaller than nodes + triangles");
+    if ((size_t)d->slot_count * 48 > d->attr_floats) return fail(c, OXPT_E_INVALID, "attrs smaller than the slot count");
+    if (!d->atlas || d->atlas_side == 0 || d->atlas_layers == 0) return fail(c, OXPT_E_INVALID, "atlas must have at least one layer");
+    if (d->atlas_side > 16384) return fail(c, OXPT_E_LIMIT, "atlas layer side above 16384");
+    if (c->borrowed_scene || c->borrowed_tables)
+        return fail(c, OXPT_E_INVALID, "a context borrowing a scene or tables cannot stage one");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    if (!c->upload) CK(c, cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking), "upload stream");
+    if (!c->staged_ready) CK(c, cudaEventCreateWithFlags(&c->staged_ready, cudaEventDisableTiming), "upload event");
+    if (!c->back_free) CK(c, cudaEventCreateWithFlags(&c->back_free, cudaEventDisableTiming), "upload event");
+    SceneSet& b = c->back;
+    c->staged = false;
+    // The back set was last traced by work enqueued before the last swap.
+    if (c->back_free_valid) CK(c, cudaStreamWaitEvent(c->upload, c->back_free, 0), "upload order");
+    size_t gbytes = d->geom_words * 4, abytes = d->attr_floats * 4;
+    size_t tbytes = (size_t)d->atlas_side * d->atlas_side * d->atlas_layers * 8;
+    if (b.geom_cap < gbytes || b.attrs_cap < abytes || b.atlas_cap < tbytes || b.tables_cap < table_words * 4)
+        CK(c, cudaStreamSynchronize(c->upload), "upload order");  // the buffers may be freed
+    if ((s = reserve_dev(c, &b.geom, &b.geom_cap, gbytes, "geom buffer"))) return s;
+    if ((s = reserve_dev(c, &b.attrs, &b.attrs_cap, abytes, "attribute buffer"))) return s;
+    if ((s = reserve_dev(c, &b.atlas, &b.atlas_cap, tbytes, "texture atlas"))) return s;
+    if ((s = reserve_dev(c, &b.tables, &b.tables_cap, table_words * 4, "tables"))) return s;
+    CK(c, cudaMemcpyAsync(b.geom, d->geom, gbytes, cudaMemcpyHostToDevice, c->upload), "geom upload");
+    CK(c, cudaMemcpyAsync(b.attrs, d->attrs, abytes, cudaMemcpyHostToDevice, c->upload), "attr upload");
+    CK(c, cudaMemcpyAsync(b.atlas, d->atlas, tbytes, cudaMemcpyHostToDevice, c->upload), "atlas upload");
+    CK(c, cudaMemcpyAsync(b.tables, tables, table_words * 4, cudaMemcpyHostToDevice, c->upload), "tables upload");
+    b.geom_vec4 = d->geom_words / 4;
+    b.slot_count = d->attr_floats / 48;
+    b.side = d->atlas_side;
+    b.layers = d->atlas_layers;
+    b.node_count = d->node_count;
+    b.table_words = table_words;
+    b.table_head.assign(tables, tables + std::min<size_t>(table_words, 4096));
+    std::string e;
+    uint32_t depth = 0;
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(b.geom);
+    if (!oxd::binary_depth_device(words, d->node_count, c->upload, &depth, &e)) return fail(c, OXPT_E_CUDA, e);
+    b.bvh_depth = depth;
+    b.bvh4_built = false;
+    uint32_t* out = reinterpret_cast<uint32_t*>(b.bvh4);
+    uint32_t n4 = 0, root = 0xffffffffu, need = 1;
+    oxd::Collapse r = oxd::collapse4_device(words, d->node_count, c->upload, &out, &b.bvh4_cap, &n4, &root, &need, &e);
+    b.bvh4 = reinterpret_cast<float4*>(out);
+    if (r == oxd::Collapse::FAILED) return fail(c, OXPT_E_CUDA, e);
+    if (r == oxd::Collapse::BUILT) {
+        b.bvh4_nodes = n4;
+        b.bvh4_root = root;
+        b.bvh4_need = need;
+        b.bvh4_built = true;
+    }
+    // REFUSED / UNSUPPORTED: the binary walk serves every ray of this scene.
+    CK(c, cudaEventRecord(c->staged_ready, c->upload), "upload event");
+    CK(c, cudaStreamSynchronize(c->upload), "staged upload");  // host buffers consumed
+    c->staged = true;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* light_slots, uint32_t out[3]) {
     if (!c || !src || !out) return fail(c, OXPT_E_INVALID, "null argument");
+    if (oxpt_status sa = activate_staged(c)) return sa;
     oxpt_status s = set_device(c);
     if (s) return s;
     CK(c, cudaStreamSynchronize(c->stream), "sync before scene build");
@@ -746,6 +896,7 @@ oxpt_status oxpt_build_scene(oxpt_ctx* c, const oxpt_scene_src* src, uint32_t* l
 
 oxpt_status oxpt_read_scene(oxpt_ctx* c, uint32_t* geom, float* attrs, uint16_t* atlas) {
     if (!c || !geom || !attrs || !atlas) return fail(c, OXPT_E_INVALID, "null argument");
+    if (oxpt_status sa = activate_staged(c)) return sa;
     if (!c->has_scene) return fail(c, OXPT_E_INVALID, "no scene");
     oxpt_status s = set_device(c);
     if (s) return s;
@@ -759,6 +910,7 @@ oxpt_status oxpt_read_scene(oxpt_ctx* c, uint32_t* geom, float* attrs, uint16_t*
 
 oxpt_status oxpt_set_tables(oxpt_ctx* c, const uint32_t* words, size_t count) {
     if (!c || !words || count == 0) return fail(c, OXPT_E_INVALID, "empty tables");
+    if (oxpt_status sa = activate_staged(c)) return sa;
     oxpt_status s = set_device(c);
     if (s) return s;
     CK(c, cudaStreamSynchronize(c->stream), "sync before tables");
@@ -780,6 +932,8 @@ oxpt_status oxpt_set_tables(oxpt_ctx* c, const uint32_t* words, size_t count) {
 oxpt_status oxpt_share_scene(oxpt_ctx* c, const oxpt_ctx* owner) {
     if (!c || !owner || c == owner) return fail(c, OXPT_E_INVALID, "sharing needs two contexts");
     if (!owner->has_scene) return fail(c, OXPT_E_INVALID, "the lending context has no scene");
+    if (owner->staged || owner->back_free_valid || c->staged)
+        return fail(c, OXPT_E_INVALID, "contexts that stage scenes (oxpt_stage_scene) do not share them");
     if (owner->device != c->device) return fail(c, OXPT_E_INVALID, "the lending context is on another device");
     oxpt_status s = set_device(c);
     if (s) return s;
@@ -832,7 +986,9 @@ oxpt_status oxpt_share_tables(oxpt_ctx* c, const oxpt_ctx* owner) {
 
 oxpt_status oxpt_set_params(oxpt_ctx* c, const oxpt_params* p) {
     if (!c || !p) return fail(c, OXPT_E_INVALID, "null params");
-    if (c->has_scene && p->env[3] > c->node_count) return fail(c, OXPT_E_INVALID, "node count above the uploaded nodes");
+    const bool scene = c->has_scene || c->staged;
+    const uint32_t nodes = c->staged ? c->back.node_count : c->node_count;
+    if (scene && p->env[3] > nodes) return fail(c, OXPT_E_INVALID, "node count above the uploaded nodes");
     if (p->env[2] && (p->env[0] == 0 || p->env[1] == 0)) return fail(c, OXPT_E_INVALID, "environment of zero size");
     c->params = *p;
     c->has_params = true;
@@ -1036,6 +1192,7 @@ oxpt_status oxpt_diag_sobol(oxpt_ctx* c, const uint32_t* dirs, uint32_t seed, si
 oxpt_status oxpt_diag_trace_rays(oxpt_ctx* c, size_t n, const float* rays, uint32_t flags, uint32_t* slot,
                                  uint32_t* gid, float* t, float* bary) {
     if (!c || (n && !rays)) return fail(c, OXPT_E_INVALID, "null argument");
+    if (oxpt_status sa = activate_staged(c)) return sa;
     if (!c->has_scene || !c->has_tables || !c->has_params) return fail(c, OXPT_E_INVALID, "scene, tables and params must be set first");
     if ((flags & 4u) && !bvh4_usable(c)) return fail(c, OXPT_E_INVALID, "no four-wide tree for this scene");
     if (n == 0) return OXPT_OK;
@@ -1112,6 +1269,12 @@ oxpt_status oxpt_diag_counters_split(const oxpt_ctx* c, uint64_t out[16]) {
     return OXPT_OK;
 }
 
+oxpt_status oxpt_diag_set_walk_shared(oxpt_ctx* c, uint32_t entries) {
+    if (!c) return OXPT_E_INVALID;
+    c->walk_lim = entries;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_diag_set_launch(oxpt_ctx* c, uint32_t threads, uint32_t blocks_per_sm, uint64_t max_paths) {
     if (!c) return OXPT_E_INVALID;
     if (threads && (threads % 32 != 0 || threads > oxd::TRACE_THREADS))
@@ -1136,8 +1299,8 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     c->max_paths = t->max_paths ? t->max_paths : (1ull << 22);
     c->wave_items = t->wave_items ? t->wave_items : oxd::DEFAULT_WAVE_ITEMS;
     c->check_every = t->check_every ? t->check_every : 4u;
-    if (t->shade_variant > 2 || t->trace_variant > 2 || t->nee_variant > 5)
-        return fail(c, OXPT_E_INVALID, "shade / trace variants are 0, 1 or 2; NEE variants 0 to 5");
+    if (t->shade_variant > 2 || t->trace_variant > 5 || t->nee_variant > 5)
+        return fail(c, OXPT_E_INVALID, "shade variants are 0, 1 or 2; trace and NEE variants 0 to 5");
     if (t->stack && t->stack != 32 && t->stack != 64) return fail(c, OXPT_E_INVALID, "stack is 0, 32 or 64");
     if (t->stack == 32 && c->bvh_depth > 32) return fail(c, OXPT_E_INVALID, "the BVH is deeper than 32 levels");
     if (t->shadow_walk > 1) return fail(c, OXPT_E_INVALID, "shadow_walk is 0 or 1");
@@ -1224,8 +1387,9 @@ oxpt_status oxpt_ctx_memory(const oxpt_ctx* c, uint64_t out[4]) {
         scene = (uint64_t)c->geom_vec4 * 16 + (uint64_t)c->slot_count * 192 +
                 (uint64_t)c->side * c->side * c->layers * 8 + (uint64_t)c->bvh4_nodes * 128;
     }
+    scene += c->back.geom_cap + c->back.attrs_cap + c->back.atlas_cap + c->back.bvh4_cap;
     out[0] = scene;
-    out[1] = c->borrowed_tables ? 0 : (uint64_t)c->table_words * 4;
+    out[1] = (c->borrowed_tables ? 0 : (uint64_t)c->table_words * 4) + c->back.tables_cap;
     uint64_t px = (uint64_t)c->w * c->h;
     out[2] = c->accum ? px * 16 + (c->img8 ? px * 4 : 0) + (c->img32 ? px * 16 : 0) : 0;
     out[3] = c->out_cap * 16 + c->wave_bytes + c->batch_cap * sizeof(oxd::BatchFrame);
@@ -1528,6 +1692,8 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         in[k] = {c->w, fr[k].first, fr[k].count, fr[k].y0, fr[k].rows};
         if (fr[k].count == 0 || fr[k].rows == 0) continue;
         if (c->device != e->device) return fail(e, OXPT_E_INVALID, at + "context on another device");
+        if (c != e && (c->staged || c->back_free_valid))
+            return fail(e, OXPT_E_INVALID, at + "a context that stages scenes is traced by its own refine");
         if ((s = ready(c))) return fail(e, s, at + c->err);
         if (fr[k].y0 >= c->h || fr[k].rows > c->h - fr[k].y0) return fail(e, OXPT_E_INVALID, at + "rows outside the image");
         uint64_t o0 = c->params.offs0[0], o1 = c->params.offs0[1];
@@ -1611,6 +1777,23 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         args.push_back(wa);
     }
     oxd::WaveArgs base{};
+    {
+        // One scene for every frame (a single tracer's refine, or views of
+        // one resident scene): the traversal kernels may stage its nodes.
+        const oxpt_ctx* s0 = nullptr;
+        bool one = true;
+        for (uint32_t k = 0; k < n && one; k++) {
+            const oxpt_ctx* c = fr[k].ctx;
+            if (!fr[k].count || !fr[k].rows) continue;
+            if (!s0) s0 = c;
+            else one = c->geom == s0->geom && c->geom_vec4 == s0->geom_vec4 &&
+                       c->params.env[3] == s0->params.env[3];
+        }
+        if (s0 && one) {
+            base.s = scene_view(s0);
+            base.one_scene = 1u;
+        }
+    }
     if ((s = ensure_wave(e, pmax, J, &base.st, &base.q, &base.ctr, &base.work))) {
         e->mode = saved_mode;
         return s;
@@ -1624,6 +1807,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.vcap = pmax;
         wa.jobs = J;
         wa.refill = e->refill;
+        wa.walk_lim = e->walk_lim;
         wa.total = total;
         wa.out = e->out;
         wa.counters = nullptr;

@@ -30,19 +30,44 @@ constexpr int MAX_DEVICES = 64;
 struct DeviceSetup {
     bool ready = false;
     float4* scratch = nullptr;  // device address of g_noalloc_scratch
+    void* context = nullptr;    // the CUDA context the address belongs to
     int sms = 0;
     int blocks_per_sm = 0;
 };
 DeviceSetup g_setup[MAX_DEVICES];
 std::mutex g_setup_lock;
 
+// The calling thread's current CUDA context (driver cuCtxGetCurrent, reached
+// through the runtime's entry-point query so the library need not link the
+// driver library), or null when it cannot be asked.
+void* current_context() {
+    typedef int (*GetCurrent)(void**);
+    static GetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        (void)cudaGetLastError();
+        return (GetCurrent)p;
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
 // Device addresses of the scratch array, looked up once per device with
 // that device current. In host code `g_noalloc_scratch` names a host-side
 // shadow, not device memory, so kernels only ever get the looked-up address.
+// A device reset (cudaDeviceReset, or a reset of the primary context) loads
+// the module again, possibly elsewhere: the lookup is redone whenever the
+// current context is no longer the one the address was taken in.
 oxpt_status setup_device(int dev, DeviceSetup** out) {
     if (dev < 0 || dev >= MAX_DEVICES) return OXPT_E_NODEV;
     std::lock_guard<std::mutex> lock(g_setup_lock);
     DeviceSetup& d = g_setup[dev];
+    void* ctx = current_context();
+    if (d.ready && ctx && ctx != d.context) d.ready = false;
     if (!d.ready) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
@@ -55,6 +80,7 @@ oxpt_status setup_device(int dev, DeviceSetup** out) {
             return OXPT_E_CUDA;
         }
         d.scratch = (float4*)p;
+        d.context = current_context();  // made current by the lookup above
         d.sms = sms;
         d.blocks_per_sm = oxd::trace_blocks_per_sm(oxd::TRACE_THREADS, false);
         if (d.blocks_per_sm <= 0) d.blocks_per_sm = 1;
@@ -75,11 +101,12 @@ extern "C" oxpt_status oxpt_dispatch_noalloc(const oxpt_device_scene* scene, con
     if (!scene->atlas || scene->atlas_side == 0 || scene->atlas_layers == 0) return OXPT_E_INVALID;
     const uint32_t w = params->dims[0], h = params->dims[1];
     if (w == 0 || h == 0) return OXPT_E_INVALID;
+    // An empty frame is a no-op wherever it lies, as for oxpt_dispatch.
+    if (frame->count == 0 || frame->rows == 0) return OXPT_OK;
     if (frame->y0 >= h || frame->rows > h - frame->y0) return OXPT_E_INVALID;
     if (frame->count > 0xffffffffu - frame->first) return OXPT_E_INVALID;
     // The unit of work per launch is whole rows: one row must fit.
     if (w > NOALLOC_MAX_PATHS) return OXPT_E_LIMIT;
-    if (frame->count == 0 || frame->rows == 0) return OXPT_OK;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         (void)cudaGetLastError();

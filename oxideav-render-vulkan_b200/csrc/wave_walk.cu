@@ -1,0 +1,234 @@
+// Traversal kernels of the wavefront plans with on-chip walk storage
+// (walk.cuh): short per-lane stacks in shared memory, the binary tree's top
+// levels staged in shared memory, alpha tests out of line. Persistent grids
+// over the ray queues with the lane refill of wave_extend / wave_shadow
+// (wavefront.cu), and the same per-ray steps, so every result, counter and
+// error bit equals theirs. Chosen by trace_variant 3-5 (occupancy targets
+// of 8, 10 and 12 resident blocks per SM).
+#include "kernels.cuh"
+#include "walk.cuh"
+#include "wavefront.cuh"
+
+namespace oxd {
+
+namespace {
+
+constexpr uint32_t NT = WAVE_TRAVERSE_THREADS;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int STEPS = 4;        // walk steps between refill checks
+constexpr int SS2 = 8;          // binary walk: stack entries per lane in shared memory
+constexpr int SS4 = 16;         // four-wide walk: stack entries per lane in shared memory
+constexpr uint32_t STACK2_BYTES = 3u * SS2 * NT * 4u;
+constexpr uint32_t STACK4_BYTES = SS4 * NT * 4u;
+constexpr uint32_t SM_SHARED = 228u * 1024u;  // shared memory per SM (sm_100)
+constexpr uint32_t CTA_RESERVED = 1024u;      // per resident CTA, reserved by the runtime
+
+extern __shared__ __align__(16) uint32_t walk_smem[];
+
+// Copies the first `staged` float4 words of the scene's geom (top nodes)
+// into shared memory after the stack columns.
+__device__ __forceinline__ WalkShared stage_nodes(const Scene& s, uint32_t stack_bytes, uint32_t staged,
+                                                  uint32_t lim) {
+    WalkShared sh;
+    sh.words = walk_smem;
+    sh.lim = lim;
+    float4* nodes = reinterpret_cast<float4*>(reinterpret_cast<char*>(walk_smem) + stack_bytes);
+    for (uint32_t i = threadIdx.x; i < staged; i += NT) nodes[i] = geomv(s, i);
+    __syncthreads();
+    sh.nodes = nodes;
+    sh.staged = staged;
+    return sh;
+}
+
+template <bool COUNT, int MINB, int SD, bool BATCH>
+__global__ void __launch_bounds__(NT, MINB) walk_extend(const __grid_constant__ WaveArgs a, uint32_t staged, uint32_t lim) {
+    Cnt cnt;
+    if (COUNT)
+        for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
+    const WalkShared sh = stage_nodes(a.s, STACK2_BYTES, staged, lim < SS2 ? lim : SS2);
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
+    bool active = false, warp_drained = false;
+    uint32_t i = 0u, k = 0u, path_seed = 0u;
+    const Scene* sc = &a.s;
+    Ray r;
+    Walk2S<SS2, SD> w;
+    for (;;) {
+        const unsigned act = __ballot_sync(FULL, active);
+        if (act == 0u && warp_drained) break;
+        if (!warp_drained && 32 - __popc(act) >= (act ? a.refill : 1u)) {
+            bool none_left = false;
+            if (!active) {
+                uint32_t q = append(&a.ctr[5]);
+                if (q < n) {
+                    i = a.q.ext[q];
+                    if (BATCH) sc = &a.frames[a.st.frame[i]].s;
+                    float4 o = a.st.org[i], d = a.st.dir[i];
+                    uint4 sd = a.st.seed[i];
+                    path_seed = sd.z;
+                    k = sd.w;
+                    bump<COUNT>(cnt, C_PATH_RAYS);
+                    r = make_ray(xyz(o), xyz(d));
+                    if (walk2s_begin<COUNT, SS2, SD>(*sc, sh, r, INF, w, cnt)) active = true;
+                    else a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+                } else {
+                    none_left = true;
+                }
+            }
+            warp_drained = __any_sync(FULL, none_left);
+        }
+#pragma unroll 1
+        for (int st = 0; st < STEPS && active; st++) {
+            if (walk2s_step<COUNT, SS2, SD, NT>(sc, sh, r, path_seed, k << 16u, k == 0u, false, NONE, w, cnt,
+                                                a.err)) {
+                active = false;
+                if (w.hit_any) {
+                    const Hit& h = w.best;
+                    a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(h.b.y),
+                                             __float_as_uint(h.b.z));
+                    a.st.hmeta[i] = w.best_mat | (h.front ? 0x80000000u : 0u);
+                } else {
+                    a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+                }
+            }
+        }
+    }
+    if (COUNT)
+        for (int c = 0; c < C_N; c++)
+            if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
+}
+
+template <int SD, bool FOUR>
+struct ShadowState {
+    Walk2S<SS2, SD> w;
+};
+template <int SD>
+struct ShadowState<SD, true> {
+    Walk4S<SS4, SD> w;
+};
+
+template <bool COUNT, int MINB, int SD, bool FOUR, bool BATCH>
+__global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ WaveArgs a, uint32_t staged, uint32_t lim) {
+    Cnt cnt;
+    if (COUNT)
+        for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
+    const uint32_t cap = FOUR ? (uint32_t)SS4 : (uint32_t)SS2;
+    const WalkShared sh = stage_nodes(a.s, FOUR ? STACK4_BYTES : STACK2_BYTES, FOUR ? 0u : staged,
+                                      lim < cap ? lim : cap);
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[1]);
+    bool active = false, warp_drained = false;
+    uint32_t slot = 0u, job = 0u, rid = 0u, skip = NONE, path_seed = 0u;
+    const Scene* sc = &a.s;
+    Ray r;
+    ShadowState<SD, FOUR> ss;
+    for (;;) {
+        const unsigned act = __ballot_sync(FULL, active);
+        if (act == 0u && warp_drained) break;
+        if (!warp_drained && 32 - __popc(act) >= (act ? a.refill : 1u)) {
+            bool none_left = false;
+            if (!active) {
+                uint32_t q = append(&a.ctr[6]);
+                if (q < n) {
+                    float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
+                    uint4 m = a.q.sh_m[q];
+                    slot = m.x;
+                    job = m.y;
+                    rid = m.z;
+                    path_seed = m.w;
+                    skip = __float_as_uint(d.w);
+                    if (BATCH) sc = &a.frames[a.st.frame[slot]].s;
+                    bump<COUNT>(cnt, C_SHADOW_RAYS);
+                    r = make_ray(xyz(o), xyz(d));
+                    bool started;
+                    if constexpr (FOUR) started = walk4s_begin<SS4, SD>(*sc, r, o.w, ss.w);
+                    else started = walk2s_begin<COUNT, SS2, SD>(*sc, sh, r, o.w, ss.w, cnt);
+                    if (started) active = true;
+                    else a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;  // nothing in the way
+                } else {
+                    none_left = true;
+                }
+            }
+            warp_drained = __any_sync(FULL, none_left);
+        }
+#pragma unroll 1
+        for (int st = 0; st < STEPS && active; st++) {
+            bool done;
+            if constexpr (FOUR)
+                done = walk4s_step<COUNT, SS4, SD, NT>(sc, walk_smem, sh.lim, r, path_seed, rid, false, skip,
+                                                      ss.w, cnt, a.err);
+            else
+                done = walk2s_step<COUNT, SS2, SD, NT>(sc, sh, r, path_seed, rid, false, true, skip, ss.w, cnt,
+                                                       a.err);
+            if (done) {
+                active = false;
+                if (!ss.w.hit_any) a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;
+            }
+        }
+    }
+    if (COUNT)
+        for (int c = 0; c < C_N; c++)
+            if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
+}
+
+template <bool C, int SD, bool B>
+void* ext_fn(int v) {
+    if (v == 0) return (void*)walk_extend<C, 8, SD, B>;
+    if (v == 1) return (void*)walk_extend<C, 10, SD, B>;
+    return (void*)walk_extend<C, 12, SD, B>;
+}
+
+template <bool C, int SD, bool FOUR, bool B>
+void* shadow_fn(int v) {
+    if (v == 0) return (void*)walk_shadow<C, 8, SD, FOUR, B>;
+    if (v == 1) return (void*)walk_shadow<C, 10, SD, FOUR, B>;
+    return (void*)walk_shadow<C, 12, SD, FOUR, B>;
+}
+
+template <bool C, bool B>
+void* kernel_c(bool ext, bool four, int v, int sd) {
+    if (ext) return sd <= 32 ? ext_fn<C, 32, B>(v) : ext_fn<C, 64, B>(v);
+    if (four) return sd <= 32 ? shadow_fn<C, 32, true, B>(v) : shadow_fn<C, 64, true, B>(v);
+    return sd <= 32 ? shadow_fn<C, 32, false, B>(v) : shadow_fn<C, 64, false, B>(v);
+}
+
+void* kernel_of(bool count, bool batch, bool ext, bool four, int v, int sd) {
+    if (batch) return count ? nullptr : kernel_c<false, true>(ext, four, v, sd);
+    return count ? kernel_c<true, false>(ext, four, v, sd) : kernel_c<false, false>(ext, four, v, sd);
+}
+
+const int TARGET_BLOCKS[3] = {8, 10, 12};
+
+}  // namespace
+
+// variant 0..2: 8 / 10 / 12 resident blocks per SM targeted. The shared
+// memory each block gets is what that many blocks leave per block; after
+// the stack columns, the rest holds the binary tree's top nodes (binary
+// walks of launches over one scene only: a plain launch, or a batch whose
+// frames all trace the same node words).
+cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
+                        cudaStream_t st) {
+    variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
+    void* fn = kernel_of(count, a.nframes > 0, ext, four, variant, sd);
+    if (!fn) return cudaErrorInvalidValue;
+    const uint32_t target = (uint32_t)TARGET_BLOCKS[variant];
+    const uint32_t stack_bytes = (ext || !four) ? STACK2_BYTES : STACK4_BYTES;
+    uint32_t per_block = SM_SHARED / target - CTA_RESERVED;
+    if (per_block > 48u * 1024u) per_block = 48u * 1024u;
+    uint32_t staged = 0u;  // float4 words of staged top nodes
+    if ((ext || !four) && (a.nframes == 0 || a.one_scene) && per_block > stack_bytes) {
+        uint64_t nodes = (per_block - stack_bytes) / 32u;
+        if (nodes > a.s.P.env[3]) nodes = a.s.P.env[3];
+        if (2 * nodes > a.s.geom_vec4) nodes = a.s.geom_vec4 / 2;
+        staged = (uint32_t)(2 * nodes);
+    }
+    const uint32_t smem = stack_bytes + staged * 16u;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem);
+    if (e != cudaSuccess) return e;
+    unsigned blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+    WaveArgs copy = a;
+    uint32_t lim = a.walk_lim;
+    void* args[] = {&copy, &staged, &lim};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(NT), args, smem, st);
+}
+
+}  // namespace oxd

@@ -35,20 +35,6 @@ namespace oxd {
 
 enum : uint32_t { ST_EMPTY = 0, ST_TRACING = 1, ST_ENDING = 2 };
 
-// Warp-aggregated append: one atomic per converged group.
-__device__ __forceinline__ uint32_t append(uint32_t* ctr) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(ctr, g.size());
-    return g.shfl(base, 0) + g.thread_rank();
-}
-__device__ __forceinline__ unsigned long long fetch_item(unsigned long long* ctr) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    unsigned long long base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(ctr, (unsigned long long)g.size());
-    return g.shfl(base, 0) + g.thread_rank();
-}
-
 __device__ __forceinline__ void load_core(const WaveArgs& a, uint32_t i, PathCore* pc, Sampler* smp, uint32_t* flags) {
     uint4 sd = a.st.seed[i];
     float4 b = a.st.beta[i], r = a.st.rad[i], d = a.st.dir[i], pp = a.st.prev[i], sg = a.st.sigma[i];
@@ -453,11 +439,13 @@ cudaError_t launch_wave_continue(cudaGraphConditionalHandle h, uint32_t* ctr, ui
 }
 
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
+    if (variant >= 3) return launch_walk(a, count, true, false, variant - 3, stack, sms, st);
     return launch_trav(a, count, true, false, variant, stack, sms, st);
 }
 
 cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, bool four, int variant, int stack, int sms,
                                cudaStream_t st) {
+    if (variant >= 3) return launch_walk(a, count, false, four, variant - 3, stack, sms, st);
     return launch_trav(a, count, false, four, variant, stack, sms, st);
 }
 

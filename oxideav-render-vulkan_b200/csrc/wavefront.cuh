@@ -1,12 +1,29 @@
 // Wavefront path-state layout and launch entry points (see wavefront.cu).
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "device.cuh"
 
 namespace oxd {
+
+// Warp-aggregated append: one atomic per converged group.
+__device__ __forceinline__ uint32_t append(uint32_t* ctr) {
+    namespace cg = cooperative_groups;
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+__device__ __forceinline__ unsigned long long fetch_item(unsigned long long* ctr) {
+    namespace cg = cooperative_groups;
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, (unsigned long long)g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
 
 constexpr uint32_t WAVE_TRAVERSE_THREADS = 128;
 
@@ -106,10 +123,19 @@ struct WaveArgs {
     const BatchFrame* frames;
     uint32_t nframes;
     NrcWave nrc;
+    // traversal variants 3-5: walk-stack entries per lane kept in shared
+    // memory (capped by the kernel's columns; deeper ones in local memory)
+    uint32_t walk_lim = 0xffffffffu;
+    // batched launches whose frames all trace one scene (the same node
+    // words): `s` is then that scene, for the traversal kernels' staged
+    // top nodes
+    uint32_t one_scene = 0u;
 };
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3
-// / 4 blocks per SM; traversal 6 / 8 / 10); `stack`: 32 or 64 entries.
+// / 4 blocks per SM; traversal 6 / 8 / 10); traversal variants 3..5 run the
+// on-chip-stack kernels of wave_walk.cu (8 / 10 / 12 blocks per SM);
+// `stack`: 32 or 64 entries.
 // With a.nframes > 0 the batched kernels run (count must then be false).
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st);
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st);
@@ -117,6 +143,11 @@ cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int s
 // binary one; stack: 32 or 64 entries, enough for the tree walked.
 cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, bool four, int variant, int stack, int sms,
                                cudaStream_t st);
+// wave_walk.cu: traversal with shared-memory short stacks and staged top
+// nodes; ext = closest hit of the continuation queue, else the shadow queue
+// (four: the four-wide tree); variant 0..2 targets 8 / 10 / 12 blocks per SM.
+cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
+                        cudaStream_t st);
 // Graph-resident loop: after an iteration, sets the enclosing while node's
 // condition to "slots still active and fewer than `cap` iterations"; on
 // reaching the bound it sets bit 3 of *err instead. tally[0] += kernels

@@ -61,6 +61,15 @@ class _CudaArray:
                                          "version": 3, "strides": None}
 
 
+def accumulator_tensor(tracer, device: int):
+    """The tracer's device accumulator as an (h, w, 4) float32 torch tensor
+    (zero copy, read-write)."""
+    import torch
+    d = N.DevImage()
+    tracer._check(N.lib().oxpt_accum_view(tracer.ctx, C.byref(d)))
+    return torch.as_tensor(_CudaArray(d.data, (d.height, d.width, 4), "<f4"), device=f"cuda:{device}")
+
+
 class ShardedPathTracer:
     """GpuPathTracer over the GPUs of a torch.distributed (NCCL) group: each
     rank refines its row tile; image() / hdr() first all-gather the
@@ -90,10 +99,7 @@ class ShardedPathTracer:
         return self.pt.samples()
 
     def accumulator(self):
-        import torch
-        d = N.DevImage()
-        self.pt._check(N.lib().oxpt_accum_view(self.pt.ctx, C.byref(d)))
-        return torch.as_tensor(_CudaArray(d.data, (d.height, d.width, 4), "<f4"), device=f"cuda:{self.device}")
+        return accumulator_tensor(self.pt, self.device)
 
     def gather(self):
         import torch

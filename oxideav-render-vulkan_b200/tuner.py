@@ -45,7 +45,7 @@ class Plan:
 SPACE = {
     "mode": [N.MODE_WAVEFRONT, N.MODE_WAVEFRONT_SPLIT, N.MODE_MEGAKERNEL],
     "shade_variant": [0, 1, 2],
-    "trace_variant": [0, 1, 2],
+    "trace_variant": [0, 1, 2, 3, 4, 5],
     "stack": [0, 64],
     "wave_slots": [1 << 19, 1 << 20, 1 << 21, 1 << 22],
     "nee_variant": [0, 1, 2, 3, 4, 5],
@@ -53,6 +53,14 @@ SPACE = {
     "refill": [1, 8, 16, 32],
     "graphs": [0, 1],
 }
+# The plan of the single-large-scene workload (1,048,820 triangles, 1920x1080,
+# 64 spp, 12 bounces): the tuner's pick on that scene. The benchmark runs it
+# by default and the GPU parity test of that workload runs exactly it, so
+# the measured plan is the tested plan.
+LARGE_SCENE_PLAN = Plan(mode=N.MODE_WAVEFRONT_SPLIT, shade_variant=0, trace_variant=0, stack=64,
+                        wave_slots=1 << 22, nee_variant=3, shadow_walk=0, graphs=1, refill=16)
+LARGE_SCENE_WAVE_ITEMS = 1 << 27  # paths per launch round: a whole frame
+
 WAVE_ONLY = ("shade_variant", "trace_variant", "stack", "wave_slots", "nee_variant", "shadow_walk", "graphs",
              "refill")
 SPLIT_ONLY = ("nee_variant",)

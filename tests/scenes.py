@@ -89,11 +89,14 @@ def materials_scene(pkg):
     return s
 
 
-def textured_scene(pkg, min_filter=5, wrap=(2, 2)):
+def textured_scene(pkg, min_filter=5, wrap=(2, 2), mag_linear=True, tex_size=256):
     """Checker-textured floor seen at a grazing angle (ray-cone LOD,
-    trilinear filtering) plus a textured, tangent-mapped sphere."""
+    trilinear filtering) plus a textured, tangent-mapped sphere. A small
+    `tex_size` makes texels larger than pixels near the camera, so camera
+    hits there take the magnification filter (LOD <= 0)."""
     s = pkg.Scene()
-    t0 = s.add_texture(checker(256, 16), srgb_encoded=True, wrap=wrap, min_filter=min_filter)
+    t0 = s.add_texture(checker(tex_size, max(2, tex_size // 16)), srgb_encoded=True, wrap=wrap,
+                       mag_linear=mag_linear, min_filter=min_filter)
     nm = np.zeros((64, 64, 4), np.float32)
     yy, xx = np.mgrid[0:64, 0:64]
     nm[..., 0] = 0.5 + 0.3 * np.sin(xx / 4.0)

@@ -1,0 +1,113 @@
+"""GPU parity on the benchmarked configuration itself.
+
+The single large scene at full size (a 1,048,820-triangle displaced
+icosphere, 64 materials, 8 x 2048^2 RGBA16F textures with mips, 16
+punctual lights, 512 emissive triangles, a 1024x512 sky with a sun disk),
+1920x1080, 64 spp, 12 bounces, traced with the plan the benchmark runs
+(tuner.LARGE_SCENE_PLAN: split wavefront, 2^22 paths in flight,
+vertex-major NEE, four-wide shadow walk, refill 16, one CUDA graph per
+step, a whole frame per launch round):
+
+* three 3-row bands (top, middle, bottom) of the 64-spp frame equal the
+  oracle's dispatch of the same rows and samples bit for bit
+  (pathtrace.wgsl:1697-2073 is the estimator matched);
+* on the same 1.22 M-node tree, closest-hit ids of 10^6 random rays equal
+  the oracle's except ties within 1e-6 relative t, and any-hit occlusion
+  (binary and four-wide walks) is identical (pathtrace.wgsl:651-735).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+W, H, SPP = 1920, 1080, 64
+
+
+@pytest.fixture(scope="module")
+def large(pkg):
+    from oxideav_render_vulkan_b200 import tuner
+    scene = pkg.Scene.icosphere(freq=229, seed=1, n_materials=64, n_textures=8, tex_size=2048, n_punctual=16,
+                                n_emissive=512, material_mix=0)
+    env = pkg.EnvironmentMap.sky(1024, 512, sun_dir=(0.3, 0.8, -0.5), sun_radiance=2000.0)
+    opts = pkg.RenderOptions(width=W, height=H, scene_camera=0,
+                             path_trace=pkg.PathTraceOptions(samples_per_pixel=SPP, max_bounces=12, rr_start=3,
+                                                             seed=0))
+    t = pkg.GpuPathTracer(0)
+    t.set_environment(env)
+    assert t.sync(scene, opts)
+    tuner.apply(t, tuner.LARGE_SCENE_PLAN)
+    t.set_tuning(wave_items=tuner.LARGE_SCENE_WAVE_ITEMS)
+    p = t.prepared()
+    assert scene.triangle_count() == 1_048_820
+    yield t, p
+    del t
+
+
+def test_plan_is_the_benchmarked_plan(pkg, large):
+    from oxideav_render_vulkan_b200 import tuner
+    t, _ = large
+    got = t.tuning()
+    want = tuner.LARGE_SCENE_PLAN
+    assert (got.mode, got.wave_slots, got.nee_variant, got.shadow_walk, got.refill, got.graphs) == \
+        (want.mode, want.wave_slots, want.nee_variant, want.shadow_walk, want.refill, want.graphs)
+    assert got.wave_items == tuner.LARGE_SCENE_WAVE_ITEMS
+
+
+def test_large_scene_64spp_row_bands_bit_exact(pkg, oracle, large):
+    t, p = large
+    t.reset()
+    t.refine(SPP)
+    t.finish()
+    gpu = t.read_accum()
+    assert np.isfinite(gpu).all()
+    cov = gpu[..., 3]
+    assert cov.min() >= 0 and cov.max() <= SPP and (cov == SPP).mean() > 0.2
+    cpu = np.zeros_like(gpu)
+    for y0 in (0, 538, 1077):
+        oracle.dispatch(p, p.params, (0, SPP, y0, 3), cpu)
+        band_gpu, band_cpu = gpu[y0:y0 + 3], cpu[y0:y0 + 3]
+        diff = band_gpu.view(np.uint32) != band_cpu.view(np.uint32)
+        assert not diff.any(), f"rows {y0}..{y0 + 2}: {np.count_nonzero(diff.any(axis=2))} pixels differ"
+        assert band_cpu[..., 3].sum() > 0
+
+
+def test_large_scene_million_rays(pkg, oracle, large):
+    import ctypes as C
+    t, p = large
+    rng = np.random.default_rng(21)
+    n = 1_000_000
+    o = rng.uniform(-1.4, 1.4, (n, 3)).astype(np.float32)
+    d = rng.standard_normal((n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 3] = 3.0e38
+    rays[:, 3][: n // 4] = rng.uniform(0.0, 3.0, n // 4).astype(np.float32)
+    rays[:, 4:7] = d
+    rays[:, 7] = np.frombuffer(np.full(n, 0xFFFFFFFF, np.uint32).tobytes(), np.float32)
+    L = pkg._native.lib()
+    info = (C.c_uint32 * 4)()
+    assert L.oxpt_diag_bvh4(t.ctx, info) == 0 and info[0] == 1
+    for flags in (0, 1, 5):  # closest hit; any hit binary; any hit four-wide
+        slot = np.empty(n, np.uint32)
+        gid = np.empty(n, np.uint32)
+        tt = np.empty(n, np.float32)
+        bary = np.empty((n, 3), np.float32)
+        st = L.oxpt_diag_trace_rays(t.ctx, n, rays.ctypes.data, flags, slot.ctypes.data, gid.ctypes.data,
+                                    tt.ctypes.data, bary.ctypes.data)
+        assert st == 0
+        oslot, ogid, ot, obary, _ = oracle.trace_rays(p, rays, flags & 3)
+        if flags & 1:
+            assert np.array_equal(slot == 0xFFFFFFFF, oslot == 0xFFFFFFFF)
+            continue
+        hit = ogid != 0xFFFFFFFF
+        assert hit.sum() > n // 4
+        diff = gid != ogid
+        if diff.any():
+            rel = np.abs(tt[diff] - ot[diff]) / np.maximum(np.abs(ot[diff]), 1e-30)
+            assert np.all(rel <= 1e-6), f"{diff.sum()} ids differ beyond ties"
+        same = ~diff
+        assert np.array_equal(tt[same].view(np.uint32), ot[same].view(np.uint32))
+        assert np.array_equal(bary[same].view(np.uint32), obary[same].view(np.uint32))

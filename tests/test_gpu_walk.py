@@ -1,0 +1,116 @@
+"""The shared-memory short-stack traversal kernels (trace_variant 3-5)
+against the oracle and against the local-memory kernels.
+
+Same walks, storage moved on chip (walk stacks in shared-memory columns,
+top nodes staged, alpha tests out of line), so:
+* accumulators equal the oracle's bit for bit under every occupancy
+  target, both execution plans, binary and four-wide shadow walks, and
+  with the shared part of the stack cut to 0, 1 or 3 entries (entries
+  spill to local memory much earlier: that path is exercised too);
+* the traversal counters (boxes, leaves, triangles, pops) equal the
+  oracle's for the binary walk and the local-memory kernels' for the
+  four-wide walk;
+* batched launches (one executor over several scenes, no node staging)
+  equal each scene's own refine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(pkg, which):
+    if which == "materials":
+        return scenes.materials_scene(pkg), None
+    if which == "alpha":
+        return scenes.alpha_scene(pkg), None
+    if which == "textured":
+        return scenes.textured_scene(pkg), None
+    scene = pkg.Scene.icosphere(freq=16, seed=2, n_materials=12, n_textures=3, tex_size=64, n_punctual=3,
+                                n_emissive=16, material_mix=1)
+    return scene, pkg.EnvironmentMap.sky(64, 32)
+
+
+def _tracer(pkg, scene, env, w=40, h=28, spp=6, bounces=10):
+    t = pkg.GpuPathTracer(0)
+    if env is not None:
+        t.set_environment(env)
+    assert t.sync(scene, pkg.RenderOptions(width=w, height=h, path_trace=pkg.PathTraceOptions(
+        samples_per_pixel=spp, max_bounces=bounces)))
+    return t
+
+
+@pytest.mark.parametrize("walk", [0, 1])
+@pytest.mark.parametrize("variant", [3, 4, 5])
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("which", ["materials", "alpha", "layered", "textured"])
+def test_short_stack_kernels_bit_exact(pkg, oracle, which, mode, variant, walk):
+    scene, env = _scene(pkg, which)
+    t = _tracer(pkg, scene, env)
+    t.set_tuning(mode=mode, trace_variant=variant, shadow_walk=walk, wave_slots=333, wave_items=2000, refill=8)
+    t.refine(6)
+    cpu, _ = oracle.render(t.prepared(), 6)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
+
+
+@pytest.mark.parametrize("lim", [0, 1, 3])
+@pytest.mark.parametrize("walk", [0, 1])
+def test_stack_entries_in_local_memory_bit_exact(pkg, oracle, lim, walk):
+    """Fewer shared entries push the walk onto its local-memory part."""
+    scene = pkg.Scene.icosphere(freq=48, seed=5, n_materials=8, n_textures=2, tex_size=64, n_punctual=4,
+                                n_emissive=32, material_mix=1)
+    env = pkg.EnvironmentMap.sky(64, 32)
+    t = _tracer(pkg, scene, env, w=48, h=32, spp=4, bounces=8)
+    t.set_tuning(mode=2, trace_variant=4, shadow_walk=walk)
+    assert pkg._native.lib().oxpt_diag_set_walk_shared(t.ctx, lim) == 0
+    t.refine(4)
+    cpu, _ = oracle.render(t.prepared(), 4)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
+
+
+@pytest.mark.parametrize("variant", [3, 5])
+@pytest.mark.parametrize("mode", [1, 2])
+def test_short_stack_counters_match(pkg, oracle, mode, variant):
+    L = pkg._native.lib()
+    scene, _ = _scene(pkg, "materials")
+    opts = pkg.RenderOptions(width=48, height=32, path_trace=pkg.PathTraceOptions(samples_per_pixel=4))
+    runs = {}
+    for tv, walk in ((variant, 1), (variant, 0), (0, 0)):
+        t = pkg.GpuPathTracer(0)
+        assert t.sync(scene, opts)
+        t.set_tuning(mode=mode, trace_variant=tv, shadow_walk=walk)
+        p = t.prepared()
+        out = (C.c_uint64 * 8)()
+        assert L.oxpt_diag_refine_counted(t.ctx, 0, 4, out) == 0
+        split = (C.c_uint64 * 16)()
+        assert L.oxpt_diag_counters_split(t.ctx, split) == 0
+        runs[(tv, walk)] = (list(out), list(split), t.read_accum())
+    cpu, cnt = oracle.render(p, 4)
+    assert runs[(variant, 1)][0] == [int(c) for c in cnt]  # binary walk: the reference's counters
+    assert runs[(variant, 0)][1] == runs[(0, 0)][1]          # four-wide: the local-memory kernel's
+    for k, (_, _, acc) in runs.items():
+        assert np.array_equal(acc.view(np.uint32), cpu.view(np.uint32)), k
+
+
+def test_short_stack_batch_equals_each_refine(pkg):
+    items = [(scenes.materials_scene(pkg), None, 40, 28, 4), (scenes.alpha_scene(pkg), None, 33, 21, 6),
+             _scene(pkg, "layered") + (48, 32, 5)]
+    tracers, want = [], []
+    for scene, env, w, h, spp in items:
+        alone = _tracer(pkg, scene, env, w, h, spp)
+        alone.set_tuning(mode=2, trace_variant=0)
+        alone.refine(spp)
+        want.append(alone.read_accum())
+        t = _tracer(pkg, scene, env, w, h, spp)
+        tracers.append(t)
+    ex = pkg.GpuPathTracer(0)
+    ex.set_tuning(mode=2, trace_variant=4, wave_slots=500, graphs=1)
+    pkg.refine_batch(tracers, [it[4] for it in items], executor=ex)
+    for t, w_ in zip(tracers, want):
+        assert np.array_equal(t.read_accum().view(np.uint32), w_.view(np.uint32))

@@ -67,3 +67,29 @@ def test_create_reports_no_device_without_a_gpu(pkg):
         pass
     else:
         raise AssertionError("GpuPathTracer must fail loudly without a CUDA device")
+
+
+def test_host_only_library_prepares_without_cuda(pkg):
+    """liboxpt_host.so (scene building and preparation, no CUDA) prepares
+    the same buffers as liboxpt.so, and a process that selects it maps
+    neither liboxpt.so nor the CUDA runtime (the CPU reference arm)."""
+    import sys
+    import tempfile
+
+    import numpy as np
+    root = ROOT
+    code = (
+        "import sys, os, numpy as np; sys.path.insert(0, %r)\n"
+        "import __graft_entry__ as g\n"
+        "pkg = g.load_package(); pkg._native.select_host_only()\n"
+        "p = pkg.prepare(pkg.Scene.cornell(), pkg.RenderOptions(width=32, height=32))\n"
+        "np.save(sys.argv[1], p.geom)\n"
+        "m = open('/proc/%%d/maps' %% os.getpid()).read()\n"
+        "print('liboxpt.so' in m, 'liboxpt_host.so' in m, 'cudart' in m)\n" % str(root))
+    with tempfile.TemporaryDirectory() as d:
+        out = Path(d) / "geom.npy"
+        r = subprocess.run([sys.executable, "-c", code, str(out)], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        assert r.stdout.split() == ["False", "True", "False"]
+        want = pkg.prepare(pkg.Scene.cornell(), pkg.RenderOptions(width=32, height=32)).geom
+        assert np.array_equal(np.load(out), want)

@@ -23,13 +23,16 @@ import scenes
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_dispatch_matches_the_context_path_on_two_calls(pkg):
+@pytest.mark.parametrize("w,h", [(640, 480), (64, 32)])
+def test_noalloc_dispatch_matches_the_context_path_on_two_calls(pkg, w, h):
+    """640x480 (307,200 pixels) is more than the 2^18-path scratch per
+    sample, so each sample runs as several row launches; 64x32 puts several
+    consecutive samples into one launch."""
     import torch
 
     N = pkg._native
     L = N.lib()
     t = pkg.GpuPathTracer(0)
-    w, h = 640, 480  # 307,200 pixels: more than the 2^18-path scratch per sample
     opts = pkg.RenderOptions(width=w, height=h, path_trace=pkg.PathTraceOptions(samples_per_pixel=5))
     t.sync(scenes.materials_scene(pkg), opts)
     p = t.prepared()
@@ -70,3 +73,20 @@ def test_noalloc_rejects_rows_wider_than_its_scratch(pkg):
     st = L.oxpt_dispatch_noalloc(C.byref(scene), C.byref(params), C.byref(frame), C.c_void_p(C.addressof(one)),
                                  None)
     assert st == N.E_LIMIT
+
+
+def test_noalloc_empty_frame_is_a_no_op_anywhere(pkg):
+    """A frame with no rows or no samples returns OK even when its first row
+    lies outside the image, as oxpt_dispatch does (nothing is launched, so
+    the dummy host pointers are never read)."""
+    N = pkg._native
+    L = N.lib()
+    params = N.Params()
+    params.dims[0] = 16
+    params.dims[1] = 8
+    one = (C.c_uint32 * 64)()
+    scene = N.DeviceScene(C.addressof(one), 8, C.addressof(one), 48, C.addressof(one), 1, C.addressof(one), 1, 1)
+    for frame in (N.Frame(0, 1, 9, 0), N.Frame(0, 0, 9, 3)):
+        st = L.oxpt_dispatch_noalloc(C.byref(scene), C.byref(params), C.byref(frame),
+                                     C.c_void_p(C.addressof(one)), None)
+        assert st == N.OK
