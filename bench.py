@@ -81,6 +81,7 @@ def parse():
                     help="shadow rays' tree with --mode wave/split (auto: the library default, four-wide)")
     ap.add_argument("--requests", type=int, default=300, help="serve workload: requests in the stream")
     ap.add_argument("--rate", type=float, default=40.0, help="serve workload: Poisson arrival rate per second")
+    ap.add_argument("--repeats", type=int, default=1, help="serve workload: independent streams (seeds) to run")
     ap.add_argument("--spp-scale", type=int, default=16,
                     help="serve workload: spp targets {4..1024} divided by this (one GPU cannot keep up with the "
                          "full stream)")
@@ -632,42 +633,53 @@ def run_serve(a):
         o.refine(1)  # binds tables and params
         o.finish()
         owners.append(o)
-    reqs = serve_stream(serve, a, n_scenes)
-
     def options(r):
         return pkg.RenderOptions(width=r.width, height=r.height, scene_camera=0,
                                  path_trace=pkg.PathTraceOptions(samples_per_pixel=r.spp, max_bounces=8))
 
-    check = set(int(x) for x in np.random.default_rng(9).choice(a.requests, size=4, replace=False))
-    ex = serve.GpuExecutor(pkg, owners, options, keep=lambda o: o.rid in check)
-    ex.exe.set_tuning(mode=2, graphs=1)
-    if a.nee_variant >= 0:
-        ex.exe.set_tuning(nee_variant=a.nee_variant)
-    budget = 150 << 30
-    served = serve.Server(ex, budget, tick_paths=1 << 24).run(reqs)
-    ex2 = serve.GpuExecutor(pkg, owners, options)
-    serial = serve.run_serial(ex2, reqs)
-    by = {r.rid: r for r in reqs}
-    same = []
-    for rid, acc in ex.kept.items():
-        v = ex2.open(by[rid])
-        v.refine(by[rid].spp)
-        same.append(bool(np.array_equal(acc.view(np.uint32), v.read_accum().view(np.uint32))))
-    line = {"metric": "Msamples/s", "value": served.msamples_per_s(), "unit": "Msamples/s", "n_gpus": 1,
-            "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    runs = []
+    for rep in range(max(1, a.repeats)):
+        reqs = serve_stream(serve, a, n_scenes, seed=3 + rep)
+        check = set(int(x) for x in np.random.default_rng(9 + rep).choice(a.requests, size=8, replace=False))
+        ex = serve.GpuExecutor(pkg, owners, options, keep=lambda o: o.rid in check)
+        ex.exe.set_tuning(mode=2, graphs=1)
+        if a.nee_variant >= 0:
+            ex.exe.set_tuning(nee_variant=a.nee_variant)
+        budget = 150 << 30
+        served = serve.Server(ex, budget, tick_paths=1 << 24).run(reqs)
+        ex2 = serve.GpuExecutor(pkg, owners, options)
+        serial = serve.run_serial(ex2, reqs)
+        by = {r.rid: r for r in reqs}
+        same = []
+        for rid, acc in ex.kept.items():
+            v = ex2.open(by[rid])
+            v.refine(by[rid].spp)
+            same.append(bool(np.array_equal(acc.view(np.uint32), v.read_accum().view(np.uint32))))
+        runs.append({"stream_seed": 3 + rep, "msamples_per_s": served.msamples_per_s(),
+                     "p50_latency_s": served.percentile(50), "p99_latency_s": served.percentile(99),
+                     "completed": len(served.completed()), "superseded": sum(o.superseded for o in served.outcomes),
+                     "ticks": served.ticks, "peak_device_bytes_accounted": served.peak_bytes,
+                     "served_wall_s": served.wall,
+                     "serial_plain": {"msamples_per_s": serial.msamples_per_s(),
+                                      "p50_latency_s": serial.percentile(50), "p99_latency_s": serial.percentile(99),
+                                      "completed": len(serial.completed()), "wall_s": serial.wall},
+                     "throughput_vs_serial": served.msamples_per_s() / serial.msamples_per_s(),
+                     "same_alone_and_in_mix": same})
+        del ex, ex2
+    ratios = [r["throughput_vs_serial"] for r in runs]
+    mid = sorted(runs, key=lambda r: r["throughput_vs_serial"])[len(runs) // 2]
+    line = {"metric": "Msamples/s", "value": mid["msamples_per_s"], "unit": "Msamples/s", "n_gpus": 1,
+            "steps": len(runs), "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"served stream: {a.requests} requests, Poisson {a.rate}/s, {n_scenes} resident "
                                    "scenes (1e3..2e6 triangles log-uniform), resolutions 128^2..1920x1080, spp "
                                    f"targets {{4,16,64,256,1024}}/{a.spp_scale}, 30% camera moves, 150 GB budget",
-                       "triangles": tris},
-            "p50_latency_s": served.percentile(50), "p99_latency_s": served.percentile(99),
-            "completed": len(served.completed()), "superseded": sum(o.superseded for o in served.outcomes),
-            "ticks": served.ticks, "peak_device_bytes_accounted": served.peak_bytes,
-            "serial_plain": {"msamples_per_s": serial.msamples_per_s(), "p50_latency_s": serial.percentile(50),
-                             "p99_latency_s": serial.percentile(99), "completed": len(serial.completed()),
-                             "wall_s": serial.wall},
-            "served_wall_s": served.wall, "throughput_vs_serial": served.msamples_per_s() / serial.msamples_per_s(),
-            "same_alone_and_in_mix": same}
+                       "triangles": tris, "repeats": f"{len(runs)} streams (seeds 3..{2 + len(runs)}); value and "
+                                                    "latencies are the median-ratio run's"},
+            "p50_latency_s": mid["p50_latency_s"], "p99_latency_s": mid["p99_latency_s"],
+            "throughput_vs_serial": {"median": statistics.median(ratios), "min": min(ratios), "max": max(ratios)},
+            "same_alone_and_in_mix": all(all(r["same_alone_and_in_mix"]) for r in runs),
+            "runs": runs}
     print(json.dumps(line), flush=True)
 
 
@@ -1033,7 +1045,8 @@ def plan_of(pt):
     return {"mode": ["megakernel", "wavefront", "wavefront-split"][t.mode], "wave_slots": t.wave_slots,
             "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack,
             "nee_variant": t.nee_variant, "shadow_walk": ["four-wide", "binary"][t.shadow_walk],
-            "refill": t.refill, "graphs": t.graphs}
+            "refill": t.refill, "graphs": t.graphs,
+            "closest_walk": ["binary (exact)", "four-wide (tolerance plan)"][t.closest_walk]}
 
 
 class TileGather:

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OXPT_ABI_VERSION 1u
+#define OXPT_ABI_VERSION 2u
 
 typedef enum oxpt_status {
     OXPT_OK = 0,

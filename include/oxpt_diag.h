@@ -33,7 +33,9 @@ oxpt_status oxpt_diag_sobol(oxpt_ctx* ctx, const uint32_t* sobol_dirs, uint32_t 
  * (global triangle id bits, 0xffffffff = none). flags bit 0 = any-hit,
  * bit 1 = primary (back-face culling of single-sided materials), bit 2 =
  * any-hit rays walk the four-wide tree (OXPT_E_INVALID when none was
- * built; which occluder is reported may differ, occlusion may not).
+ * built; which occluder is reported may differ, occlusion may not), bit 3
+ * = closest-hit rays walk the four-wide tree (the tolerance plan's walk:
+ * the hit may differ only between candidates at nearly equal distance).
  * Outputs per ray: slot (0xffffffff = miss), global id, t, barycentrics
  * (3 floats). Any output pointer may be NULL.
  */
@@ -127,6 +129,16 @@ oxpt_status oxpt_diag_set_walk_shared(oxpt_ctx* ctx, uint32_t entries);
  *   refill         wavefront traversal: a warp gives its idle lanes new rays
  *                  once this many of its 32 lanes are idle (1 = as soon as
  *                  one is; 32 = when all are); 0 = library default (8).
+ *   closest_walk   0 = continuation rays take the reference's ordered
+ *                  binary walk (every plan above is then bit-identical);
+ *                  1 = the four-wide tree, nearest child first with entry
+ *                  distances on the stack (trace_variant 3-5 only; scenes
+ *                  without an exact four-wide tree keep the binary walk).
+ *                  The tolerance plan: a closest hit can differ from the
+ *                  binary walk's only between candidates within rounding of
+ *                  the same distance, so accumulators match the oracle to
+ *                  image tolerance (>= 60 dB PSNR), not bit for bit.
+ *   reserved       0.
  */
 enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1, OXPT_MODE_WAVEFRONT_SPLIT = 2 };
 typedef struct oxpt_tuning {
@@ -144,6 +156,8 @@ typedef struct oxpt_tuning {
     uint32_t shadow_walk;
     uint32_t graphs;
     uint32_t refill;
+    uint32_t closest_walk;
+    uint32_t reserved;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);

@@ -120,6 +120,7 @@ struct oxpt_ctx {
     bool bvh4_built = false;
     uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
     uint32_t shadow_walk = 0;
+    uint32_t closest_walk = 0;  // 1: continuation rays on the four-wide tree (tolerance plan)
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
     uint32_t walk_lim = 0xffffffffu;  // traversal variants 3-5: shared stack entries per lane (diagnostic)
     void* wave_mem = nullptr;
@@ -432,6 +433,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const ox
     wa.nframes = 0;
     wa.nrc = nrc ? *nrc : oxd::NrcWave{};
     wa.walk_lim = c->walk_lim;
+    wa.closest4 = (c->closest_walk && c->trace_variant >= 3 && bvh4_usable(c)) ? 1u : 0u;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
     bool four = c->shadow_walk == 0 && bvh4_usable(c);
@@ -476,7 +478,7 @@ int enqueue_iteration(oxpt_ctx* c, const oxd::WaveArgs& wa, const oxd::WaveArgs&
     } else {
         run(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, st); });
     }
-    run(3, [&] { return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, sd, c->sms, st); });
+    run(3, [&] { return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, wa.closest4 ? sd4 : sd, c->sms, st); });
     run(4, [&] {
         return oxd::launch_wave_shadow(wsh, count, four, (int)c->trace_variant, four ? sd4 : sd, c->sms, st);
     });
@@ -1194,7 +1196,7 @@ oxpt_status oxpt_diag_trace_rays(oxpt_ctx* c, size_t n, const float* rays, uint3
     if (!c || (n && !rays)) return fail(c, OXPT_E_INVALID, "null argument");
     if (oxpt_status sa = activate_staged(c)) return sa;
     if (!c->has_scene || !c->has_tables || !c->has_params) return fail(c, OXPT_E_INVALID, "scene, tables and params must be set first");
-    if ((flags & 4u) && !bvh4_usable(c)) return fail(c, OXPT_E_INVALID, "no four-wide tree for this scene");
+    if ((flags & 12u) && !bvh4_usable(c)) return fail(c, OXPT_E_INVALID, "no four-wide tree for this scene");
     if (n == 0) return OXPT_OK;
     oxpt_status s = set_device(c);
     if (s) return s;
@@ -1306,6 +1308,10 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     if (t->shadow_walk > 1) return fail(c, OXPT_E_INVALID, "shadow_walk is 0 or 1");
     if (t->graphs > 1) return fail(c, OXPT_E_INVALID, "graphs is 0 or 1");
     if (t->refill > 32) return fail(c, OXPT_E_INVALID, "refill is 0 (default) to 32");
+    if (t->closest_walk > 1) return fail(c, OXPT_E_INVALID, "closest_walk is 0 or 1");
+    if (t->closest_walk && t->trace_variant < 3)
+        return fail(c, OXPT_E_INVALID, "closest_walk 1 needs the short-stack traversal kernels (trace_variant 3-5)");
+    c->closest_walk = t->closest_walk;
     c->refill = t->refill ? t->refill : 8u;
     c->shadow_walk = t->shadow_walk;
     c->graphs = t->graphs;
@@ -1333,6 +1339,8 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->shadow_walk = c->shadow_walk;
     t->graphs = c->graphs;
     t->refill = c->refill;
+    t->closest_walk = c->closest_walk;
+    t->reserved = 0;
     return OXPT_OK;
 }
 
@@ -1555,6 +1563,13 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
                                  (uint64_t)(uintptr_t)e->out, (uint64_t)(uintptr_t)e->dev_err,
                                  (uint64_t)(uintptr_t)e->stream, args.empty() ? 0 : args[0].vcap,
                                  args.empty() ? 0 : args[0].jobs};
+    if (!args.empty()) {
+        // Launch parameters the captured kernels keep: the staged scene's
+        // node words (one-scene batches), the walk's storage split and tree.
+        const oxd::WaveArgs& a0 = args[0];
+        key.insert(key.end(), {(uint64_t)(uintptr_t)a0.s.geom, a0.s.geom_vec4, a0.s.P.env[3], a0.one_scene,
+                               a0.closest4, a0.walk_lim});
+    }
     for (size_t k = 0; k < rounds.size(); k++) {
         const oxd::WaveArgs& wa = args[k];
         key.insert(key.end(), {wa.slots, wa.total, (uint64_t)(uintptr_t)wa.frames, wa.nframes,
@@ -1742,7 +1757,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
             J = std::max(J, c->params.cfg[2] + 1u);
             max_bounces = std::max(max_bounces, c->params.dims[3]);
             if (c->bvh_depth > 32) sd = 64;
-            if (e->shadow_walk == 0 && bvh4_usable(c) && c->bvh4_need > 32) sd = 64;
+            if ((e->shadow_walk == 0 || e->closest_walk) && bvh4_usable(c) && c->bvh4_need > 32) sd = 64;
         }
     // Records go through pinned staging: the host waits only until the
     // previous batch's records were copied, not for that batch to finish.
@@ -1776,6 +1791,9 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.total = total;
         args.push_back(wa);
     }
+    bool closest4 = e->closest_walk && e->trace_variant >= 3;
+    for (uint32_t k = 0; k < n; k++)
+        if (fr[k].count && fr[k].rows && !bvh4_usable(fr[k].ctx)) closest4 = false;
     oxd::WaveArgs base{};
     {
         // One scene for every frame (a single tracer's refine, or views of
@@ -1808,6 +1826,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.jobs = J;
         wa.refill = e->refill;
         wa.walk_lim = e->walk_lim;
+        wa.closest4 = closest4 ? 1u : 0u;
         wa.total = total;
         wa.out = e->out;
         wa.counters = nullptr;

@@ -18,6 +18,7 @@
 #include "kernels.cuh"
 #include "shade.cuh"
 #include "traverse.cuh"
+#include "walk.cuh"
 #include "path.cuh"
 
 namespace oxd {
@@ -144,11 +145,27 @@ __global__ void __launch_bounds__(128) trace_rays(const __grid_constant__ RayArg
         uint32_t m = 0;
         Ray ray = make_ray(mk(r[0], r[1], r[2]), mk(r[4], r[5], r[6]));
         bool primary = (a.flags & 2u) != 0u;
-        bool got = (a.flags & 5u) == 5u
-                       ? occluded4<COUNT, STACK>(a.s, ray, r[3], smp, 0u, primary, __float_as_uint(r[7]), &h, &m, cnt,
-                                                 a.err)
-                       : traverse<COUNT>(a.s, ray, r[3], smp, 0u, primary, (a.flags & 1u) != 0u,
-                                         __float_as_uint(r[7]), &h, &m, cnt, a.err);
+        bool got;
+        if ((a.flags & 9u) == 8u) {
+            // Closest hit over the four-wide tree (the tolerance plan's walk),
+            // its whole stack in local memory.
+            __shared__ uint32_t unused_columns[1];
+            Walk4C<1, STACK> w;
+            got = false;
+            if (walk4c_begin<1, STACK>(a.s, ray, r[3], w)) {
+                while (!walk4c_step<COUNT, 1, STACK, 128>(&a.s, unused_columns, 0u, ray, 0u, 0u, primary,
+                                                          __float_as_uint(r[7]), w, cnt, a.err)) {
+                }
+            }
+            got = w.hit_any;
+            h = w.best;
+        } else {
+            got = (a.flags & 5u) == 5u
+                      ? occluded4<COUNT, STACK>(a.s, ray, r[3], smp, 0u, primary, __float_as_uint(r[7]), &h, &m,
+                                                cnt, a.err)
+                      : traverse<COUNT>(a.s, ray, r[3], smp, 0u, primary, (a.flags & 1u) != 0u,
+                                        __float_as_uint(r[7]), &h, &m, cnt, a.err);
+        }
         if (a.slot) a.slot[i] = got ? h.slot : NONE;
         if (a.gid) a.gid[i] = got ? tri_word(a.s, h.slot, 0u) : NONE;
         if (a.t) a.t[i] = got ? h.t : 0.0f;

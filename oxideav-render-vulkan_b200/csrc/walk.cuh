@@ -307,4 +307,160 @@ __device__ __forceinline__ bool walk4s_step(const Scene* sp_, uint32_t* stack_wo
     return false;
 }
 
+// ---------------------------------------------------------------------
+// Four-wide closest-hit walk (the tolerance plan, not the reference's
+// order). Per inner node the four child boxes are slab-tested against the
+// current t_max; the nearest passing child is taken next and the others
+// pushed with their entry distances, farthest first, so pops come back in
+// near-to-far order; a popped entry farther than t_max is culled. With
+// every child box inside its parent's it reaches every leaf the binary
+// walk could need, so the closest hit is the binary walk's except where
+// two candidate hits lie within rounding of each other (exact ties, and a
+// leaf whose box entry rounds past a contained hit at nearly the same
+// distance): there the order decides, and it differs. Stack entries are
+// (reference, entry distance) in two column blocks of SS x NT words.
+// ---------------------------------------------------------------------
+template <int SS, int SD>
+struct Walk4C {
+    float t_max;
+    uint32_t cur, sp, guard;
+    bool hit_any;
+    uint32_t best_mat;
+    Hit best;
+    uint32_t deep_ref[SD];
+    float deep_t[SD];
+};
+
+template <int SS, int SD>
+__device__ __forceinline__ bool walk4c_begin(const Scene& s, const Ray& r, float t_max, Walk4C<SS, SD>& w) {
+    w.best.slot = NONE;
+    w.hit_any = false;
+    w.best_mat = 0u;
+    if (!r.valid || s.bvh4_root == NONE || s.P.env[3] == 0u) return false;
+    w.t_max = t_max;
+    w.cur = s.bvh4_root;
+    w.sp = 0u;
+    w.guard = 4u * s.bvh4_nodes + 8u;
+    return true;
+}
+
+template <bool COUNT, int SS, int SD, int NT>
+__device__ __forceinline__ bool walk4c_step(const Scene* sp_, uint32_t* words, uint32_t lim, const Ray& r,
+                                            uint32_t path_seed, uint32_t ray_id, bool primary, uint32_t skip,
+                                            Walk4C<SS, SD>& w, Cnt& cnt, uint32_t* err) {
+    const Scene& s = *sp_;
+    const uint32_t lane = threadIdx.x;
+    uint32_t* col_ref = words;
+    float* col_t = reinterpret_cast<float*>(words + SS * NT);
+    if (w.guard-- == 0u) {
+        atomicOr(err, 1u);
+        w.best.slot = NONE;
+        w.hit_any = false;
+        return true;
+    }
+    const uint32_t cur = w.cur;
+    if (cur & 0x80000000u) {
+        bump<COUNT>(cnt, C_LEAVES);
+        uint32_t first = cur & 0x07ffffffu, end = first + ((cur >> 27) & 15u) + 1u;
+        if ((uint64_t)end > s.slot_count) {
+            atomicOr(err, 2u);
+            w.best.slot = NONE;
+            w.hit_any = false;
+            return true;
+        }
+        for (uint32_t slot = first; slot < end; slot++) {
+            bump<COUNT>(cnt, C_TRIS);
+            uint64_t tb = tri_base(s, slot);
+            float4 q0 = geomv(s, tb), q1 = geomv(s, tb + 1), q2 = geomv(s, tb + 2);
+            Hit h;
+            if (!intersect(r, q0, q1, q2, w.t_max, &h)) continue;
+            uint32_t gid = __float_as_uint(q0.w);
+            if (gid == skip) continue;
+            uint32_t m = __float_as_uint(q2.w);
+            if (!accept_ol(sp_, slot, m, gid, h, path_seed, ray_id, primary)) continue;
+            h.slot = slot;
+            w.best = h;
+            w.best_mat = m;
+            w.hit_any = true;
+            w.t_max = h.t;
+        }
+    } else {
+        if (cur >= s.bvh4_nodes) {
+            atomicOr(err, 1u);
+            w.best.slot = NONE;
+            w.hit_any = false;
+            return true;
+        }
+        bump<COUNT>(cnt, C_BOXES, 4);
+        const float4* nd = s.bvh4 + (uint64_t)cur * 8u;
+        float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+        float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+        uint4 rf = __ldg(reinterpret_cast<const uint4*>(nd) + 6);
+        uint32_t ref[4] = {rf.x, rf.y, rf.z, rf.w};
+        float t[4];
+        t[0] = rf.x == NONE ? -1.0f : slab6(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, w.t_max);
+        t[1] = rf.y == NONE ? -1.0f : slab6(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, w.t_max);
+        t[2] = rf.z == NONE ? -1.0f : slab6(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, w.t_max);
+        t[3] = rf.w == NONE ? -1.0f : slab6(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, w.t_max);
+        // Order the passing children near to far (ties by child index).
+        uint32_t ord[4] = {0u, 1u, 2u, 3u};
+        uint32_t n = 0u;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (t[k] >= 0.0f) ord[n++] = (uint32_t)k;
+#pragma unroll
+        for (int i = 1; i < 4; i++) {
+#pragma unroll
+            for (int j = i; j > 0; j--) {
+                if ((uint32_t)j >= n) continue;
+                uint32_t a = ord[j - 1], b = ord[j];
+                if (t[b] < t[a]) {
+                    ord[j - 1] = b;
+                    ord[j] = a;
+                }
+            }
+        }
+        if (n > 0u) {
+            // Push all but the nearest, farthest first.
+            for (uint32_t q = n - 1u; q >= 1u; q--) {
+                if (w.sp >= (uint32_t)SD) {  // excluded on upload
+                    atomicOr(err, 4u);
+                    w.best.slot = NONE;
+                    w.hit_any = false;
+                    return true;
+                }
+                uint32_t k = ord[q];
+                if (w.sp < lim) {
+                    col_ref[w.sp * NT + lane] = ref[k];
+                    col_t[w.sp * NT + lane] = t[k];
+                } else {
+                    w.deep_ref[w.sp] = ref[k];
+                    w.deep_t[w.sp] = t[k];
+                }
+                w.sp++;
+            }
+            w.cur = ref[ord[0]];
+            return false;
+        }
+    }
+    while (w.sp != 0u) {
+        w.sp--;
+        bump<COUNT>(cnt, C_POPS);
+        float te;
+        uint32_t rr;
+        if (w.sp < lim) {
+            te = col_t[w.sp * NT + lane];
+            rr = col_ref[w.sp * NT + lane];
+        } else {
+            te = w.deep_t[w.sp];
+            rr = w.deep_ref[w.sp];
+        }
+        if (te <= w.t_max) {
+            w.cur = rr;
+            return false;
+        }
+    }
+    return true;
+}
+
 }  // namespace oxd

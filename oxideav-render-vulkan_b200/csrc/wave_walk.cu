@@ -17,9 +17,11 @@ constexpr uint32_t NT = WAVE_TRAVERSE_THREADS;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int STEPS = 4;        // walk steps between refill checks
 constexpr int SS2 = 8;          // binary walk: stack entries per lane in shared memory
-constexpr int SS4 = 16;         // four-wide walk: stack entries per lane in shared memory
+constexpr int SS4 = 16;         // four-wide any-hit walk: stack entries per lane in shared memory
+constexpr int SS4C = 12;        // four-wide closest-hit walk: stack entries per lane in shared memory
 constexpr uint32_t STACK2_BYTES = 3u * SS2 * NT * 4u;
 constexpr uint32_t STACK4_BYTES = SS4 * NT * 4u;
+constexpr uint32_t STACK4C_BYTES = 2u * SS4C * NT * 4u;
 constexpr uint32_t SM_SHARED = 228u * 1024u;  // shared memory per SM (sm_100)
 constexpr uint32_t CTA_RESERVED = 1024u;      // per resident CTA, reserved by the runtime
 
@@ -80,6 +82,65 @@ __global__ void __launch_bounds__(NT, MINB) walk_extend(const __grid_constant__ 
         for (int st = 0; st < STEPS && active; st++) {
             if (walk2s_step<COUNT, SS2, SD, NT>(sc, sh, r, path_seed, k << 16u, k == 0u, false, NONE, w, cnt,
                                                 a.err)) {
+                active = false;
+                if (w.hit_any) {
+                    const Hit& h = w.best;
+                    a.st.hit[i] = make_uint4(h.slot, __float_as_uint(h.t), __float_as_uint(h.b.y),
+                                             __float_as_uint(h.b.z));
+                    a.st.hmeta[i] = w.best_mat | (h.front ? 0x80000000u : 0u);
+                } else {
+                    a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+                }
+            }
+        }
+    }
+    if (COUNT)
+        for (int c = 0; c < C_N; c++)
+            if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
+}
+
+// Closest hits over the four-wide tree (the tolerance plan: the closest
+// hit equals the binary walk's except near-ties, see walk4c_step).
+template <bool COUNT, int MINB, int SD, bool BATCH>
+__global__ void __launch_bounds__(NT, MINB) walk_extend4(const __grid_constant__ WaveArgs a, uint32_t lim) {
+    Cnt cnt;
+    if (COUNT)
+        for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
+    const uint32_t slim = lim < (uint32_t)SS4C ? lim : (uint32_t)SS4C;
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
+    bool active = false, warp_drained = false;
+    uint32_t i = 0u, k = 0u, path_seed = 0u;
+    const Scene* sc = &a.s;
+    Ray r;
+    Walk4C<SS4C, SD> w;
+    for (;;) {
+        const unsigned act = __ballot_sync(FULL, active);
+        if (act == 0u && warp_drained) break;
+        if (!warp_drained && 32 - __popc(act) >= (act ? a.refill : 1u)) {
+            bool none_left = false;
+            if (!active) {
+                uint32_t q = append(&a.ctr[5]);
+                if (q < n) {
+                    i = a.q.ext[q];
+                    if (BATCH) sc = &a.frames[a.st.frame[i]].s;
+                    float4 o = a.st.org[i], d = a.st.dir[i];
+                    uint4 sd = a.st.seed[i];
+                    path_seed = sd.z;
+                    k = sd.w;
+                    bump<COUNT>(cnt, C_PATH_RAYS);
+                    r = make_ray(xyz(o), xyz(d));
+                    if (walk4c_begin<SS4C, SD>(*sc, r, INF, w)) active = true;
+                    else a.st.hit[i] = make_uint4(NONE, 0u, 0u, 0u);
+                } else {
+                    none_left = true;
+                }
+            }
+            warp_drained = __any_sync(FULL, none_left);
+        }
+#pragma unroll 1
+        for (int st = 0; st < STEPS && active; st++) {
+            if (walk4c_step<COUNT, SS4C, SD, NT>(sc, walk_smem, slim, r, path_seed, k << 16u, k == 0u, NONE, w, cnt,
+                                                 a.err)) {
                 active = false;
                 if (w.hit_any) {
                     const Hit& h = w.best;
@@ -176,6 +237,13 @@ void* ext_fn(int v) {
     return (void*)walk_extend<C, 12, SD, B>;
 }
 
+template <bool C, int SD, bool B>
+void* ext4_fn(int v) {
+    if (v == 0) return (void*)walk_extend4<C, 8, SD, B>;
+    if (v == 1) return (void*)walk_extend4<C, 10, SD, B>;
+    return (void*)walk_extend4<C, 12, SD, B>;
+}
+
 template <bool C, int SD, bool FOUR, bool B>
 void* shadow_fn(int v) {
     if (v == 0) return (void*)walk_shadow<C, 8, SD, FOUR, B>;
@@ -185,6 +253,7 @@ void* shadow_fn(int v) {
 
 template <bool C, bool B>
 void* kernel_c(bool ext, bool four, int v, int sd) {
+    if (ext && four) return sd <= 32 ? ext4_fn<C, 32, B>(v) : ext4_fn<C, 64, B>(v);
     if (ext) return sd <= 32 ? ext_fn<C, 32, B>(v) : ext_fn<C, 64, B>(v);
     if (four) return sd <= 32 ? shadow_fn<C, 32, true, B>(v) : shadow_fn<C, 64, true, B>(v);
     return sd <= 32 ? shadow_fn<C, 32, false, B>(v) : shadow_fn<C, 64, false, B>(v);
@@ -199,6 +268,7 @@ const int TARGET_BLOCKS[3] = {8, 10, 12};
 
 }  // namespace
 
+// ext && four: closest hits over the four-wide tree (walk_extend4).
 // variant 0..2: 8 / 10 / 12 resident blocks per SM targeted. The shared
 // memory each block gets is what that many blocks leave per block; after
 // the stack columns, the rest holds the binary tree's top nodes (binary
@@ -210,11 +280,11 @@ cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int 
     void* fn = kernel_of(count, a.nframes > 0, ext, four, variant, sd);
     if (!fn) return cudaErrorInvalidValue;
     const uint32_t target = (uint32_t)TARGET_BLOCKS[variant];
-    const uint32_t stack_bytes = (ext || !four) ? STACK2_BYTES : STACK4_BYTES;
+    const uint32_t stack_bytes = four ? (ext ? STACK4C_BYTES : STACK4_BYTES) : STACK2_BYTES;
     uint32_t per_block = SM_SHARED / target - CTA_RESERVED;
     if (per_block > 48u * 1024u) per_block = 48u * 1024u;
-    uint32_t staged = 0u;  // float4 words of staged top nodes
-    if ((ext || !four) && (a.nframes == 0 || a.one_scene) && per_block > stack_bytes) {
+    uint32_t staged = 0u;  // float4 words of staged top nodes (binary walks)
+    if (!four && (a.nframes == 0 || a.one_scene) && per_block > stack_bytes) {
         uint64_t nodes = (per_block - stack_bytes) / 32u;
         if (nodes > a.s.P.env[3]) nodes = a.s.P.env[3];
         if (2 * nodes > a.s.geom_vec4) nodes = a.s.geom_vec4 / 2;
@@ -227,8 +297,9 @@ cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int 
     unsigned blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
     WaveArgs copy = a;
     uint32_t lim = a.walk_lim;
-    void* args[] = {&copy, &staged, &lim};
-    return cudaLaunchKernel(fn, dim3(blocks), dim3(NT), args, smem, st);
+    void* args3[] = {&copy, &staged, &lim};
+    void* args2[] = {&copy, &lim};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(NT), (ext && four) ? args2 : args3, smem, st);
 }
 
 }  // namespace oxd

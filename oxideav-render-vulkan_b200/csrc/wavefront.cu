@@ -439,7 +439,7 @@ cudaError_t launch_wave_continue(cudaGraphConditionalHandle h, uint32_t* ctr, ui
 }
 
 cudaError_t launch_wave_extend(const WaveArgs& a, bool count, int variant, int stack, int sms, cudaStream_t st) {
-    if (variant >= 3) return launch_walk(a, count, true, false, variant - 3, stack, sms, st);
+    if (variant >= 3) return launch_walk(a, count, true, a.closest4 != 0u, variant - 3, stack, sms, st);
     return launch_trav(a, count, true, false, variant, stack, sms, st);
 }
 

@@ -130,6 +130,9 @@ struct WaveArgs {
     // words): `s` is then that scene, for the traversal kernels' staged
     // top nodes
     uint32_t one_scene = 0u;
+    // continuation rays walk the four-wide tree (traversal variants 3-5;
+    // the tolerance plan: closest hits equal except near-ties)
+    uint32_t closest4 = 0u;
 };
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3

@@ -36,10 +36,11 @@ class Plan:
     shadow_walk: int = 0
     graphs: int = 0
     refill: int = 8
+    closest_walk: int = 0  # 1: the tolerance plan (four-wide closest-hit walk), never chosen by the tuner
 
     def key(self):
         return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant,
-                self.shadow_walk, self.graphs, self.refill)
+                self.shadow_walk, self.graphs, self.refill, self.closest_walk)
 
 
 SPACE = {
@@ -99,7 +100,8 @@ def coordinate_descent(measure: Callable[[Plan], float], start: Optional[Plan] =
 def apply(tracer, plan: Plan):
     tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
                       stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant,
-                      shadow_walk=plan.shadow_walk, graphs=plan.graphs, refill=plan.refill)
+                      shadow_walk=plan.shadow_walk, graphs=plan.graphs, refill=plan.refill,
+                      closest_walk=plan.closest_walk)
 
 
 def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:

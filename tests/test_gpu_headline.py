@@ -13,7 +13,10 @@ step, a whole frame per launch round):
   (pathtrace.wgsl:1697-2073 is the estimator matched);
 * on the same 1.22 M-node tree, closest-hit ids of 10^6 random rays equal
   the oracle's except ties within 1e-6 relative t, and any-hit occlusion
-  (binary and four-wide walks) is identical (pathtrace.wgsl:651-735).
+  (binary and four-wide walks) is identical (pathtrace.wgsl:651-735);
+* the tolerance plan (closest hits over the four-wide tree): the same id
+  check on that tree, and a 64-spp band of the frame within 60 dB PSNR of
+  the oracle built with the C library's transcendentals.
 """
 from __future__ import annotations
 
@@ -111,3 +114,29 @@ def test_large_scene_million_rays(pkg, oracle, large):
         same = ~diff
         assert np.array_equal(tt[same].view(np.uint32), ot[same].view(np.uint32))
         assert np.array_equal(bary[same].view(np.uint32), obary[same].view(np.uint32))
+
+
+def test_large_scene_tolerance_plan(pkg, oracle, large):
+    import ctypes as C
+    import test_gpu_tolerance as tol
+    import scenes
+    t, p = large
+    rays = tol._rays(np.random.default_rng(22), 1_000_000, -1.4, 1.4)
+    tol.check_ids(pkg, oracle, t, p, rays, 250_000)
+    from oxideav_render_vulkan_b200 import tuner
+    t.set_tuning(trace_variant=4, closest_walk=1)
+    try:
+        t.reset()
+        y0, rows = 520, 24
+        L = pkg._native.lib()
+        assert L.oxpt_tracer_refine_rows(t._h, SPP, y0, rows) == 0
+        gpu = t.read_accum()
+        cpu = np.zeros_like(gpu)
+        oracle.dispatch(p, p.params, (0, SPP, y0, rows), cpu, libm=True)
+        rp = t.resolve_params(False)
+        img = oracle.resolve(gpu[y0:y0 + rows], rp, hdr=False)
+        ref = oracle.resolve(cpu[y0:y0 + rows], rp, hdr=False, libm=True)
+        assert scenes.psnr_rgb8(img, ref) >= 60.0
+    finally:
+        tuner.apply(t, tuner.LARGE_SCENE_PLAN)
+        t.reset()

@@ -47,8 +47,9 @@ def test_python_bindings_cover_the_headers(pkg):
 
 def test_abi_version_and_struct_sizes(pkg):
     lib = pkg._native.lib()
-    assert lib.oxpt_abi_version() == 1
+    assert lib.oxpt_abi_version() == 2  # 2: oxpt_tuning gained closest_walk
     N = pkg._native
+    assert C.sizeof(N.Tuning) == 72
     assert C.sizeof(N.Params) == 176  # src/pathtrace.rs:100-114
     assert C.sizeof(N.Frame) == 16  # src/pathtrace.rs:116-123
     assert C.sizeof(N.ResolveParams) == 48  # src/pathtrace.rs:125-131
