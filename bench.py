@@ -1026,6 +1026,17 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": kd["traffic_bytes_per_launch"],
                              "kernel": dom, "peak_kind": peak_kind,
+                             "dram_gbs": (kd["traffic_bytes_per_launch"] / (kd["launch_ms"] * 1e-3) / 1e9
+                                          if kd["traffic_bytes_per_launch"] else None),
+                             "dram_frac": (kd["traffic_bytes_per_launch"] / (kd["launch_ms"] * 1e-3) / 1e9 / peak
+                                           if kd["traffic_bytes_per_launch"] else None),
+                             "l1_l2_served_share": (1.0 - kd["traffic_bytes_per_launch"] /
+                                                    kd["algorithmic_bytes_per_launch"]
+                                                    if kd["traffic_bytes_per_launch"] else None),
+                             "limiter": "dependent-load latency and SIMD divergence of the walks: node and "
+                                        "triangle bytes are served mostly by L1/L2 (see l1_l2_served_share), "
+                                        "so frac is an effective bandwidth against the HBM copy peak, and "
+                                        "dram_frac the kernel's real HBM use",
                              "algorithmic_bytes_per_launch": kd["algorithmic_bytes_per_launch"],
                              "launch_ms": kd["launch_ms"], "launches": kd["launches"],
                              "algorithmic_bytes_per_path": bytes_per_path, "kernels": kernels,
