@@ -87,11 +87,14 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
                                  uint64_t max_paths_per_launch);
 
 /* Traversal kernels of trace_variant 3-5: walk-stack entries per lane kept
- * in shared memory (default all the kernel's columns: 8 for binary walks,
- * 16 for four-wide ones); deeper entries live in local memory. Smaller
- * values only move entries to local memory (results are unchanged), which
- * lets tests exercise that path on shallow trees. */
-oxpt_status oxpt_diag_set_walk_shared(oxpt_ctx* ctx, uint32_t entries);
+ * in shared memory (at most 16; deeper entries live in local memory) and
+ * the number of top nodes of the binary tree each CTA stages in shared
+ * memory (within what the variant's occupancy leaves a block). Both only
+ * move data between memories (results are unchanged); shared memory is
+ * taken from L1, so the defaults are measured choices. 0 entries puts the
+ * whole stack in local memory, which lets tests exercise that path. */
+oxpt_status oxpt_diag_set_walk(oxpt_ctx* ctx, uint32_t stack_entries, uint32_t staged_nodes);
+oxpt_status oxpt_diag_get_walk(const oxpt_ctx* ctx, uint32_t out[2]);
 
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left

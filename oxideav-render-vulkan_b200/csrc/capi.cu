@@ -122,7 +122,9 @@ struct oxpt_ctx {
     uint32_t shadow_walk = 0;
     uint32_t closest_walk = 0;  // 1: continuation rays on the four-wide tree (tolerance plan)
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
-    uint32_t walk_lim = 0xffffffffu;  // traversal variants 3-5: shared stack entries per lane (diagnostic)
+    // traversal variants 3-5: stack entries per lane kept in shared memory,
+    // top nodes of the binary tree staged per CTA (oxpt_diag_set_walk)
+    uint32_t walk_lim = oxd::WaveArgs{}.walk_lim, walk_stage = oxd::WaveArgs{}.walk_stage;
     void* wave_mem = nullptr;
     size_t wave_bytes = 0;
     uint32_t wave_cap_slots = 0, wave_cap_jobs = 0;
@@ -433,6 +435,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const ox
     wa.nframes = 0;
     wa.nrc = nrc ? *nrc : oxd::NrcWave{};
     wa.walk_lim = c->walk_lim;
+    wa.walk_stage = c->walk_stage;
     wa.closest4 = (c->closest_walk && c->trace_variant >= 3 && bvh4_usable(c)) ? 1u : 0u;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
@@ -1271,9 +1274,17 @@ oxpt_status oxpt_diag_counters_split(const oxpt_ctx* c, uint64_t out[16]) {
     return OXPT_OK;
 }
 
-oxpt_status oxpt_diag_set_walk_shared(oxpt_ctx* c, uint32_t entries) {
+oxpt_status oxpt_diag_set_walk(oxpt_ctx* c, uint32_t stack_entries, uint32_t staged_nodes) {
     if (!c) return OXPT_E_INVALID;
-    c->walk_lim = entries;
+    c->walk_lim = stack_entries;
+    c->walk_stage = staged_nodes;
+    return OXPT_OK;
+}
+
+oxpt_status oxpt_diag_get_walk(const oxpt_ctx* c, uint32_t out[2]) {
+    if (!c || !out) return OXPT_E_INVALID;
+    out[0] = c->walk_lim;
+    out[1] = c->walk_stage;
     return OXPT_OK;
 }
 
@@ -1568,7 +1579,7 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
         // node words (one-scene batches), the walk's storage split and tree.
         const oxd::WaveArgs& a0 = args[0];
         key.insert(key.end(), {(uint64_t)(uintptr_t)a0.s.geom, a0.s.geom_vec4, a0.s.P.env[3], a0.one_scene,
-                               a0.closest4, a0.walk_lim});
+                               a0.closest4, a0.walk_lim, a0.walk_stage});
     }
     for (size_t k = 0; k < rounds.size(); k++) {
         const oxd::WaveArgs& wa = args[k];
@@ -1826,6 +1837,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.jobs = J;
         wa.refill = e->refill;
         wa.walk_lim = e->walk_lim;
+        wa.walk_stage = e->walk_stage;
         wa.closest4 = closest4 ? 1u : 0u;
         wa.total = total;
         wa.out = e->out;

@@ -6,10 +6,11 @@
 // the far child on overflow) and the exact four-wide any-hit walk — with
 // the storage moved on chip:
 //
-// * Walk stacks: the first SS entries of each lane's stack live in shared
-//   memory as columns (entry k of lane j at word k * NT + j), so the 32
-//   lanes of a warp push and pop with one conflict-free shared-memory
-//   access; deeper entries go to local memory. Near-first walks of the
+// * Walk stacks: the first `lim` entries (at most SS) of each lane's stack
+//   live in shared memory as columns (entry k of lane j at word k * NT + j,
+//   one block of lim * NT words per field), so the 32 lanes of a warp push
+//   and pop with one conflict-free shared-memory access; deeper entries go
+//   to local memory. Near-first walks of the
 //   scenes here rarely go deeper than a handful of entries, so the per-
 //   thread local stack (512-768 bytes per lane, more than L1 holds at
 //   traversal occupancy) is no longer touched on the common path.
@@ -67,8 +68,8 @@ __device__ __forceinline__ float4 node_vec(const Scene& s, const WalkShared& sh,
 
 // ---------------------------------------------------------------------
 // Ordered binary walk with a short shared stack: entries (first, count, t)
-// in three column blocks of SS x NT words; entries from sh.lim on in local
-// memory. SD is the full depth (64 as the reference, or 32 when the tree
+// in three column blocks of sh.lim x NT words; entries from sh.lim on in
+// local memory. SD is the full depth (64 as the reference, or 32 when the tree
 // has at most 32 levels).
 // ---------------------------------------------------------------------
 template <int SS, int SD>
@@ -108,8 +109,8 @@ __device__ __forceinline__ bool walk2s_step(const Scene* sp_, const WalkShared& 
     const Scene& s = *sp_;
     const uint32_t lane = threadIdx.x;
     uint32_t* col_f = sh.words;
-    uint32_t* col_c = sh.words + SS * NT;
-    float* col_t = reinterpret_cast<float*>(sh.words + 2 * SS * NT);
+    uint32_t* col_c = sh.words + sh.lim * NT;
+    float* col_t = reinterpret_cast<float*>(sh.words + 2 * sh.lim * NT);
     if (w.guard-- == 0u) {
         atomicOr(err, 1u);
         w.best.slot = NONE;
@@ -318,7 +319,7 @@ __device__ __forceinline__ bool walk4s_step(const Scene* sp_, uint32_t* stack_wo
 // two candidate hits lie within rounding of each other (exact ties, and a
 // leaf whose box entry rounds past a contained hit at nearly the same
 // distance): there the order decides, and it differs. Stack entries are
-// (reference, entry distance) in two column blocks of SS x NT words.
+// (reference, entry distance) in two column blocks of lim x NT words.
 // ---------------------------------------------------------------------
 template <int SS, int SD>
 struct Walk4C {
@@ -351,7 +352,7 @@ __device__ __forceinline__ bool walk4c_step(const Scene* sp_, uint32_t* words, u
     const Scene& s = *sp_;
     const uint32_t lane = threadIdx.x;
     uint32_t* col_ref = words;
-    float* col_t = reinterpret_cast<float*>(words + SS * NT);
+    float* col_t = reinterpret_cast<float*>(words + lim * NT);
     if (w.guard-- == 0u) {
         atomicOr(err, 1u);
         w.best.slot = NONE;

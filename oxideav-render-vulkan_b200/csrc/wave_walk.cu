@@ -4,7 +4,10 @@
 // over the ray queues with the lane refill of wave_extend / wave_shadow
 // (wavefront.cu), and the same per-ray steps, so every result, counter and
 // error bit equals theirs. Chosen by trace_variant 3-5 (occupancy targets
-// of 8, 10 and 12 resident blocks per SM).
+// of 6, 8 and 10 resident blocks per SM). How many stack entries per lane
+// live in shared memory and how many top nodes a CTA stages are launch
+// parameters (shared memory taken from L1: more on chip is not always
+// faster), set per context (oxpt_diag_set_walk).
 #include "kernels.cuh"
 #include "walk.cuh"
 #include "wavefront.cuh"
@@ -16,14 +19,19 @@ namespace {
 constexpr uint32_t NT = WAVE_TRAVERSE_THREADS;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int STEPS = 4;        // walk steps between refill checks
-constexpr int SS2 = 8;          // binary walk: stack entries per lane in shared memory
-constexpr int SS4 = 16;         // four-wide any-hit walk: stack entries per lane in shared memory
-constexpr int SS4C = 12;        // four-wide closest-hit walk: stack entries per lane in shared memory
-constexpr uint32_t STACK2_BYTES = 3u * SS2 * NT * 4u;
-constexpr uint32_t STACK4_BYTES = SS4 * NT * 4u;
-constexpr uint32_t STACK4C_BYTES = 2u * SS4C * NT * 4u;
+// Most stack entries per lane a walk keeps in shared memory (the launch
+// may keep fewer): binary walk (3 words an entry), four-wide any-hit walk
+// (1 word), four-wide closest-hit walk (2 words).
+constexpr int SS2 = 16;
+constexpr int SS4 = 16;
+constexpr int SS4C = 16;
 constexpr uint32_t SM_SHARED = 228u * 1024u;  // shared memory per SM (sm_100)
 constexpr uint32_t CTA_RESERVED = 1024u;      // per resident CTA, reserved by the runtime
+
+// Shared-memory bytes of `lim` stack entries per lane.
+__host__ __device__ constexpr uint32_t stack_bytes_of(uint32_t words_per_entry, uint32_t lim) {
+    return words_per_entry * lim * NT * 4u;
+}
 
 extern __shared__ __align__(16) uint32_t walk_smem[];
 
@@ -47,7 +55,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_extend(const __grid_constant__ 
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
-    const WalkShared sh = stage_nodes(a.s, STACK2_BYTES, staged, lim < SS2 ? lim : SS2);
+    const WalkShared sh = stage_nodes(a.s, stack_bytes_of(3u, lim), staged, lim);
     const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
     bool active = false, warp_drained = false;
     uint32_t i = 0u, k = 0u, path_seed = 0u;
@@ -106,7 +114,6 @@ __global__ void __launch_bounds__(NT, MINB) walk_extend4(const __grid_constant__
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
-    const uint32_t slim = lim < (uint32_t)SS4C ? lim : (uint32_t)SS4C;
     const uint32_t n = *((volatile uint32_t*)&a.ctr[0]);
     bool active = false, warp_drained = false;
     uint32_t i = 0u, k = 0u, path_seed = 0u;
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_extend4(const __grid_constant__
         }
 #pragma unroll 1
         for (int st = 0; st < STEPS && active; st++) {
-            if (walk4c_step<COUNT, SS4C, SD, NT>(sc, walk_smem, slim, r, path_seed, k << 16u, k == 0u, NONE, w, cnt,
+            if (walk4c_step<COUNT, SS4C, SD, NT>(sc, walk_smem, lim, r, path_seed, k << 16u, k == 0u, NONE, w, cnt,
                                                  a.err)) {
                 active = false;
                 if (w.hit_any) {
@@ -172,9 +179,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ 
     Cnt cnt;
     if (COUNT)
         for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
-    const uint32_t cap = FOUR ? (uint32_t)SS4 : (uint32_t)SS2;
-    const WalkShared sh = stage_nodes(a.s, FOUR ? STACK4_BYTES : STACK2_BYTES, FOUR ? 0u : staged,
-                                      lim < cap ? lim : cap);
+    const WalkShared sh = stage_nodes(a.s, stack_bytes_of(FOUR ? 1u : 3u, lim), FOUR ? 0u : staged, lim);
     const uint32_t n = *((volatile uint32_t*)&a.ctr[1]);
     bool active = false, warp_drained = false;
     uint32_t slot = 0u, job = 0u, rid = 0u, skip = NONE, path_seed = 0u;
@@ -232,23 +237,23 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ 
 
 template <bool C, int SD, bool B>
 void* ext_fn(int v) {
-    if (v == 0) return (void*)walk_extend<C, 8, SD, B>;
-    if (v == 1) return (void*)walk_extend<C, 10, SD, B>;
-    return (void*)walk_extend<C, 12, SD, B>;
+    if (v == 0) return (void*)walk_extend<C, 6, SD, B>;
+    if (v == 1) return (void*)walk_extend<C, 8, SD, B>;
+    return (void*)walk_extend<C, 10, SD, B>;
 }
 
 template <bool C, int SD, bool B>
 void* ext4_fn(int v) {
-    if (v == 0) return (void*)walk_extend4<C, 8, SD, B>;
-    if (v == 1) return (void*)walk_extend4<C, 10, SD, B>;
-    return (void*)walk_extend4<C, 12, SD, B>;
+    if (v == 0) return (void*)walk_extend4<C, 6, SD, B>;
+    if (v == 1) return (void*)walk_extend4<C, 8, SD, B>;
+    return (void*)walk_extend4<C, 10, SD, B>;
 }
 
 template <bool C, int SD, bool FOUR, bool B>
 void* shadow_fn(int v) {
-    if (v == 0) return (void*)walk_shadow<C, 8, SD, FOUR, B>;
-    if (v == 1) return (void*)walk_shadow<C, 10, SD, FOUR, B>;
-    return (void*)walk_shadow<C, 12, SD, FOUR, B>;
+    if (v == 0) return (void*)walk_shadow<C, 6, SD, FOUR, B>;
+    if (v == 1) return (void*)walk_shadow<C, 8, SD, FOUR, B>;
+    return (void*)walk_shadow<C, 10, SD, FOUR, B>;
 }
 
 template <bool C, bool B>
@@ -264,28 +269,33 @@ void* kernel_of(bool count, bool batch, bool ext, bool four, int v, int sd) {
     return count ? kernel_c<true, false>(ext, four, v, sd) : kernel_c<false, false>(ext, four, v, sd);
 }
 
-const int TARGET_BLOCKS[3] = {8, 10, 12};
+const int TARGET_BLOCKS[3] = {6, 8, 10};
 
 }  // namespace
 
 // ext && four: closest hits over the four-wide tree (walk_extend4).
-// variant 0..2: 8 / 10 / 12 resident blocks per SM targeted. The shared
-// memory each block gets is what that many blocks leave per block; after
-// the stack columns, the rest holds the binary tree's top nodes (binary
-// walks of launches over one scene only: a plain launch, or a batch whose
-// frames all trace the same node words).
+// variant 0..2: 6 / 8 / 10 resident blocks per SM targeted. a.walk_lim
+// stack entries per lane (at most the walk's SS) live in shared memory;
+// binary walks of launches over one scene (a plain launch, or a batch
+// whose frames all trace the same node words) also stage up to
+// a.walk_stage top nodes, within what the targeted number of blocks leaves
+// each block.
 cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
                         cudaStream_t st) {
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
     void* fn = kernel_of(count, a.nframes > 0, ext, four, variant, sd);
     if (!fn) return cudaErrorInvalidValue;
     const uint32_t target = (uint32_t)TARGET_BLOCKS[variant];
-    const uint32_t stack_bytes = four ? (ext ? STACK4C_BYTES : STACK4_BYTES) : STACK2_BYTES;
+    const uint32_t words = four ? (ext ? 2u : 1u) : 3u;
+    const uint32_t cap = four ? (ext ? (uint32_t)SS4C : (uint32_t)SS4) : (uint32_t)SS2;
+    uint32_t lim = a.walk_lim < cap ? a.walk_lim : cap;
+    const uint32_t stack_bytes = stack_bytes_of(words, lim);
     uint32_t per_block = SM_SHARED / target - CTA_RESERVED;
     if (per_block > 48u * 1024u) per_block = 48u * 1024u;
     uint32_t staged = 0u;  // float4 words of staged top nodes (binary walks)
     if (!four && (a.nframes == 0 || a.one_scene) && per_block > stack_bytes) {
         uint64_t nodes = (per_block - stack_bytes) / 32u;
+        if (nodes > a.walk_stage) nodes = a.walk_stage;
         if (nodes > a.s.P.env[3]) nodes = a.s.P.env[3];
         if (2 * nodes > a.s.geom_vec4) nodes = a.s.geom_vec4 / 2;
         staged = (uint32_t)(2 * nodes);
@@ -296,7 +306,6 @@ cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int 
     if (e != cudaSuccess) return e;
     unsigned blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
     WaveArgs copy = a;
-    uint32_t lim = a.walk_lim;
     void* args3[] = {&copy, &staged, &lim};
     void* args2[] = {&copy, &lim};
     return cudaLaunchKernel(fn, dim3(blocks), dim3(NT), (ext && four) ? args2 : args3, smem, st);

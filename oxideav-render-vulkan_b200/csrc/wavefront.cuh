@@ -124,8 +124,10 @@ struct WaveArgs {
     uint32_t nframes;
     NrcWave nrc;
     // traversal variants 3-5: walk-stack entries per lane kept in shared
-    // memory (capped by the kernel's columns; deeper ones in local memory)
-    uint32_t walk_lim = 0xffffffffu;
+    // memory (capped by the kernel's columns; deeper ones in local memory),
+    // and top nodes of the binary tree a CTA stages in shared memory
+    uint32_t walk_lim = 8u;
+    uint32_t walk_stage = 0u;
     // batched launches whose frames all trace one scene (the same node
     // words): `s` is then that scene, for the traversal kernels' staged
     // top nodes
@@ -137,7 +139,7 @@ struct WaveArgs {
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3
 // / 4 blocks per SM; traversal 6 / 8 / 10); traversal variants 3..5 run the
-// on-chip-stack kernels of wave_walk.cu (8 / 10 / 12 blocks per SM);
+// on-chip-stack kernels of wave_walk.cu (6 / 8 / 10 blocks per SM);
 // `stack`: 32 or 64 entries.
 // With a.nframes > 0 the batched kernels run (count must then be false).
 cudaError_t launch_wave_logic(const WaveArgs& a, bool count, int variant, cudaStream_t st);
@@ -148,7 +150,7 @@ cudaError_t launch_wave_shadow(const WaveArgs& a, bool count, bool four, int var
                                cudaStream_t st);
 // wave_walk.cu: traversal with shared-memory short stacks and staged top
 // nodes; ext = closest hit of the continuation queue, else the shadow queue
-// (four: the four-wide tree); variant 0..2 targets 8 / 10 / 12 blocks per SM.
+// (four: the four-wide tree); variant 0..2 targets 6 / 8 / 10 blocks per SM.
 cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
                         cudaStream_t st);
 // Graph-resident loop: after an iteration, sets the enclosing while node's

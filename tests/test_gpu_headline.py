@@ -68,12 +68,14 @@ def test_large_scene_64spp_row_bands_bit_exact(pkg, oracle, large):
     cov = gpu[..., 3]
     assert cov.min() >= 0 and cov.max() <= SPP and (cov == SPP).mean() > 0.2
     cpu = np.zeros_like(gpu)
+    covered = 0.0
     for y0 in (0, 538, 1077):
         oracle.dispatch(p, p.params, (0, SPP, y0, 3), cpu)
         band_gpu, band_cpu = gpu[y0:y0 + 3], cpu[y0:y0 + 3]
         diff = band_gpu.view(np.uint32) != band_cpu.view(np.uint32)
         assert not diff.any(), f"rows {y0}..{y0 + 2}: {np.count_nonzero(diff.any(axis=2))} pixels differ"
-        assert band_cpu[..., 3].sum() > 0
+        covered += float(band_cpu[..., 3].sum())
+    assert covered > 0  # the middle band crosses the sphere (the top one sees only sky)
 
 
 def test_large_scene_million_rays(pkg, oracle, large):

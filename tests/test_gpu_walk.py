@@ -59,16 +59,21 @@ def test_short_stack_kernels_bit_exact(pkg, oracle, which, mode, variant, walk):
     assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
 
 
-@pytest.mark.parametrize("lim", [0, 1, 3])
+@pytest.mark.parametrize("stage", [0, 200])
+@pytest.mark.parametrize("lim", [0, 1, 3, 16])
 @pytest.mark.parametrize("walk", [0, 1])
-def test_stack_entries_in_local_memory_bit_exact(pkg, oracle, lim, walk):
-    """Fewer shared entries push the walk onto its local-memory part."""
+def test_stack_entries_in_local_memory_bit_exact(pkg, oracle, lim, walk, stage):
+    """Fewer shared entries push the walk onto its local-memory part; staged
+    top nodes serve the binary walk's first levels from shared memory."""
     scene = pkg.Scene.icosphere(freq=48, seed=5, n_materials=8, n_textures=2, tex_size=64, n_punctual=4,
                                 n_emissive=32, material_mix=1)
     env = pkg.EnvironmentMap.sky(64, 32)
     t = _tracer(pkg, scene, env, w=48, h=32, spp=4, bounces=8)
     t.set_tuning(mode=2, trace_variant=4, shadow_walk=walk)
-    assert pkg._native.lib().oxpt_diag_set_walk_shared(t.ctx, lim) == 0
+    L = pkg._native.lib()
+    cur = (C.c_uint32 * 2)()
+    assert L.oxpt_diag_get_walk(t.ctx, cur) == 0 and cur[0] > 0
+    assert L.oxpt_diag_set_walk(t.ctx, lim, stage) == 0
     t.refine(4)
     cpu, _ = oracle.render(t.prepared(), 4)
     assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
