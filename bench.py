@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tolerance-plan", action="store_true",
+                    help="skip timing the tolerance plan (four-wide closest hits) beside the exact one")
     ap.add_argument("--mode", default="auto", choices=["auto", "mega", "wave", "split"],
                     help="execution plan; auto = the library default")
     ap.add_argument("--slots", type=int, default=0, help="wavefront paths in flight (0 = default)")
@@ -1010,6 +1012,37 @@ def main():
                "pipeline": "scene staged into a second buffer set during the previous step's trace; "
                            "image read back on the copy stream"}
 
+    # The tolerance plan (closest hits over the four-wide tree: images within
+    # 60 dB of the CPU tracer, hit ids equal except near-ties, not bit-exact)
+    # on the same frames, device-timed the same way; `value` stays the
+    # bit-exact plan's.
+    tolerance = None
+    if not a.no_tolerance_plan:
+        saved = pt.tuning()
+        tv = saved.trace_variant if saved.trace_variant >= 3 else 3
+        pt.set_tuning(trace_variant=tv, closest_walk=1)
+        for _ in range(max(1, a.warmup // 2)):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tsec = e0.elapsed_time(e1) / 1e3
+        if world > 1:
+            t = torch.tensor([tsec], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tsec = float(t.item())
+        tolerance = {"value": frames * a.steps * paths_step / tsec / 1e6, "unit": "Msamples/s",
+                     "ms_per_step": 1e3 * tsec / a.steps, "plan": plan_of(pt),
+                     "checks": "tests/test_gpu_tolerance.py, tests/test_gpu_headline.py: ids on 10^6 rays equal "
+                               "except ties within 1e-6 relative t; >= 60 dB PSNR against the libm oracle"}
+        pt.set_tuning(trace_variant=saved.trace_variant, closest_walk=saved.closest_walk)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         import oracle
@@ -1042,7 +1075,8 @@ def main():
                              "algorithmic_bytes_per_path": bytes_per_path, "kernels": kernels,
                              "trace_phase_ms": tms.value, "reduce_ms_total": rms.value,
                              "kernel_timing": kernel_timing},
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(n1.value - n0.value),
+                "cpu_baseline": cpu, "e2e": e2e, "tolerance_plan": tolerance,
+                "gpu_launches": int(n1.value - n0.value),
                 "clocks": clk.summary(), "rays_per_path": rays_per_path,
                 "plan": plan_of(pt), "tuner_trials": len(tune_log)}
         print(json.dumps(line), flush=True)
