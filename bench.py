@@ -861,20 +861,19 @@ def main():
     pt.set_environment(env)
     pt.sync(scene, opts)
     tune_log = []
-    if a.mode != "auto" or a.slots:
-        kw = {"wave_slots": a.slots} if a.slots else {}
-        if a.mode != "auto":
-            kw["mode"] = {"mega": 0, "wave": 1, "split": 2}[a.mode]
-        if a.shadow_walk != "auto":
-            kw["shadow_walk"] = {"four": 0, "binary": 1}[a.shadow_walk]
-        pt.set_tuning(**kw)
-    elif a.tune:
-        from oxideav_render_vulkan_b200 import tuner
+    from oxideav_render_vulkan_b200 import tuner
+    if a.tune:
         tuner.tune(pt, spp=min(a.spp, 4), repeats=3, log=tune_log)  # best of three per trial: steadier picks
     elif not a.no_tune:
-        from oxideav_render_vulkan_b200 import tuner
         tuner.apply(pt, tuner.LARGE_SCENE_PLAN)  # the tuner's pick on this scene, and the tested plan
         pt.set_tuning(wave_items=tuner.LARGE_SCENE_WAVE_ITEMS)
+    # Overrides on top of the plan.
+    if a.mode != "auto":
+        pt.set_tuning(mode={"mega": 0, "wave": 1, "split": 2}[a.mode])
+    if a.slots:
+        pt.set_tuning(wave_slots=a.slots)
+    if a.shadow_walk != "auto":
+        pt.set_tuning(shadow_walk={"four": 0, "binary": 1}[a.shadow_walk])
     if a.wave_items:
         pt.set_tuning(wave_items=a.wave_items)
     if a.trace_variant >= 0:
@@ -903,6 +902,8 @@ def main():
         "split_shade": (BYTES_ATTR + BYTES_MAT) * c[6] / npaths,
         "split_nee": 0.0,
     }
+    kernel_bytes["walk_extend"] = kernel_bytes["wave_extend"]  # on-chip-stack kernels (trace_variant 3-5)
+    kernel_bytes["walk_shadow"] = kernel_bytes["wave_shadow"]
     rays_per_path = (c[1] + c[2]) / npaths
 
     from oxideav_render_vulkan_b200 import shard
@@ -975,9 +976,11 @@ def main():
         kernel_timing = "same frames re-run without the graph (per-launch CUDA events)"
     paths_timed = paths_step * a.steps
     mode = pt.tuning().mode
-    kinds = {0: ((0, "trace_paths"),), 1: ((2, "wave_logic"), (3, "wave_extend"), (4, "wave_shadow")),
-             2: ((2, "split_logic"), (5, "split_shade"), (6, "split_nee"), (3, "wave_extend"),
-                 (4, "wave_shadow"))}[mode]
+    walk = pt.tuning().trace_variant >= 3
+    ext_name, sh_name = ("walk_extend", "walk_shadow") if walk else ("wave_extend", "wave_shadow")
+    kinds = {0: ((0, "trace_paths"),), 1: ((2, "wave_logic"), (3, ext_name), (4, sh_name)),
+             2: ((2, "split_logic"), (5, "split_shade"), (6, "split_nee"), (3, ext_name),
+                 (4, sh_name))}[mode]
     traffic_db = {}
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():

@@ -126,7 +126,9 @@ struct WaveArgs {
     // traversal variants 3-5: walk-stack entries per lane kept in shared
     // memory (capped by the kernel's columns; deeper ones in local memory),
     // and top nodes of the binary tree a CTA stages in shared memory
-    uint32_t walk_lim = 8u;
+    // (defaults measured on the 1.05 M-triangle scene: 2 entries and no
+    // staged nodes; more on chip only took L1 from the node fetches)
+    uint32_t walk_lim = 2u;
     uint32_t walk_stage = 0u;
     // batched launches whose frames all trace one scene (the same node
     // words): `s` is then that scene, for the traversal kernels' staged

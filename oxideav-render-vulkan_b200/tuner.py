@@ -58,7 +58,7 @@ SPACE = {
 # 64 spp, 12 bounces): the tuner's pick on that scene. The benchmark runs it
 # by default and the GPU parity test of that workload runs exactly it, so
 # the measured plan is the tested plan.
-LARGE_SCENE_PLAN = Plan(mode=N.MODE_WAVEFRONT_SPLIT, shade_variant=0, trace_variant=0, stack=64,
+LARGE_SCENE_PLAN = Plan(mode=N.MODE_WAVEFRONT_SPLIT, shade_variant=0, trace_variant=4, stack=64,
                         wave_slots=1 << 22, nee_variant=3, shadow_walk=0, graphs=1, refill=16)
 LARGE_SCENE_WAVE_ITEMS = 1 << 27  # paths per launch round: a whole frame
 

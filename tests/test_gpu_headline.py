@@ -53,8 +53,10 @@ def test_plan_is_the_benchmarked_plan(pkg, large):
     t, _ = large
     got = t.tuning()
     want = tuner.LARGE_SCENE_PLAN
-    assert (got.mode, got.wave_slots, got.nee_variant, got.shadow_walk, got.refill, got.graphs) == \
-        (want.mode, want.wave_slots, want.nee_variant, want.shadow_walk, want.refill, want.graphs)
+    assert (got.mode, got.wave_slots, got.nee_variant, got.shadow_walk, got.refill, got.graphs,
+            got.trace_variant, got.closest_walk) == \
+        (want.mode, want.wave_slots, want.nee_variant, want.shadow_walk, want.refill, want.graphs,
+         want.trace_variant, want.closest_walk)
     assert got.wave_items == tuner.LARGE_SCENE_WAVE_ITEMS
 
 
@@ -124,7 +126,7 @@ def test_large_scene_tolerance_plan(pkg, oracle, large):
     import scenes
     t, p = large
     rays = tol._rays(np.random.default_rng(22), 1_000_000, -1.4, 1.4)
-    tol.check_ids(pkg, oracle, t, p, rays, 250_000)
+    tol.check_ids(pkg, oracle, t, p, rays, 100_000)
     from oxideav_render_vulkan_b200 import tuner
     t.set_tuning(trace_variant=4, closest_walk=1)
     try:
