@@ -77,6 +77,11 @@ def parse():
     ap.add_argument("--trace-variant", type=int, default=-1, help="override the plan's traversal kernels "
                     "(0-2 local-memory stacks, 3-5 shared-memory short stacks)")
     ap.add_argument("--refill", type=int, default=0, help="override the plan's traversal refill threshold")
+    ap.add_argument("--graphs", type=int, default=-1, choices=[-1, 0, 1],
+                    help="override the plan's CUDA graphs (0: host-driven loop, e.g. for profilers that cannot "
+                         "see kernels inside graphs with conditional nodes)")
+    ap.add_argument("--nee-mask", type=int, default=-1, choices=[-1, 0, 1],
+                    help="split plan's NEE results as per-slot visibility bits (1, default) or per-job records (0)")
     ap.add_argument("--nee-variant", type=int, default=-1, help="serve workload: the executor's NEE kernel "
                     "(-1: the serving executor's default, job-major)")
     ap.add_argument("--shadow-walk", default="auto", choices=["auto", "four", "binary"],
@@ -880,6 +885,10 @@ def main():
         pt.set_tuning(trace_variant=a.trace_variant)
     if a.refill:
         pt.set_tuning(refill=a.refill)
+    if a.graphs >= 0:
+        pt.set_tuning(graphs=a.graphs)
+    if a.nee_mask >= 0:
+        L.oxpt_diag_set_nee_mask(pt.ctx, a.nee_mask)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):

@@ -95,6 +95,11 @@ oxpt_status oxpt_diag_set_launch(oxpt_ctx* ctx, uint32_t threads, uint32_t block
  * whole stack in local memory, which lets tests exercise that path. */
 oxpt_status oxpt_diag_set_walk(oxpt_ctx* ctx, uint32_t stack_entries, uint32_t staged_nodes);
 oxpt_status oxpt_diag_get_walk(const oxpt_ctx* ctx, uint32_t out[2]);
+/* Split plan with at most 32 NEE jobs per vertex: 1 (default) = the shadow
+ * kernels set a per-slot visibility bit and only queued jobs' contributions
+ * are stored, 0 = a pending record per job with a visibility word. The
+ * logic kernel adds the same contributions in the same order either way. */
+oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* ctx, int on);
 
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left

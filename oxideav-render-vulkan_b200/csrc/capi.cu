@@ -121,6 +121,9 @@ struct oxpt_ctx {
     uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
     uint32_t shadow_walk = 0;
     uint32_t closest_walk = 0;  // 1: continuation rays on the four-wide tree (tolerance plan)
+    // split plan: per-slot visibility masks instead of a pending record per
+    // NEE job (oxpt_diag_set_nee_mask; results are the same either way)
+    bool nee_mask = true;
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
     // traversal variants 3-5: stack entries per lane kept in shared memory,
     // top nodes of the binary tree staged per CTA (oxpt_diag_set_walk)
@@ -351,8 +354,9 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     bool split = c->mode == OXPT_MODE_WAVEFRONT_SPLIT;
     size_t sizes[] = {P * 8, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 4, P * 4,
                       PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64,
-                      split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0, P * 4};
-    constexpr int NB = 21;
+                      split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0, P * 4,
+                      (split && jobs <= 32) ? P * 4 : 0};
+    constexpr int NB = 22;
     size_t total = 0;
     for (size_t s : sizes) total += align256(s);
     if (slots > c->wave_cap_slots || jobs > c->wave_cap_jobs || total > c->wave_bytes) {
@@ -391,6 +395,7 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     st->nee_n = (uint32_t*)ptr[10];
     st->pend = (float4*)ptr[11];
     st->frame = (uint32_t*)ptr[20];
+    st->vis = (split && jobs <= 32 && c->nee_mask) ? (uint32_t*)ptr[21] : nullptr;
     q->ext = (uint32_t*)ptr[12];
     q->sh_o = (float4*)ptr[13];
     q->sh_d = (float4*)ptr[14];
@@ -1281,6 +1286,12 @@ oxpt_status oxpt_diag_set_walk(oxpt_ctx* c, uint32_t stack_entries, uint32_t sta
     return OXPT_OK;
 }
 
+oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* c, int on) {
+    if (!c) return OXPT_E_INVALID;
+    c->nee_mask = on != 0;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_diag_get_walk(const oxpt_ctx* c, uint32_t out[2]) {
     if (!c || !out) return OXPT_E_INVALID;
     out[0] = c->walk_lim;
@@ -1579,7 +1590,7 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
         // node words (one-scene batches), the walk's storage split and tree.
         const oxd::WaveArgs& a0 = args[0];
         key.insert(key.end(), {(uint64_t)(uintptr_t)a0.s.geom, a0.s.geom_vec4, a0.s.P.env[3], a0.one_scene,
-                               a0.closest4, a0.walk_lim, a0.walk_stage});
+                               a0.closest4, a0.walk_lim, a0.walk_stage, (uint64_t)(uintptr_t)a0.st.vis});
     }
     for (size_t k = 0; k < rounds.size(); k++) {
         const oxd::WaveArgs& wa = args[k];

@@ -210,9 +210,19 @@ __global__ void __launch_bounds__(128, 4) split_logic(const __grid_constant__ Wa
         const Scene& s = slot_scene<BATCH>(a, i);
         load_state(a, i, &pc, &smp);
         uint32_t n = a.st.nee_n[i];
-        for (uint32_t j = 0; j < n; j++) {
-            float4 pe = a.st.pend[(uint64_t)i * J + j];
-            if (pe.w == 2.0f) pc.radiance = pc.radiance + xyz(pe);
+        if (a.st.vis) {
+            // The unoccluded jobs' contributions, in job order.
+            uint32_t m = n ? a.st.vis[i] : 0u;
+            while (m) {
+                uint32_t j = __ffs(m) - 1u;
+                m &= m - 1u;
+                if (j < n) pc.radiance = pc.radiance + xyz(a.st.pend[(uint64_t)i * J + j]);
+            }
+        } else {
+            for (uint32_t j = 0; j < n; j++) {
+                float4 pe = a.st.pend[(uint64_t)i * J + j];
+                if (pe.w == 2.0f) pc.radiance = pc.radiance + xyz(pe);
+            }
         }
         if (n) a.st.nee_n[i] = 0u;
         int r = PATH_DONE;
@@ -391,14 +401,16 @@ __global__ void __launch_bounds__(128, MINB) split_nee(const __grid_constant__ W
         get_vertex(a, v, &vx, &pc, &path_seed);
         ShadowRay sr;
         float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (nee_job(s, s_sheen, pc, vx, j, &sr)) {
+        if (a.st.vis && j == 0u) a.st.vis[slot] = 0u;
+        bool queued = nee_job(s, s_sheen, pc, vx, j, &sr);
+        if (queued) {
             pe = make_float4(sr.pending.x, sr.pending.y, sr.pending.z, 1.0f);
             uint32_t q = append1(&a.ctr[1]);
             a.q.sh_o[q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
             a.q.sh_d[q] = make_float4(sr.d.x, sr.d.y, sr.d.z, __uint_as_float(sr.skip));
             a.q.sh_m[q] = make_uint4(slot, j, sr.rid, path_seed);
         }
-        a.st.pend[(uint64_t)slot * a.jobs + j] = pe;
+        if (queued || !a.st.vis) a.st.pend[(uint64_t)slot * a.jobs + j] = pe;
     }
 }
 
@@ -424,17 +436,19 @@ __global__ void __launch_bounds__(128, MINB) split_nee_v(const __grid_constant__
         PathCore pc;
         uint32_t path_seed;
         get_vertex(a, v, &vx, &pc, &path_seed);
+        if (a.st.vis) a.st.vis[slot] = 0u;
         for (uint32_t j = 0; j < J; j++) {
             ShadowRay sr;
             float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (nee_job(s, s_sheen, pc, vx, j, &sr)) {
+            bool queued = nee_job(s, s_sheen, pc, vx, j, &sr);
+            if (queued) {
                 pe = make_float4(sr.pending.x, sr.pending.y, sr.pending.z, 1.0f);
                 uint32_t q = append1(&a.ctr[1]);
                 a.q.sh_o[q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
                 a.q.sh_d[q] = make_float4(sr.d.x, sr.d.y, sr.d.z, __uint_as_float(sr.skip));
                 a.q.sh_m[q] = make_uint4(slot, j, sr.rid, path_seed);
             }
-            a.st.pend[(uint64_t)slot * a.jobs + j] = pe;
+            if (queued || !a.st.vis) a.st.pend[(uint64_t)slot * a.jobs + j] = pe;
         }
     }
 }

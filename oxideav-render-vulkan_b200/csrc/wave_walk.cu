@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ 
                     if constexpr (FOUR) started = walk4s_begin<SS4, SD>(*sc, r, o.w, ss.w);
                     else started = walk2s_begin<COUNT, SS2, SD>(*sc, sh, r, o.w, ss.w, cnt);
                     if (started) active = true;
-                    else a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;  // nothing in the way
+                    else mark_visible(a.st, a.jobs, slot, job);  // nothing in the way
                 } else {
                     none_left = true;
                 }
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ 
                                                        a.err);
             if (done) {
                 active = false;
-                if (!ss.w.hit_any) a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;
+                if (!ss.w.hit_any) mark_visible(a.st, a.jobs, slot, job);
             }
         }
     }

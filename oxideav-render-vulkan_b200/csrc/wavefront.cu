@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
                     if constexpr (FOUR) started = walk4_begin<SD>(*sc, r, o.w, sw.w);
                     else started = walk2_begin<COUNT, SD>(*sc, r, o.w, sw.w, cnt);
                     if (started) active = true;
-                    else a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;  // nothing in the way
+                    else mark_visible(a.st, a.jobs, slot, job);  // nothing in the way
                 } else {
                     none_left = true;
                 }
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(WAVE_TRAVERSE_THREADS, MINB) wave_shadow(const
             else done = walk2_step<COUNT, SD>(*sc, r, smp, rid, false, true, skip, sw.w, cnt, a.err);
             if (done) {
                 active = false;
-                if (!sw.w.hit_any) a.st.pend[(uint64_t)slot * a.jobs + job].w = 2.0f;
+                if (!sw.w.hit_any) mark_visible(a.st, a.jobs, slot, job);
             }
         }
     }

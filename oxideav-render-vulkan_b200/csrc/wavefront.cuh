@@ -43,7 +43,17 @@ struct WaveState {
     uint32_t* nee_n;           // NEE jobs of the last vertex to add (0..J)
     float4* pend;              // slots x J: contribution.xyz, 0 none / 1 queued / 2 visible
     uint32_t* frame;           // batched launches: the slot's frame
+    // split plan with at most 32 NEE jobs (else null): per slot, bit j set
+    // when job j's shadow ray found nothing in the way; pend then holds
+    // only the queued jobs' contributions and its w is not used
+    uint32_t* vis;
 };
+
+// Job `job` of `slot` is unoccluded: its contribution is added.
+__device__ __forceinline__ void mark_visible(const WaveState& st, uint32_t jobs, uint32_t slot, uint32_t job) {
+    if (st.vis) atomicOr(st.vis + slot, 1u << job);
+    else st.pend[(uint64_t)slot * jobs + job].w = 2.0f;
+}
 
 // One frame of a batched launch: a scene's samples [first, first + count)
 // over npix pixels from row y0, as the launch's items [base, base + total).

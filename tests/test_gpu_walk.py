@@ -119,3 +119,18 @@ def test_short_stack_batch_equals_each_refine(pkg):
     pkg.refine_batch(tracers, [it[4] for it in items], executor=ex)
     for t, w_ in zip(tracers, want):
         assert np.array_equal(t.read_accum().view(np.uint32), w_.view(np.uint32))
+
+
+@pytest.mark.parametrize("mask", [0, 1])
+@pytest.mark.parametrize("nee", [0, 3])
+@pytest.mark.parametrize("which", ["materials", "layered", "alpha"])
+def test_nee_visibility_masks_bit_exact(pkg, oracle, which, nee, mask):
+    """The split plan's NEE results as per-slot visibility bits (1) or a
+    pending record per job (0): the oracle's accumulator either way."""
+    scene, env = _scene(pkg, which)
+    t = _tracer(pkg, scene, env)
+    t.set_tuning(mode=2, nee_variant=nee, trace_variant=4, wave_slots=333, wave_items=2000)
+    assert pkg._native.lib().oxpt_diag_set_nee_mask(t.ctx, mask) == 0
+    t.refine(6)
+    cpu, _ = oracle.render(t.prepared(), 6)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
