@@ -101,7 +101,7 @@ def parse():
     ap.add_argument("--nrc-spread", type=float, default=0.01, help="nrc workload: path-spread constant (0: every "
                     "path ends at the query bounce)")
     ap.add_argument("--workload", default="single",
-                    choices=["single", "batch", "cornell", "cornell16", "serve", "nrc", "prepare"],
+                    choices=["single", "batch", "cornell", "cornell16", "serve", "nrc", "prepare", "walk-sweep"],
                     help="single: the large scene (headline); batch: 64 mixed scenes in batched launches; "
                          "cornell: the reference's own Cornell benchmark shape (256^2, 8 bounces); "
                          "cornell16: the Cornell box at 256^2, 16 spp, 8 bounces, roulette from 3, seed 0, "
@@ -425,6 +425,14 @@ def run_cornell16(a):
     tune_log = []
     if not a.no_tune:
         tuner.tune(pt, spp=spp, repeats=3, log=tune_log)
+    if a.mode != "auto":
+        pt.set_tuning(mode={"mega": 0, "wave": 1, "split": 2}[a.mode])
+    if a.slots:
+        pt.set_tuning(wave_slots=a.slots)
+    if a.graphs >= 0:
+        pt.set_tuning(graphs=a.graphs)
+    if a.trace_variant >= 0:
+        pt.set_tuning(trace_variant=a.trace_variant)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     frames = max(20, a.steps)
     for _ in range(a.warmup):
@@ -497,6 +505,60 @@ def run_cornell16(a):
             "cpu_baseline": cpu, "gpu_launches": int(n1.value - n0.value), "clocks": clk.summary(),
             "plan": plan_of(pt), "tuner_trials": len(tune_log)}
     print(json.dumps(line), flush=True)
+
+
+def run_walk_sweep(a):
+    """Traversal-kernel sweep on the single large scene: per-launch CUDA-event
+    times of the extension and shadow kernels, summed over a `--spp` refine
+    of the frame (graphs off, so every launch is timed), for each traversal
+    variant (0-2 local-memory stacks at 6 / 8 / 10 blocks per SM; 3-5
+    shared-memory short stacks at 6 / 8 / 10), stack entries kept on chip and
+    staged top nodes, and the tolerance plan. One JSON line per point."""
+    import torch
+    torch.cuda.set_device(0)
+    __graft_entry__.build()
+    pkg = __graft_entry__.load_package()
+    L = pkg._native.lib()
+    from oxideav_render_vulkan_b200 import tuner
+    scene, env = workload(pkg, a)
+    t = pkg.GpuPathTracer(0)
+    t.set_environment(env)
+    t.sync(scene, options(pkg, a))
+    tuner.apply(t, tuner.LARGE_SCENE_PLAN)
+    t.set_tuning(graphs=0, wave_items=tuner.LARGE_SCENE_WAVE_ITEMS)
+    t.prepared()
+    ctx = t.ctx
+    spp = min(a.spp, 8)
+
+    def run(tv, lim, stage, closest=0):
+        t.set_tuning(trace_variant=tv, closest_walk=closest)
+        L.oxpt_diag_set_walk(ctx, lim, stage)
+        t.reset()
+        t.refine(spp)
+        t.finish()
+        L.oxpt_diag_set_timing(ctx, 1)
+        L.oxpt_diag_timing(ctx, None, None, None, None)
+        t.reset()
+        t.refine(spp)
+        t.finish()
+        L.oxpt_diag_timing(ctx, None, None, None, None)
+        L.oxpt_diag_set_timing(ctx, 0)
+        kms, kn = (C.c_double * 12)(), (C.c_uint64 * 12)()
+        L.oxpt_diag_timing_kinds(ctx, kms, kn)
+        line = {"workload": f"traversal sweep, single large scene 1920x1080, {spp} spp, graphs off",
+                "trace_variant": tv, "stack_entries_on_chip": lim, "staged_nodes": stage, "closest_walk": closest,
+                "extend_ms": kms[3], "shadow_ms": kms[4], "frame_kernels_ms": sum(kms[k] for k in (2, 3, 4, 5, 6))}
+        print(json.dumps(line), flush=True)
+
+    for tv in (0, 1, 2):
+        run(tv, 2, 0)
+    for tv in (3, 4, 5):
+        for lim in (0, 2, 4, 8, 16):
+            for stage in (0, 127, 511):
+                run(tv, lim, stage)
+    for tv in (3, 4):
+        for lim in (2, 8):
+            run(tv, lim, 0, closest=1)
 
 
 def _leaf_depth_sum(geom, nodes):
@@ -830,6 +892,9 @@ def main():
         return
     if a.workload == "cornell16":
         run_cornell16(a)
+        return
+    if a.workload == "walk-sweep":
+        run_walk_sweep(a)
         return
     if a.workload == "prepare":
         run_prepare(a)
