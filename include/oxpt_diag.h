@@ -116,9 +116,11 @@ oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* ctx, int on);
  *                  checks.
  *   shade_variant  wavefront logic kernel compiled for 2 / 3 / 4 resident
  *                  blocks per SM (0 / 1 / 2): registers against occupancy.
- *   trace_variant  wavefront traversal kernels for 6 / 8 / 10 blocks; 3-5:
- *                  shared-memory short stacks and staged top nodes, for
- *                  8 / 10 / 12 blocks.
+ *   trace_variant  wavefront traversal kernels: 0-2 with local-memory walk
+ *                  stacks for 6 / 8 / 10 blocks per SM; 3-5 with short
+ *                  stacks in shared memory, alpha tests out of line and
+ *                  optional staged top nodes (oxpt_diag_set_walk), for
+ *                  6 / 8 / 10 blocks. Default 4.
  *   nee_variant    split wavefront NEE kernel: job-major (0, 1, 2) or
  *                  vertex-major (3, 4, 5) for 4 / 5 / 6 blocks.
  *   OXPT_MODE_WAVEFRONT_SPLIT: the wavefront with the shading of a bounce

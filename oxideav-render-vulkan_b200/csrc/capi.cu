@@ -113,7 +113,7 @@ struct oxpt_ctx {
     uint32_t wave_slots = 1u << 20;
     uint64_t wave_items = oxd::DEFAULT_WAVE_ITEMS;
     uint32_t check_every = 4;
-    uint32_t shade_variant = 1, trace_variant = 0, nee_variant = 3, stack = 0;
+    uint32_t shade_variant = 1, trace_variant = 4, nee_variant = 3, stack = 0;
     uint32_t bvh_depth = 0;
     // four-wide any-hit tree (host/bvh4.cpp), built on upload when exact
     float4* bvh4 = nullptr;

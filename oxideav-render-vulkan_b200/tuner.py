@@ -29,7 +29,7 @@ TUNE_FIRST_SAMPLE = 1 << 30  # sample indices the tuner uses (not rendered by us
 class Plan:
     mode: int = N.MODE_WAVEFRONT
     shade_variant: int = 1
-    trace_variant: int = 0
+    trace_variant: int = 4
     stack: int = 0
     wave_slots: int = 1 << 20
     nee_variant: int = 3

@@ -205,9 +205,10 @@ def test_images_vs_libm_oracle_psnr_at_least_60db(pkg, oracle):
     assert psnr >= 60.0, psnr
 
 
+@pytest.mark.parametrize("tv", [0, 4])
 @pytest.mark.parametrize("mode,refill", [(0, 0), (1, 8), (2, 8), (1, 1), (2, 32), (2, 16)])
 @pytest.mark.parametrize("which", ["materials", "layered", "alpha"])
-def test_both_execution_modes_bit_exact(pkg, oracle, mode, refill, which):
+def test_both_execution_modes_bit_exact(pkg, oracle, mode, refill, which, tv):
     """Megakernel and wavefront plans give the oracle's accumulator, also
     with few wavefront slots (path regeneration), split launches and every
     traversal refill policy (lanes taking new rays while others walk)."""
@@ -220,7 +221,8 @@ def test_both_execution_modes_bit_exact(pkg, oracle, mode, refill, which):
                                     n_emissive=16, material_mix=1)
         env = pkg.EnvironmentMap.sky(64, 32)
     t = _tracer(pkg, scene, _opts(pkg, 40, 28, 6, bounces=10), env)
-    t.set_tuning(mode=mode, wave_slots=333, wave_items=2000, max_paths=2000, check_every=3, refill=refill)
+    t.set_tuning(mode=mode, wave_slots=333, wave_items=2000, max_paths=2000, check_every=3, refill=refill,
+                 trace_variant=tv)
     t.refine(6)
     gpu = t.read_accum()
     cpu, _ = oracle.render(t.prepared(), 6)
