@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--graphs", type=int, default=-1, choices=[-1, 0, 1],
                     help="override the plan's CUDA graphs (0: host-driven loop, e.g. for profilers that cannot "
                          "see kernels inside graphs with conditional nodes)")
+    ap.add_argument("--shadow-postpone", type=int, default=-1, choices=[-1, 0, 1],
+                    help="four-wide shadow walks park leaves until the warp has no node work (1) or not (0)")
     ap.add_argument("--nee-mask", type=int, default=-1, choices=[-1, 0, 1],
                     help="split plan's NEE results as per-slot visibility bits (1, default) or per-job records (0)")
     ap.add_argument("--nee-variant", type=int, default=-1, help="serve workload: the executor's NEE kernel "
@@ -529,6 +531,7 @@ def run_walk_sweep(a):
     t.prepared()
     ctx = t.ctx
     spp = min(a.spp, 8)
+    line_extra = {}
 
     def run(tv, lim, stage, closest=0):
         t.set_tuning(trace_variant=tv, closest_walk=closest)
@@ -548,6 +551,7 @@ def run_walk_sweep(a):
         line = {"workload": f"traversal sweep, single large scene 1920x1080, {spp} spp, graphs off",
                 "trace_variant": tv, "stack_entries_on_chip": lim, "staged_nodes": stage, "closest_walk": closest,
                 "extend_ms": kms[3], "shadow_ms": kms[4], "frame_kernels_ms": sum(kms[k] for k in (2, 3, 4, 5, 6))}
+        line.update(line_extra)
         print(json.dumps(line), flush=True)
 
     for tv in (0, 1, 2):
@@ -559,6 +563,17 @@ def run_walk_sweep(a):
     for tv in (3, 4):
         for lim in (2, 8):
             run(tv, lim, 0, closest=1)
+    # Refill threshold and postponed shadow leaves on the chosen kernels.
+    L.oxpt_diag_set_walk(ctx, 2, 0)
+    for post in (0, 1):
+        L.oxpt_diag_set_shadow_postpone(ctx, post)
+        for refill in (2, 4, 8, 16, 32):
+            t.set_tuning(refill=refill)
+            line_extra["refill"] = refill
+            line_extra["shadow_postpone"] = post
+            run(4, 2, 0)
+    L.oxpt_diag_set_shadow_postpone(ctx, 0)
+    line_extra.clear()
 
 
 def _leaf_depth_sum(geom, nodes):
@@ -954,6 +969,8 @@ def main():
         pt.set_tuning(graphs=a.graphs)
     if a.nee_mask >= 0:
         L.oxpt_diag_set_nee_mask(pt.ctx, a.nee_mask)
+    if a.shadow_postpone >= 0:
+        L.oxpt_diag_set_shadow_postpone(pt.ctx, a.shadow_postpone)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):

@@ -100,6 +100,12 @@ oxpt_status oxpt_diag_get_walk(const oxpt_ctx* ctx, uint32_t out[2]);
  * are stored, 0 = a pending record per job with a visibility word. The
  * logic kernel adds the same contributions in the same order either way. */
 oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* ctx, int on);
+/* Four-wide shadow walks of trace_variant 3-5: 1 = lanes park the leaves
+ * they reach and keep walking inner nodes, and the warp tests parked
+ * leaves together once no lane has node work left (speculative traversal);
+ * 0 (default) = each lane tests a leaf when it reaches it. Occlusion does
+ * not depend on the order, so results are the same. */
+oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* ctx, int on);
 
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left

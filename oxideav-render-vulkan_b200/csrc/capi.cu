@@ -124,6 +124,7 @@ struct oxpt_ctx {
     // split plan: per-slot visibility masks instead of a pending record per
     // NEE job (oxpt_diag_set_nee_mask; results are the same either way)
     bool nee_mask = true;
+    uint32_t shadow_post = 0;  // four-wide shadow walks with postponed leaves (oxpt_diag_set_shadow_postpone)
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
     // traversal variants 3-5: stack entries per lane kept in shared memory,
     // top nodes of the binary tree staged per CTA (oxpt_diag_set_walk)
@@ -441,6 +442,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const ox
     wa.nrc = nrc ? *nrc : oxd::NrcWave{};
     wa.walk_lim = c->walk_lim;
     wa.walk_stage = c->walk_stage;
+    wa.shadow_post = c->shadow_post;
     wa.closest4 = (c->closest_walk && c->trace_variant >= 3 && bvh4_usable(c)) ? 1u : 0u;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
@@ -1286,6 +1288,12 @@ oxpt_status oxpt_diag_set_walk(oxpt_ctx* c, uint32_t stack_entries, uint32_t sta
     return OXPT_OK;
 }
 
+oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* c, int on) {
+    if (!c) return OXPT_E_INVALID;
+    c->shadow_post = on ? 1u : 0u;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* c, int on) {
     if (!c) return OXPT_E_INVALID;
     c->nee_mask = on != 0;
@@ -1590,7 +1598,8 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
         // node words (one-scene batches), the walk's storage split and tree.
         const oxd::WaveArgs& a0 = args[0];
         key.insert(key.end(), {(uint64_t)(uintptr_t)a0.s.geom, a0.s.geom_vec4, a0.s.P.env[3], a0.one_scene,
-                               a0.closest4, a0.walk_lim, a0.walk_stage, (uint64_t)(uintptr_t)a0.st.vis});
+                               a0.closest4, a0.walk_lim, a0.walk_stage, (uint64_t)(uintptr_t)a0.st.vis,
+                               a0.shadow_post});
     }
     for (size_t k = 0; k < rounds.size(); k++) {
         const oxd::WaveArgs& wa = args[k];
@@ -1849,6 +1858,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.refill = e->refill;
         wa.walk_lim = e->walk_lim;
         wa.walk_stage = e->walk_stage;
+        wa.shadow_post = e->shadow_post;
         wa.closest4 = closest4 ? 1u : 0u;
         wa.total = total;
         wa.out = e->out;

@@ -309,6 +309,145 @@ __device__ __forceinline__ bool walk4s_step(const Scene* sp_, uint32_t* stack_wo
 }
 
 // ---------------------------------------------------------------------
+// Four-wide any-hit walk with postponed leaves (Aila & Laine 2009,
+// "Understanding the efficiency of ray traversal on GPUs": speculative
+// traversal). A lane that reaches a leaf parks it and goes on with inner
+// nodes; the warp tests leaves only in steps where no lane has node work
+// left (every lane has parked a leaf and met a second one, or has run out
+// of nodes), so node steps and leaf steps are not interleaved within a
+// warp. Occlusion is order-free, so the answer is walk4s_step's; only
+// steps that visit a node or test a leaf count against the guard (a lane
+// waiting for the leaf step is not walking).
+// ---------------------------------------------------------------------
+template <int SS, int SD>
+struct Walk4P {
+    float t_max;
+    uint32_t cur, pend, sp, guard;
+    bool hit_any;
+    uint32_t deep[SD];
+};
+
+template <int SS, int SD>
+__device__ __forceinline__ bool walk4p_begin(const Scene& s, const Ray& r, float t_max, Walk4P<SS, SD>& w) {
+    w.hit_any = false;
+    if (!r.valid || s.bvh4_root == NONE) return false;
+    w.t_max = t_max;
+    w.cur = s.bvh4_root;
+    w.pend = NONE;
+    w.sp = 0u;
+    w.guard = 4u * s.bvh4_nodes + 8u;
+    return true;
+}
+
+// Whether the lane can take a node step now.
+template <int SS, int SD>
+__device__ __forceinline__ bool walk4p_node_work(const Walk4P<SS, SD>& w) {
+    return w.cur != NONE && !((w.cur & 0x80000000u) && w.pend != NONE);
+}
+
+template <bool COUNT, int SS, int SD, int NT>
+__device__ __forceinline__ bool walk4p_step(const Scene* sp_, uint32_t* stack_words, uint32_t lim, const Ray& r,
+                                            uint32_t path_seed, uint32_t ray_id, bool primary, uint32_t skip,
+                                            bool leaf_step, Walk4P<SS, SD>& w, Cnt& cnt, uint32_t* err) {
+    const Scene& s = *sp_;
+    const uint32_t lane = threadIdx.x;
+    if (leaf_step) {
+        if (w.pend != NONE) {
+            if (w.guard-- == 0u) {
+                atomicOr(err, 1u);
+                return true;
+            }
+            bump<COUNT>(cnt, C_LEAVES);
+            const uint32_t lf = w.pend;
+            w.pend = NONE;
+            uint32_t first = lf & 0x07ffffffu, end = first + ((lf >> 27) & 15u) + 1u;
+            if ((uint64_t)end > s.slot_count) {
+                atomicOr(err, 2u);
+                return true;
+            }
+            for (uint32_t slot = first; slot < end; slot++) {
+                bump<COUNT>(cnt, C_TRIS);
+                uint64_t tb = tri_base(s, slot);
+                float4 q0 = geomv(s, tb), q1 = geomv(s, tb + 1), q2 = geomv(s, tb + 2);
+                Hit h;
+                if (!intersect(r, q0, q1, q2, w.t_max, &h)) continue;
+                uint32_t gid = __float_as_uint(q0.w);
+                if (gid == skip) continue;
+                uint32_t m = __float_as_uint(q2.w);
+                if (!accept_ol(sp_, slot, m, gid, h, path_seed, ray_id, primary)) continue;
+                w.hit_any = true;
+                return true;
+            }
+        }
+        return w.cur == NONE && w.pend == NONE;
+    }
+    uint32_t cur = w.cur;
+    if (cur == NONE) return w.pend == NONE;
+    if (cur & 0x80000000u) {
+        if (w.pend != NONE) return false;  // parked: waits for the leaf step
+        w.pend = cur;
+    } else {
+        if (w.guard-- == 0u) {
+            atomicOr(err, 1u);
+            return true;
+        }
+        if (cur >= s.bvh4_nodes) {
+            atomicOr(err, 1u);
+            return true;
+        }
+        bump<COUNT>(cnt, C_BOXES, 4);
+        const float4* nd = s.bvh4 + (uint64_t)cur * 8u;
+        float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+        float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+        uint4 rf = __ldg(reinterpret_cast<const uint4*>(nd) + 6);
+        uint32_t ref[4] = {rf.x, rf.y, rf.z, rf.w};
+        float t[4];
+        t[0] = rf.x == NONE ? -1.0f : slab6(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, w.t_max);
+        t[1] = rf.y == NONE ? -1.0f : slab6(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, w.t_max);
+        t[2] = rf.z == NONE ? -1.0f : slab6(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, w.t_max);
+        t[3] = rf.w == NONE ? -1.0f : slab6(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, w.t_max);
+        int best = -1;
+        float bt = 0.0f;
+        uint32_t bref = NONE;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (t[k] >= 0.0f && (best < 0 || t[k] < bt)) {
+                best = k;
+                bt = t[k];
+                bref = ref[k];
+            }
+        if (best >= 0) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (k == best || !(t[k] >= 0.0f)) continue;
+                if (w.sp >= (uint32_t)SD) {  // excluded on upload
+                    atomicOr(err, 4u);
+                    return true;
+                }
+                if (w.sp < lim) stack_words[w.sp * NT + lane] = ref[k];
+                else w.deep[w.sp] = ref[k];
+                w.sp++;
+            }
+            // A leaf child is parked at once when the lane has none parked.
+            if ((bref & 0x80000000u) && w.pend == NONE) w.pend = bref;
+            else {
+                w.cur = bref;
+                return false;
+            }
+        }
+    }
+    // Next node (or leaf) from the stack; none left: only the parked leaf.
+    if (w.sp == 0u) {
+        w.cur = NONE;
+        return w.pend == NONE;
+    }
+    bump<COUNT>(cnt, C_POPS);
+    --w.sp;
+    w.cur = w.sp < lim ? stack_words[w.sp * NT + lane] : w.deep[w.sp];
+    return false;
+}
+
+// ---------------------------------------------------------------------
 // Four-wide closest-hit walk (the tolerance plan, not the reference's
 // order). Per inner node the four child boxes are slab-tested against the
 // current t_max; the nearest passing child is taken next and the others

@@ -235,6 +235,71 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ 
             if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
 }
 
+// Shadow rays over the four-wide tree with postponed leaves (walk4p_step):
+// per step the warp takes node steps while any lane has node work, and a
+// leaf step (every parked leaf tested) when none has.
+template <bool COUNT, int MINB, int SD, bool BATCH>
+__global__ void __launch_bounds__(NT, MINB) walk_shadow4p(const __grid_constant__ WaveArgs a, uint32_t staged,
+                                                          uint32_t lim) {
+    Cnt cnt;
+    if (COUNT)
+        for (int k = 0; k < C_N; k++) cnt.c[k] = 0;
+    (void)staged;
+    const uint32_t n = *((volatile uint32_t*)&a.ctr[1]);
+    bool active = false, warp_drained = false;
+    uint32_t slot = 0u, job = 0u, rid = 0u, skip = NONE, path_seed = 0u;
+    const Scene* sc = &a.s;
+    Ray r;
+    Walk4P<SS4, SD> w;
+    for (;;) {
+        const unsigned act = __ballot_sync(FULL, active);
+        if (act == 0u && warp_drained) break;
+        if (!warp_drained && 32 - __popc(act) >= (act ? a.refill : 1u)) {
+            bool none_left = false;
+            if (!active) {
+                uint32_t q = append(&a.ctr[6]);
+                if (q < n) {
+                    float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
+                    uint4 m = a.q.sh_m[q];
+                    slot = m.x;
+                    job = m.y;
+                    rid = m.z;
+                    path_seed = m.w;
+                    skip = __float_as_uint(d.w);
+                    if (BATCH) sc = &a.frames[a.st.frame[slot]].s;
+                    bump<COUNT>(cnt, C_SHADOW_RAYS);
+                    r = make_ray(xyz(o), xyz(d));
+                    if (walk4p_begin<SS4, SD>(*sc, r, o.w, w)) active = true;
+                    else mark_visible(a.st, a.jobs, slot, job);  // nothing in the way
+                } else {
+                    none_left = true;
+                }
+            }
+            warp_drained = __any_sync(FULL, none_left);
+        }
+#pragma unroll 1
+        for (int st = 0; st < STEPS; st++) {
+            const bool leaf_step = __ballot_sync(FULL, active && walk4p_node_work(w)) == 0u;
+            if (!active) continue;
+            if (walk4p_step<COUNT, SS4, SD, NT>(sc, walk_smem, lim, r, path_seed, rid, false, skip, leaf_step, w, cnt,
+                                                a.err)) {
+                active = false;
+                if (!w.hit_any) mark_visible(a.st, a.jobs, slot, job);
+            }
+        }
+    }
+    if (COUNT)
+        for (int c = 0; c < C_N; c++)
+            if (cnt.c[c]) atomicAdd(a.counters + c, cnt.c[c]);
+}
+
+template <bool C, int SD, bool B>
+void* shadow4p_fn(int v) {
+    if (v == 0) return (void*)walk_shadow4p<C, 6, SD, B>;
+    if (v == 1) return (void*)walk_shadow4p<C, 8, SD, B>;
+    return (void*)walk_shadow4p<C, 10, SD, B>;
+}
+
 template <bool C, int SD, bool B>
 void* ext_fn(int v) {
     if (v == 0) return (void*)walk_extend<C, 6, SD, B>;
@@ -257,23 +322,25 @@ void* shadow_fn(int v) {
 }
 
 template <bool C, bool B>
-void* kernel_c(bool ext, bool four, int v, int sd) {
+void* kernel_c(bool ext, bool four, bool post, int v, int sd) {
     if (ext && four) return sd <= 32 ? ext4_fn<C, 32, B>(v) : ext4_fn<C, 64, B>(v);
+    if (four && post) return sd <= 32 ? shadow4p_fn<C, 32, B>(v) : shadow4p_fn<C, 64, B>(v);
     if (ext) return sd <= 32 ? ext_fn<C, 32, B>(v) : ext_fn<C, 64, B>(v);
     if (four) return sd <= 32 ? shadow_fn<C, 32, true, B>(v) : shadow_fn<C, 64, true, B>(v);
     return sd <= 32 ? shadow_fn<C, 32, false, B>(v) : shadow_fn<C, 64, false, B>(v);
 }
 
-void* kernel_of(bool count, bool batch, bool ext, bool four, int v, int sd) {
-    if (batch) return count ? nullptr : kernel_c<false, true>(ext, four, v, sd);
-    return count ? kernel_c<true, false>(ext, four, v, sd) : kernel_c<false, false>(ext, four, v, sd);
+void* kernel_of(bool count, bool batch, bool ext, bool four, bool post, int v, int sd) {
+    if (batch) return count ? nullptr : kernel_c<false, true>(ext, four, post, v, sd);
+    return count ? kernel_c<true, false>(ext, four, post, v, sd) : kernel_c<false, false>(ext, four, post, v, sd);
 }
 
 const int TARGET_BLOCKS[3] = {6, 8, 10};
 
 }  // namespace
 
-// ext && four: closest hits over the four-wide tree (walk_extend4).
+// ext && four: closest hits over the four-wide tree (walk_extend4);
+// !ext && four && a.shadow_post: shadow rays with postponed leaves.
 // variant 0..2: 6 / 8 / 10 resident blocks per SM targeted. a.walk_lim
 // stack entries per lane (at most the walk's SS) live in shared memory;
 // binary walks of launches over one scene (a plain launch, or a batch
@@ -283,7 +350,7 @@ const int TARGET_BLOCKS[3] = {6, 8, 10};
 cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int variant, int sd, int sms,
                         cudaStream_t st) {
     variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant);
-    void* fn = kernel_of(count, a.nframes > 0, ext, four, variant, sd);
+    void* fn = kernel_of(count, a.nframes > 0, ext, four, a.shadow_post != 0u, variant, sd);
     if (!fn) return cudaErrorInvalidValue;
     const uint32_t target = (uint32_t)TARGET_BLOCKS[variant];
     const uint32_t words = four ? (ext ? 2u : 1u) : 3u;

@@ -147,6 +147,9 @@ struct WaveArgs {
     // continuation rays walk the four-wide tree (traversal variants 3-5;
     // the tolerance plan: closest hits equal except near-ties)
     uint32_t closest4 = 0u;
+    // four-wide shadow walks of variants 3-5 park leaves until the warp
+    // has no node work (same occlusion, fewer mixed node/leaf steps)
+    uint32_t shadow_post = 0u;
 };
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3
