@@ -9,8 +9,11 @@
 // shading normal and roughness, encoded by 12 sine / cosine frequencies
 // each; the loss is the relative L2 (y - t)^2 / (sg(y)^2 + 0.01).
 //
-// Kernels (one warpgroup per CTA, 128 samples per tile, persistent grids):
-//   nrc_forward   encodes a tile into shared memory, then per layer issues
+// Kernels (128 samples per tile, persistent grids):
+//   nrc_forward   two warpgroups per CTA on alternate tiles, each with its
+//                 own operand tiles and TMEM columns, so one issues MMAs
+//                 while the other encodes and activates; a warpgroup
+//                 encodes a tile into shared memory, then per layer issues
 //                 tcgen05.mma over the K slices (A = activations, B = the
 //                 layer's weights, both resident in shared memory), waits
 //                 on an mbarrier, reads the 128 x N FP32 accumulator from
@@ -43,11 +46,15 @@ using umma::cm_offset;
 // ---------------------------------------------------------------------
 // Shared-memory plans.
 // ---------------------------------------------------------------------
+// Forward: the weights once, then per warpgroup (two per CTA) its own
+// 128 x 256 encoded-input tile and 128 x 64 hidden tile.
 constexpr uint32_t FWD_W = W_BYTES;                 // forward weights, all layers
-constexpr uint32_t FWD_A0 = FWD_W;                  // 128 x 256 encoded inputs
-constexpr uint32_t FWD_H = FWD_A0 + TILE * IN * 2;  // 128 x 64 hidden
-constexpr uint32_t FWD_BAR = FWD_H + TILE * HID * 2;
+constexpr uint32_t FWD_WG = TILE * IN * 2 + TILE * HID * 2;
+__host__ __device__ constexpr uint32_t fwd_a0(uint32_t wg) { return FWD_W + wg * FWD_WG; }
+__host__ __device__ constexpr uint32_t fwd_h(uint32_t wg) { return fwd_a0(wg) + TILE * IN * 2; }
+constexpr uint32_t FWD_BAR = FWD_W + 2 * FWD_WG;     // two mbarriers, then the TMEM slot
 constexpr uint32_t FWD_SMEM = FWD_BAR + 64;
+constexpr uint32_t FWD_THREADS = 2 * TILE;
 
 constexpr uint32_t BWD_WT = 0;                             // transposed weights, layers 1..4
 constexpr uint32_t BWD_GCM = BWD_WT + WT_BYTES;            // gradient operand: rows = samples, 128 x 64
@@ -153,45 +160,80 @@ __device__ __forceinline__ void read_row(uint32_t tmem, uint32_t cols, float* v)
     for (uint32_t c = 0; c < cols; c += 16) umma::tmem_ld16(base + c, v + c);
 }
 
-__global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ Args a) {
+// Warpgroup-local synchronisation (named barriers 1 and 2; 0 is the CTA's).
+__device__ __forceinline__ void wg_sync(uint32_t id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool wg_all(uint32_t id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0u;
+}
+__device__ __forceinline__ void publish_smem_wg(uint32_t id) {
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    wg_sync(id);
+    umma::fence_after_sync();
+}
+__device__ __forceinline__ bool await_mma_wg(uint32_t id, uint64_t* bar, uint32_t* phase, uint32_t* err) {
+    bool ok = umma::bar_wait(bar, *phase, WAIT_LIMIT);
+    *phase ^= 1u;
+    umma::fence_after_sync();
+    if (!ok) atomicOr(err, 16u);
+    return wg_all(id, ok);
+}
+
+// Two warpgroups per CTA take alternate tiles, each with its own operand
+// tiles, mbarrier and 64 TMEM columns: while one waits for its MMAs the
+// other encodes, reads back and activates, so the tensor core and the
+// CUDA cores work on different tiles at once. Warp w reads TMEM lanes
+// 32 (w mod 4) .. +31, the rows of its warpgroup's tile.
+__global__ void __launch_bounds__(FWD_THREADS, 1) nrc_forward(const __grid_constant__ Args a) {
     extern __shared__ __align__(1024) char smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + FWD_BAR);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + FWD_BAR + 8);
-    const uint32_t t = threadIdx.x;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + FWD_BAR + 16);
+    const uint32_t wg = threadIdx.x >> 7, t = threadIdx.x & 127u;
+    const uint32_t bid = 1u + wg;  // this warpgroup's named barrier
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + FWD_BAR) + wg;
     // Weights: a straight copy of the core-matrix image.
-    for (uint32_t i = t; i < FWD_W / 16; i += TILE)
+    for (uint32_t i = threadIdx.x; i < FWD_W / 16; i += FWD_THREADS)
         reinterpret_cast<uint4*>(smem)[i] = reinterpret_cast<const uint4*>(a.wf)[i];
     if (t == 0) umma::bar_init(bar, 1);
-    if (t < 32) umma::tmem_alloc(tslot, 64);
+    if (threadIdx.x < 32) umma::tmem_alloc(tslot, 128);
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    const uint32_t tmem = *tslot;
-    const uint32_t s_w = umma::smem_addr(smem), s_a0 = s_w + FWD_A0, s_h = s_w + FWD_H;
+    const uint32_t tmem = *tslot + wg * 64u;
+    const uint32_t lanes = ((threadIdx.x >> 5) & 3u) * 32u;
+    const uint32_t s_w = umma::smem_addr(smem), s_a0 = s_w + fwd_a0(wg), s_h = s_w + fwd_h(wg);
+    char* a0_tile = smem + fwd_a0(wg);
+    char* h_tile = smem + fwd_h(wg);
     uint32_t phase = 0;
     const uint32_t n = count_of(a);
     const float grad_scale = a.grad_scale != 0.0f ? a.grad_scale : 1.0f / (3.0f * (float)(n ? n : 1u));
     const uint32_t tiles = (n + TILE - 1) / TILE;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (uint32_t tile = 2u * blockIdx.x + wg; tile < tiles; tile += 2u * gridDim.x) {
         const uint32_t s = tile * TILE + t;
         float f[IN];
         encode(a.in, s, n, f);
-        put_row<IN>(smem + FWD_A0, t, f);
-        publish_smem();
+        put_row<IN>(a0_tile, t, f);
+        publish_smem_wg(bid);
         bool ok = true;
         float v[HID];
         for (int l = 0; l < LAYERS && ok; l++) {
             const uint32_t K = l == 0 ? IN : HID, N = l == LAYERS - 1 ? OUT_PAD : HID;
             if (t == 0) layer_mma(tmem, l == 0 ? s_a0 : s_h, s_w + W_OFF(l), K, N, bar);
-            ok = await_mma(bar, &phase, a.err);
+            ok = await_mma_wg(bid, bar, &phase, a.err);
             if (!ok) break;
-            read_row(tmem, N, v);
+            for (uint32_t c = 0; c < N; c += 16) umma::tmem_ld16(tmem + (lanes << 16) + c, v + c);
             if (l < LAYERS - 1) {
 #pragma unroll
                 for (int k = 0; k < HID; k++) v[k] = fmaxf(v[k], 0.0f);
                 umma::fence_before_sync();
-                __syncthreads();  // every row read before the next MMA overwrites D
-                put_row<HID>(smem + FWD_H, t, v);
+                wg_sync(bid);  // every row read before the next MMA overwrites D
+                put_row<HID>(h_tile, t, v);
                 if (a.acts && s < n) {
                     uint4* dst = reinterpret_cast<uint4*>(a.acts + ((size_t)s * (LAYERS - 1) + l) * HID);
 #pragma unroll
@@ -200,7 +242,7 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
                                              pack_bf16(v[8 * kb + 4], v[8 * kb + 5]),
                                              pack_bf16(v[8 * kb + 6], v[8 * kb + 7]));
                 }
-                publish_smem();
+                publish_smem_wg(bid);
             }
         }
         if (!ok) break;
@@ -241,13 +283,13 @@ __global__ void __launch_bounds__(TILE, 1) nrc_forward(const __grid_constant__ A
             if ((t & 31) == 0 && loss != 0.0f) atomicAdd(a.loss, loss);
         }
         umma::fence_before_sync();
-        __syncthreads();  // D and A0 are reused by the next tile
+        wg_sync(bid);  // D and A0 are reused by this warpgroup's next tile
         umma::fence_after_sync();
     }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    if (t < 32) umma::tmem_free(tmem, 64);
+    if (threadIdx.x < 32) umma::tmem_free(*tslot, 128);
 }
 
 // Writes column r (one sample) of a K-major core-matrix tile whose rows
@@ -463,8 +505,9 @@ cudaError_t launch_forward(const Args& a, int sms, cudaStream_t st) {
     }
     uint32_t tiles = (a.n + TILE - 1) / TILE;
     if (tiles == 0) return cudaSuccess;
-    uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
-    nrc_forward<<<grid, TILE, FWD_SMEM, st>>>(a);
+    uint32_t pairs = (tiles + 1) / 2;
+    uint32_t grid = pairs < (uint32_t)sms ? pairs : (uint32_t)sms;
+    nrc_forward<<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
     return cudaGetLastError();
 }
 
