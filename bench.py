@@ -861,6 +861,31 @@ def run_nrc(a):
     nrc_curve = progress(nt, lambda n: cache.refine(n), untrained)
     q, smp = cache.frame_counts()
 
+    # Where a frame's time goes (CUDA events per launch, 8 more frames of
+    # each; the plain tracer without its graph so its launches are timed).
+    L = pkg._native.lib()
+    names = {0: "trace", 1: "reduce", 2: "logic", 3: "extend", 4: "shadow", 5: "shade", 6: "nee",
+             7: "cache_inference", 8: "cache_train_forward", 9: "cache_backward"}
+
+    def breakdown(t, fn, frames=8):
+        t.finish()
+        L.oxpt_diag_set_timing(t.ctx, 1)
+        L.oxpt_diag_timing(t.ctx, None, None, None, None)
+        fn(frames)
+        t.finish()
+        L.oxpt_diag_timing(t.ctx, None, None, None, None)
+        L.oxpt_diag_set_timing(t.ctx, 0)
+        kms, kn = (C.c_double * 12)(), (C.c_uint64 * 12)()
+        L.oxpt_diag_timing_kinds(t.ctx, kms, kn)
+        return {names[k]: kms[k] / frames for k in names if kn[k] and k != 0}
+
+    cache_ms = breakdown(nt, lambda n: cache.refine(n))
+    del nt, cache
+    plain2 = tracer()
+    plain2.set_tuning(wave_slots=1 << 21)
+    plain_ms = breakdown(plain2, lambda n: [plain2.refine(1) for _ in range(n)])
+    del plain2
+
     def time_to(curve, db):
         prev = None
         for p in curve:
@@ -890,7 +915,8 @@ def run_nrc(a):
             "plain_seconds_to_35db": tp, "ratio_to_plain": (tn / tp) if (tn and tp) else None,
             "plain_ms_per_frame": frame_ms(plain_curve), "cache_ms_per_frame": frame_ms(nrc_curve),
             "plain": plain_curve, "cache": nrc_curve,
-            "last_frame_queries": q, "last_frame_training_samples": smp}
+            "last_frame_queries": q, "last_frame_training_samples": smp,
+            "kernel_ms_per_frame": {"plain": plain_ms, "cache": cache_ms}}
     print(json.dumps(line), flush=True)
 
 
