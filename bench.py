@@ -82,6 +82,8 @@ def parse():
                          "see kernels inside graphs with conditional nodes)")
     ap.add_argument("--shadow-postpone", type=int, default=-1, choices=[-1, 0, 1],
                     help="four-wide shadow walks park leaves until the warp has no node work (1) or not (0)")
+    ap.add_argument("--ray-order", type=int, default=-1, choices=[-1, 0, 1],
+                    help="reorder the continuation rays by origin cell and direction octant before the walk (1)")
     ap.add_argument("--nee-mask", type=int, default=-1, choices=[-1, 0, 1],
                     help="split plan's NEE results as per-slot visibility bits (1, default) or per-job records (0)")
     ap.add_argument("--nee-variant", type=int, default=-1, help="serve workload: the executor's NEE kernel "
@@ -550,7 +552,8 @@ def run_walk_sweep(a):
         L.oxpt_diag_timing_kinds(ctx, kms, kn)
         line = {"workload": f"traversal sweep, single large scene 1920x1080, {spp} spp, graphs off",
                 "trace_variant": tv, "stack_entries_on_chip": lim, "staged_nodes": stage, "closest_walk": closest,
-                "extend_ms": kms[3], "shadow_ms": kms[4], "frame_kernels_ms": sum(kms[k] for k in (2, 3, 4, 5, 6))}
+                "extend_ms": kms[3], "shadow_ms": kms[4], "order_ms": kms[10],
+                "frame_kernels_ms": sum(kms[k] for k in (2, 3, 4, 5, 6, 10))}
         line.update(line_extra)
         print(json.dumps(line), flush=True)
 
@@ -573,6 +576,13 @@ def run_walk_sweep(a):
             line_extra["shadow_postpone"] = post
             run(4, 2, 0)
     L.oxpt_diag_set_shadow_postpone(ctx, 0)
+    line_extra.clear()
+    # Continuation rays reordered before the closest-hit walk.
+    L.oxpt_diag_set_ray_order(ctx, 1)
+    line_extra["ray_order"] = 1
+    run(4, 2, 0)
+    run(4, 2, 0, closest=1)
+    L.oxpt_diag_set_ray_order(ctx, 0)
     line_extra.clear()
 
 
@@ -997,6 +1007,8 @@ def main():
         L.oxpt_diag_set_nee_mask(pt.ctx, a.nee_mask)
     if a.shadow_postpone >= 0:
         L.oxpt_diag_set_shadow_postpone(pt.ctx, a.shadow_postpone)
+    if a.ray_order >= 0:
+        L.oxpt_diag_set_ray_order(pt.ctx, a.ray_order)
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):

@@ -72,7 +72,7 @@ oxpt_status oxpt_diag_timing(oxpt_ctx* ctx, double* trace_ms, uint64_t* trace_la
  * ordered reduce, 2 wavefront logic, 3 wavefront extension traversal, 4
  * wavefront shadow traversal, 5 split-wavefront shading, 6 split-wavefront
  * NEE, 7 radiance-cache inference, 8 cache training forward, 9 cache
- * backward; 10, 11 unused. */
+ * backward, 10 continuation-ray reordering; 11 unused. */
 oxpt_status oxpt_diag_timing_kinds(const oxpt_ctx* ctx, double ms[12], uint64_t n[12]);
 /* The last oxpt_diag_refine_counted totals split by ray kind: out[0..7] for
  * continuation rays and shading (wavefront logic + extension), out[8..15]
@@ -106,6 +106,12 @@ oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* ctx, int on);
  * 0 (default) = each lane tests a leaf when it reaches it. Occlusion does
  * not depend on the order, so results are the same. */
 oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* ctx, int on);
+/* Wavefront plans: 1 = before the closest-hit walk, the continuation rays
+ * are reordered (counting sort on direction octant and a 16^3 Morton cell
+ * of the origin in the scene's root box) so that a warp walks similar
+ * rays; 0 (default) = queue order. Each ray is walked alone by one lane, so
+ * results are the same either way. Its launches time as kind 10. */
+oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* ctx, int on);
 
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left

@@ -125,6 +125,7 @@ struct oxpt_ctx {
     // NEE job (oxpt_diag_set_nee_mask; results are the same either way)
     bool nee_mask = true;
     uint32_t shadow_post = 0;  // four-wide shadow walks with postponed leaves (oxpt_diag_set_shadow_postpone)
+    uint32_t ray_order = 0;    // continuation queue reordered before the walk (oxpt_diag_set_ray_order)
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
     // traversal variants 3-5: stack entries per lane kept in shared memory,
     // top nodes of the binary tree staged per CTA (oxpt_diag_set_walk)
@@ -356,8 +357,8 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     size_t sizes[] = {P * 8, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 4, P * 4,
                       PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64,
                       split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0, P * 4,
-                      (split && jobs <= 32) ? P * 4 : 0};
-    constexpr int NB = 22;
+                      (split && jobs <= 32) ? P * 4 : 0, P * 4, P * 4, P * 4, (size_t)(1u << 15) * 4};
+    constexpr int NB = 26;
     size_t total = 0;
     for (size_t s : sizes) total += align256(s);
     if (slots > c->wave_cap_slots || jobs > c->wave_cap_jobs || total > c->wave_bytes) {
@@ -397,6 +398,10 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     st->pend = (float4*)ptr[11];
     st->frame = (uint32_t*)ptr[20];
     st->vis = (split && jobs <= 32 && c->nee_mask) ? (uint32_t*)ptr[21] : nullptr;
+    q->ext_sorted = (uint32_t*)ptr[22];
+    q->ord_key = (uint32_t*)ptr[23];
+    q->ord_rank = (uint32_t*)ptr[24];
+    q->ord_hist = (uint32_t*)ptr[25];
     q->ext = (uint32_t*)ptr[12];
     q->sh_o = (float4*)ptr[13];
     q->sh_d = (float4*)ptr[14];
@@ -443,6 +448,7 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const ox
     wa.walk_lim = c->walk_lim;
     wa.walk_stage = c->walk_stage;
     wa.shadow_post = c->shadow_post;
+    wa.ray_order = c->ray_order;
     wa.closest4 = (c->closest_walk && c->trace_variant >= 3 && bvh4_usable(c)) ? 1u : 0u;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
@@ -488,7 +494,14 @@ int enqueue_iteration(oxpt_ctx* c, const oxd::WaveArgs& wa, const oxd::WaveArgs&
     } else {
         run(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, st); });
     }
-    run(3, [&] { return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, wa.closest4 ? sd4 : sd, c->sms, st); });
+    if (wa.ray_order) {
+        run(10, [&] { return oxd::launch_order_ext(wa, c->sms, st); });
+        oxd::WaveArgs wo = wa;
+        wo.q.ext = wa.q.ext_sorted;
+        run(3, [&] { return oxd::launch_wave_extend(wo, count, (int)c->trace_variant, wa.closest4 ? sd4 : sd, c->sms, st); });
+    } else {
+        run(3, [&] { return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, wa.closest4 ? sd4 : sd, c->sms, st); });
+    }
     run(4, [&] {
         return oxd::launch_wave_shadow(wsh, count, four, (int)c->trace_variant, four ? sd4 : sd, c->sms, st);
     });
@@ -1288,6 +1301,12 @@ oxpt_status oxpt_diag_set_walk(oxpt_ctx* c, uint32_t stack_entries, uint32_t sta
     return OXPT_OK;
 }
 
+oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* c, int on) {
+    if (!c) return OXPT_E_INVALID;
+    c->ray_order = on ? 1u : 0u;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* c, int on) {
     if (!c) return OXPT_E_INVALID;
     c->shadow_post = on ? 1u : 0u;
@@ -1599,7 +1618,7 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
         const oxd::WaveArgs& a0 = args[0];
         key.insert(key.end(), {(uint64_t)(uintptr_t)a0.s.geom, a0.s.geom_vec4, a0.s.P.env[3], a0.one_scene,
                                a0.closest4, a0.walk_lim, a0.walk_stage, (uint64_t)(uintptr_t)a0.st.vis,
-                               a0.shadow_post});
+                               a0.shadow_post, a0.ray_order});
     }
     for (size_t k = 0; k < rounds.size(); k++) {
         const oxd::WaveArgs& wa = args[k];
@@ -1859,6 +1878,7 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.walk_lim = e->walk_lim;
         wa.walk_stage = e->walk_stage;
         wa.shadow_post = e->shadow_post;
+        wa.ray_order = e->ray_order;
         wa.closest4 = closest4 ? 1u : 0u;
         wa.total = total;
         wa.out = e->out;

@@ -167,3 +167,38 @@ def test_postponed_leaf_shadow_walk_in_a_batch(pkg):
     pkg.refine_batch(tracers, [it[4] for it in items], executor=ex)
     for t, w_ in zip(tracers, want):
         assert np.array_equal(t.read_accum().view(np.uint32), w_.view(np.uint32))
+
+
+@pytest.mark.parametrize("variant", [0, 4])
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("which", ["materials", "alpha", "layered"])
+def test_reordered_continuation_rays_bit_exact(pkg, oracle, which, mode, variant):
+    """Continuation rays sorted by origin cell and direction octant before
+    the closest-hit walk: every ray is walked alone, so the accumulator is
+    the oracle's bit for bit."""
+    scene, env = _scene(pkg, which)
+    t = _tracer(pkg, scene, env)
+    t.set_tuning(mode=mode, trace_variant=variant, wave_slots=333, wave_items=2000)
+    assert pkg._native.lib().oxpt_diag_set_ray_order(t.ctx, 1) == 0
+    t.refine(6)
+    cpu, _ = oracle.render(t.prepared(), 6)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
+
+
+def test_reordered_continuation_rays_in_a_graph_batch(pkg):
+    items = [(scenes.materials_scene(pkg), None, 40, 28, 4), _scene(pkg, "layered") + (48, 32, 5)]
+    tracers, want = [], []
+    for scene, env, w, h, spp in items:
+        alone = _tracer(pkg, scene, env, w, h, spp)
+        alone.refine(spp)
+        want.append(alone.read_accum())
+        tracers.append(_tracer(pkg, scene, env, w, h, spp))
+    ex = pkg.GpuPathTracer(0)
+    ex.set_tuning(mode=2, trace_variant=4, wave_slots=500, graphs=1)
+    assert pkg._native.lib().oxpt_diag_set_ray_order(ex.ctx, 1) == 0
+    for _ in range(2):  # the second step reuses the graph
+        for t in tracers:
+            t.reset()
+        pkg.refine_batch(tracers, [it[4] for it in items], executor=ex)
+        for t, w_ in zip(tracers, want):
+            assert np.array_equal(t.read_accum().view(np.uint32), w_.view(np.uint32))
