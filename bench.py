@@ -82,8 +82,9 @@ def parse():
                          "see kernels inside graphs with conditional nodes)")
     ap.add_argument("--shadow-postpone", type=int, default=-1, choices=[-1, 0, 1],
                     help="four-wide shadow walks park leaves until the warp has no node work (1) or not (0)")
-    ap.add_argument("--ray-order", type=int, default=-1, choices=[-1, 0, 1],
-                    help="reorder the continuation rays by origin cell and direction octant before the walk (1)")
+    ap.add_argument("--ray-order", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
+                    help="reorder ray queues before the walks: 1 continuation rays (origin cell, direction "
+                         "octant), 2 shadow rays (light, origin cell), 3 both")
     ap.add_argument("--nee-mask", type=int, default=-1, choices=[-1, 0, 1],
                     help="split plan's NEE results as per-slot visibility bits (1, default) or per-job records (0)")
     ap.add_argument("--nee-variant", type=int, default=-1, help="serve workload: the executor's NEE kernel "
@@ -577,10 +578,11 @@ def run_walk_sweep(a):
             run(4, 2, 0)
     L.oxpt_diag_set_shadow_postpone(ctx, 0)
     line_extra.clear()
-    # Continuation rays reordered before the closest-hit walk.
-    L.oxpt_diag_set_ray_order(ctx, 1)
-    line_extra["ray_order"] = 1
-    run(4, 2, 0)
+    # Ray queues reordered before the walks (1: continuation rays, 2: shadow rays, 3: both).
+    for mode in (1, 2, 3):
+        L.oxpt_diag_set_ray_order(ctx, mode)
+        line_extra["ray_order"] = mode
+        run(4, 2, 0)
     run(4, 2, 0, closest=1)
     L.oxpt_diag_set_ray_order(ctx, 0)
     line_extra.clear()

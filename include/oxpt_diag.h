@@ -106,12 +106,14 @@ oxpt_status oxpt_diag_set_nee_mask(oxpt_ctx* ctx, int on);
  * 0 (default) = each lane tests a leaf when it reaches it. Occlusion does
  * not depend on the order, so results are the same. */
 oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* ctx, int on);
-/* Wavefront plans: 1 = before the closest-hit walk, the continuation rays
- * are reordered (counting sort on direction octant and a 16^3 Morton cell
- * of the origin in the scene's root box) so that a warp walks similar
- * rays; 0 (default) = queue order. Each ray is walked alone by one lane, so
- * results are the same either way. Its launches time as kind 10. */
-oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* ctx, int on);
+/* Wavefront plans, bit 0: before the closest-hit walk the continuation
+ * rays are reordered (counting sort on direction octant and a 16^3 Morton
+ * cell of the origin in the scene's root box) so that a warp walks similar
+ * rays; bit 1 (trace_variant 3-5): the shadow rays are walked in the order
+ * of their light and origin cell; 0 (default) = queue order. Each ray is
+ * walked alone by one lane, so results are the same either way. The
+ * reordering launches time as kind 10. */
+oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* ctx, int mode);
 
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left

@@ -357,8 +357,8 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     size_t sizes[] = {P * 8, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 16, P * 4, P * 4,
                       PJ * 16, P * 4, PJ * 16, PJ * 16, PJ * 16, 64,
                       split ? P * 4 : 0, split ? P * 4 : 0, split ? 13 * P * 16 : 0, P * 4,
-                      (split && jobs <= 32) ? P * 4 : 0, P * 4, P * 4, P * 4, (size_t)(1u << 15) * 4};
-    constexpr int NB = 26;
+                      (split && jobs <= 32) ? P * 4 : 0, P * 4, PJ * 4, PJ * 4, (size_t)(1u << 17) * 4, PJ * 4};
+    constexpr int NB = 27;
     size_t total = 0;
     for (size_t s : sizes) total += align256(s);
     if (slots > c->wave_cap_slots || jobs > c->wave_cap_jobs || total > c->wave_bytes) {
@@ -402,6 +402,7 @@ oxpt_status ensure_wave(oxpt_ctx* c, uint32_t slots, uint32_t jobs, oxd::WaveSta
     q->ord_key = (uint32_t*)ptr[23];
     q->ord_rank = (uint32_t*)ptr[24];
     q->ord_hist = (uint32_t*)ptr[25];
+    q->sh_perm = (uint32_t*)ptr[26];
     q->ext = (uint32_t*)ptr[12];
     q->sh_o = (float4*)ptr[13];
     q->sh_d = (float4*)ptr[14];
@@ -494,7 +495,7 @@ int enqueue_iteration(oxpt_ctx* c, const oxd::WaveArgs& wa, const oxd::WaveArgs&
     } else {
         run(2, [&] { return oxd::launch_wave_logic(wa, count, (int)c->shade_variant, st); });
     }
-    if (wa.ray_order) {
+    if (wa.ray_order & 1u) {
         run(10, [&] { return oxd::launch_order_ext(wa, c->sms, st); });
         oxd::WaveArgs wo = wa;
         wo.q.ext = wa.q.ext_sorted;
@@ -502,6 +503,8 @@ int enqueue_iteration(oxpt_ctx* c, const oxd::WaveArgs& wa, const oxd::WaveArgs&
     } else {
         run(3, [&] { return oxd::launch_wave_extend(wa, count, (int)c->trace_variant, wa.closest4 ? sd4 : sd, c->sms, st); });
     }
+    if ((wa.ray_order & 2u) && c->trace_variant >= 3)
+        run(10, [&] { return oxd::launch_order_shadow(wa, c->sms, st); });
     run(4, [&] {
         return oxd::launch_wave_shadow(wsh, count, four, (int)c->trace_variant, four ? sd4 : sd, c->sms, st);
     });
@@ -1301,9 +1304,9 @@ oxpt_status oxpt_diag_set_walk(oxpt_ctx* c, uint32_t stack_entries, uint32_t sta
     return OXPT_OK;
 }
 
-oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* c, int on) {
-    if (!c) return OXPT_E_INVALID;
-    c->ray_order = on ? 1u : 0u;
+oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* c, int mode) {
+    if (!c || mode < 0 || mode > 3) return fail(c, OXPT_E_INVALID, "ray order is 0 to 3");
+    c->ray_order = (uint32_t)mode;
     return OXPT_OK;
 }
 

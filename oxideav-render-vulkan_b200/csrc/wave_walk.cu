@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow(const __grid_constant__ 
             if (!active) {
                 uint32_t q = append(&a.ctr[6]);
                 if (q < n) {
+                    if (a.ray_order & 2u) q = a.q.sh_perm[q];
                     float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
                     uint4 m = a.q.sh_m[q];
                     slot = m.x;
@@ -259,6 +260,7 @@ __global__ void __launch_bounds__(NT, MINB) walk_shadow4p(const __grid_constant_
             if (!active) {
                 uint32_t q = append(&a.ctr[6]);
                 if (q < n) {
+                    if (a.ray_order & 2u) q = a.q.sh_perm[q];
                     float4 o = a.q.sh_o[q], d = a.q.sh_d[q];
                     uint4 m = a.q.sh_m[q];
                     slot = m.x;

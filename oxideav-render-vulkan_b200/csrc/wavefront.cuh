@@ -113,6 +113,7 @@ struct WaveQueues {
     // continuation-ray reordering (ray_order.cu): the queue sorted, and per
     // entry its bucket and rank; bucket counts / offsets (2^15)
     uint32_t* ext_sorted;
+    uint32_t* sh_perm;  // shadow queue order (sorted position -> entry)
     uint32_t* ord_key;
     uint32_t* ord_rank;
     uint32_t* ord_hist;
@@ -156,13 +157,17 @@ struct WaveArgs {
     // four-wide shadow walks of variants 3-5 park leaves until the warp
     // has no node work (same occlusion, fewer mixed node/leaf steps)
     uint32_t shadow_post = 0u;
-    // 1: the continuation queue is reordered by origin cell and direction
-    // octant before the closest-hit walk (same results, other warps)
+    // bit 0: the continuation queue is reordered by origin cell and
+    // direction octant before the closest-hit walk; bit 1: the shadow queue
+    // by light and origin cell, read through q.sh_perm by the short-stack
+    // shadow walks (same results, other warps)
     uint32_t ray_order = 0u;
 };
 
-// Reorders a.q.ext into a.q.ext_sorted (ray_order.cu).
+// Reorders a.q.ext into a.q.ext_sorted / the shadow queue into
+// a.q.sh_perm (ray_order.cu).
 cudaError_t launch_order_ext(const WaveArgs& a, int sms, cudaStream_t st);
+cudaError_t launch_order_shadow(const WaveArgs& a, int sms, cudaStream_t st);
 
 // `variant`: 0..2, the occupancy target of the compiled kernel (logic 2 / 3
 // / 4 blocks per SM; traversal 6 / 8 / 10); traversal variants 3..5 run the

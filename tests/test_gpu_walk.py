@@ -174,12 +174,13 @@ def test_postponed_leaf_shadow_walk_in_a_batch(pkg):
 @pytest.mark.parametrize("which", ["materials", "alpha", "layered"])
 def test_reordered_continuation_rays_bit_exact(pkg, oracle, which, mode, variant):
     """Continuation rays sorted by origin cell and direction octant before
-    the closest-hit walk: every ray is walked alone, so the accumulator is
-    the oracle's bit for bit."""
+    the closest-hit walk, shadow rays walked in the order of their light and
+    origin cell: every ray is walked alone, so the accumulator is the
+    oracle's bit for bit."""
     scene, env = _scene(pkg, which)
     t = _tracer(pkg, scene, env)
     t.set_tuning(mode=mode, trace_variant=variant, wave_slots=333, wave_items=2000)
-    assert pkg._native.lib().oxpt_diag_set_ray_order(t.ctx, 1) == 0
+    assert pkg._native.lib().oxpt_diag_set_ray_order(t.ctx, 3) == 0  # both queues (shadow: variants 3-5)
     t.refine(6)
     cpu, _ = oracle.render(t.prepared(), 6)
     assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
@@ -195,7 +196,7 @@ def test_reordered_continuation_rays_in_a_graph_batch(pkg):
         tracers.append(_tracer(pkg, scene, env, w, h, spp))
     ex = pkg.GpuPathTracer(0)
     ex.set_tuning(mode=2, trace_variant=4, wave_slots=500, graphs=1)
-    assert pkg._native.lib().oxpt_diag_set_ray_order(ex.ctx, 1) == 0
+    assert pkg._native.lib().oxpt_diag_set_ray_order(ex.ctx, 3) == 0
     for _ in range(2):  # the second step reuses the graph
         for t in tracers:
             t.reset()
