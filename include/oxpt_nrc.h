@@ -64,7 +64,9 @@ oxpt_status oxpt_nrc_train(oxpt_nrc* nrc, const float* inputs, const float* targ
  * With `train_suffix` > 0 a training path ends into the cache that many
  * bounces after the query vertex and its target adds the cache's
  * prediction there (self-training, which keeps every path short). All of
- * a frame's paths are in flight at once (one wavefront slot per pixel).
+ * a frame's paths are in flight at once (one wavefront slot per pixel);
+ * with `frames_per_wave` > 1 consecutive frames share one wavefront, and
+ * the training step follows each wave rather than each frame.
  * `enabled` = 0 renders plain frames (the ablation). The frame must fit
  * one launch of the context's plan (width x height <= its items per
  * launch).
@@ -82,13 +84,16 @@ typedef struct oxpt_nrc_config {
                                (sum over its bounces of sqrt(t^2 / (pdf |cos|)))^2 exceeds
                                spread x the primary vertex's t^2 / (4 pi |cos|); 0 = exactly
                                at query_bounce */
-    uint32_t reserved;
+    uint32_t frames_per_wave; /* frames traced as one wavefront (0 or 1: one), at most 64: the
+                               next frame's paths take the slots the previous frame's paths free,
+                               so frame tails overlap; the wave's queries are answered and one
+                               training step (on at most max_train samples) is taken after it */
 } oxpt_nrc_config;
-void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1, 4, 0.01 */
+void oxpt_nrc_config_default(oxpt_nrc_config* cfg); /* 1, 2, 16, 65536, 1, 4, 0.01, 1 */
 
 /* `count` cache frames with sample indices first_sample.. on `ctx`'s
- * accumulator; *loss (optional, waits for the GPU) = the last frame's mean
- * training loss before its update. */
+ * accumulator; *loss (optional, waits for the GPU) = the last training
+ * step's mean loss before its update. */
 oxpt_status oxpt_nrc_refine(oxpt_nrc* nrc, oxpt_ctx* ctx, uint32_t first_sample, uint32_t count,
                             const oxpt_nrc_config* cfg, float* loss);
 /* refine() of a tracer with cache frames: `frames` samples per pixel, one

@@ -55,7 +55,7 @@ class BatchFrame(C.Structure):
 
 class NrcConfig(C.Structure):
     _fields_ = [("enabled", u32), ("query_bounce", u32), ("train_one_in", u32), ("max_train", u32),
-                ("train", u32), ("train_suffix", u32), ("spread", C.c_float), ("reserved", u32)]
+                ("train", u32), ("train_suffix", u32), ("spread", C.c_float), ("frames_per_wave", u32)]
 
 
 class DevImage(C.Structure):

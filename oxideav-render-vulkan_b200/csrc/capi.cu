@@ -1950,6 +1950,7 @@ void oxpt_nrc_config_default(oxpt_nrc_config* cfg) {
     cfg->train = 1;
     cfg->train_suffix = 4;
     cfg->spread = 0.01f;
+    cfg->frames_per_wave = 1;
 }
 
 }  // extern "C"
@@ -2039,18 +2040,26 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
     if ((s = ready(c))) return s;
     const uint64_t npix = (uint64_t)c->w * c->h;
     if (npix > c->wave_items) return fail(c, OXPT_E_LIMIT, "a cache frame must fit one launch (width x height <= wave_items)");
-    const uint32_t P = (uint32_t)npix;  // every path of the frame in flight at once
+    const uint32_t P = (uint32_t)npix;  // every path of a frame in flight at once
     const uint32_t max_train = std::max(cfg->max_train, 1u);
+    // Frames traced as one wavefront: refill takes the next frame's paths
+    // into the slots the previous frame's paths free, so a frame's tail of
+    // nearly empty iterations overlaps the next frame's first bounces.
+    const uint32_t G = std::max(cfg->frames_per_wave, 1u);
+    if (G > 64) return fail(c, OXPT_E_INVALID, "frames_per_wave above 64");
+    if (npix * G > c->wave_items) return fail(c, OXPT_E_LIMIT, "frames_per_wave x width x height exceeds wave_items");
     if (cfg->train_suffix > 64) return fail(c, OXPT_E_INVALID, "train_suffix above 64");
     if (!(cfg->spread >= 0.0f) || !std::isfinite(cfg->spread))
         return fail(c, OXPT_E_INVALID, "spread must be finite and not negative");
-    if ((s = nrc_buffers(c, r, npix, max_train, P))) return s;
+    if ((s = nrc_buffers(c, r, npix * G, max_train, P))) return s;
     if ((s = oxd::nrc::ensure_scratch(r, max_train))) return s;
-    if ((s = ensure_out(c, npix))) return s;
+    if ((s = ensure_out(c, npix * G))) return s;
     uint32_t saved_mode = c->mode, saved_slots = c->wave_slots;
     c->mode = OXPT_MODE_WAVEFRONT_SPLIT;
-    c->wave_slots = std::max<uint32_t>(c->wave_slots, P);
-    for (uint32_t i = 0; i < count && !s; i++) {
+    c->wave_slots = P;  // the cache's per-slot state holds one frame's paths
+    for (uint32_t i = 0; i < count && !s; i += G) {
+        const uint32_t g = std::min(G, count - i);
+        const uint64_t items = npix * g;
         cudaError_t ce = cudaMemsetAsync(r->counts, 0, 8, c->stream);
         if (ce) {
             s = cuda_fail(c, ce, "cache counters");
@@ -2059,11 +2068,11 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         oxd::TraceArgs ta;
         ta.s = scene_view(c);
         ta.first = first + i;
-        ta.count = 1;
+        ta.count = g;
         ta.y0 = 0;
         ta.rows = c->h;
         ta.npix = (uint32_t)npix;
-        ta.total = npix;
+        ta.total = items;
         ta.out = c->out;
         ta.counters = nullptr;
         ta.err = c->dev_err;
@@ -2071,7 +2080,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         nw.on = 1;
         nw.query_k = cfg->query_bounce;
         nw.train_mask = cfg->train_one_in - 1;
-        nw.q_cap = (uint32_t)npix;
+        nw.q_cap = (uint32_t)items;
         nw.t_cap = max_train;
         nw.counts = r->counts;
         nw.q_in = r->q_in;
@@ -2091,7 +2100,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
         // The cache's predictions complete the rendering paths.
         oxd::nrc::Args a = oxd::nrc::base_args(r);
         a.in = r->q_in;
-        a.n = (uint32_t)npix;
+        a.n = (uint32_t)items;
         a.n_dev = r->counts;
         a.query_beta = r->q_beta;
         a.query_item = r->q_item;
@@ -2101,7 +2110,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
             s = cuda_fail(c, ce, "cache inference");
             break;
         }
-        oxd::ReduceArgs ra{c->accum, c->out, c->w, 0, (uint32_t)npix, 1};
+        oxd::ReduceArgs ra{c->accum, c->out, c->w, 0, (uint32_t)npix, g};
         if ((ce = oxd::launch_reduce(ra, c->stream))) {
             s = cuda_fail(c, ce, "reduce");
             break;
@@ -2119,7 +2128,7 @@ oxpt_status oxpt_nrc_refine(oxpt_nrc* r, oxpt_ctx* c, uint32_t first, uint32_t c
             b.dy = r->dy;
             b.grad_scale = 0.0f;
             if (!ce && cfg->train_suffix)
-                ce = oxd::nrc::launch_tail_targets(r->counts, max_train, (uint32_t)npix, r->t_tail, r->q_pred,
+                ce = oxd::nrc::launch_tail_targets(r->counts, max_train, (uint32_t)items, r->t_tail, r->q_pred,
                                                    r->t_target, c->stream);
             if (!ce) ce = timed_launch(c, 8, [&] { return oxd::nrc::launch_forward(b, c->sms, c->stream); });
             if (!ce) ce = timed_launch(c, 9, [&] { return oxd::nrc::launch_backward(b, c->sms, c->stream); });

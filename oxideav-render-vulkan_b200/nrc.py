@@ -32,7 +32,7 @@ class RadianceCache:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and N is not None:  # None while the interpreter shuts down
             N.lib().oxpt_nrc_destroy(h)
             self._h = None
 

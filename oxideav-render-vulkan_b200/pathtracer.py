@@ -136,7 +136,7 @@ class Scene:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and N is not None:  # None while the interpreter shuts down
             N.lib().oxpt_scene_free(h)
             self._h = None
 
@@ -213,7 +213,7 @@ class EnvironmentMap:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and N is not None:  # None while the interpreter shuts down
             N.lib().oxpt_env_free(h)
             self._h = None
 
@@ -291,7 +291,7 @@ class PinnedImage:
 
     def __del__(self):
         p = getattr(self, "ptr", None)
-        if p:
+        if p and N is not None:  # None while the interpreter shuts down
             if self._tracer is not None:
                 N.lib().oxpt_tracer_present_wait(self._tracer._h)
             N.lib().oxpt_host_free(p)
@@ -315,7 +315,7 @@ class GpuPathTracer:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and N is not None:  # None while the interpreter shuts down
             N.lib().oxpt_tracer_free(h)
             self._h = None
 

@@ -156,6 +156,42 @@ def test_zero_cache_ends_paths_exactly_at_the_query_bounce(pkg, oracle):
     assert q > 0 and s == 0
 
 
+@pytest.mark.parametrize("per_wave", [2, 3])
+def test_frames_sharing_a_wavefront_are_the_same_frames(pkg, per_wave):
+    """Frames traced as one wavefront (the next frame's paths refill the
+    slots the previous frame's free) are the frames traced one by one: with
+    a zero cache and no training, bit for bit the plain tracer cut after
+    two bounces, for a refine whose frame count is not a multiple of the
+    frames per wave too."""
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg)
+    cache = RadianceCache(t)
+    cache.set_weights(np.zeros(nrc.PARAMS, np.float32))
+    cache.configure(train_one_in=1 << 31, train=0, spread=0, frames_per_wave=per_wave)
+    cache.refine(5)
+    assert t.samples() == 5
+    cut = _tracer(pkg, bounces=2)
+    cut.refine(5)
+    assert np.array_equal(t.read_accum().view(np.uint32), cut.read_accum().view(np.uint32))
+    q, s = cache.frame_counts()
+    assert q > 0 and s == 0
+
+
+def test_frames_sharing_a_wavefront_train(pkg):
+    """Online training with four frames per wavefront: finite losses that
+    fall, and at most max_train samples per training step."""
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg, 64, 64, 8, pkg.Scene.cornell())
+    cache = RadianceCache(t)
+    cache.configure(frames_per_wave=4, max_train=8192)
+    losses = [cache.refine(4, loss=True) for _ in range(12)]
+    assert np.isfinite(losses).all()
+    assert np.mean(losses[-3:]) < np.mean(losses[:3]), losses
+    q, s = cache.frame_counts()
+    assert q > 0 and 0 < s
+    assert t.samples() == 48
+
+
 def test_training_paths_are_the_plain_tracer(pkg):
     """When every path is a training path nothing is cut: the frames equal
     the plain tracer's, and the paths that reach the query vertex become
