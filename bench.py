@@ -97,6 +97,8 @@ def parse():
     ap.add_argument("--spp-scale", type=int, default=16,
                     help="serve workload: spp targets {4..1024} divided by this (one GPU cannot keep up with the "
                          "full stream)")
+    ap.add_argument("--serve-idle-views", type=int, default=2, help="serve workload: closed sessions' views kept "
+                    "per scene for the next request (0: every session makes and frees its own)")
     ap.add_argument("--frames", type=int, default=512, help="nrc workload: frames of 1 spp")
     ap.add_argument("--ref-spp", type=int, default=16384, help="nrc workload: spp of the plain reference")
     ap.add_argument("--nrc-scene", default="large", choices=["large", "cornell"], help="nrc workload: scene")
@@ -105,7 +107,7 @@ def parse():
                     "end into the cache")
     ap.add_argument("--nrc-spread", type=float, default=0.01, help="nrc workload: path-spread constant (0: every "
                     "path ends at the query bounce)")
-    ap.add_argument("--nrc-frames-per-wave", default="1,4", help="nrc workload: comma list of cache frames traced "
+    ap.add_argument("--nrc-frames-per-wave", default="1,4,8", help="nrc workload: comma list of cache frames traced "
                     "as one wavefront (one training step per wave); the line reports the fastest to 35 dB and "
                     "lists every one")
     ap.add_argument("--workload", default="single",
@@ -740,13 +742,20 @@ def run_serve(a):
     for rep in range(max(1, a.repeats)):
         reqs = serve_stream(serve, a, n_scenes, seed=3 + rep)
         check = set(int(x) for x in np.random.default_rng(9 + rep).choice(a.requests, size=8, replace=False))
-        ex = serve.GpuExecutor(pkg, owners, options, keep=lambda o: o.rid in check)
+        ex = serve.GpuExecutor(pkg, owners, options, keep=lambda o: o.rid in check, idle_views=a.serve_idle_views)
         ex.exe.set_tuning(mode=2, graphs=1)
         if a.nee_variant >= 0:
             ex.exe.set_tuning(nee_variant=a.nee_variant)
         budget = 150 << 30
+        # device time of the ticks (CUDA events around each batched step)
+        L = pkg._native.lib()
+        L.oxpt_diag_set_timing(ex.exe.ctx, 1)
         served = serve.Server(ex, budget, tick_paths=1 << 24).run(reqs)
-        ex2 = serve.GpuExecutor(pkg, owners, options)
+        kms, kn = (C.c_double * 12)(), (C.c_uint64 * 12)()
+        L.oxpt_diag_timing_kinds(ex.exe.ctx, kms, kn)
+        L.oxpt_diag_set_timing(ex.exe.ctx, 0)
+        busy_s = kms[0] / 1e3
+        ex2 = serve.GpuExecutor(pkg, owners, options, idle_views=a.serve_idle_views)
         serial = serve.run_serial(ex2, reqs)
         by = {r.rid: r for r in reqs}
         same = []
@@ -758,7 +767,8 @@ def run_serve(a):
                      "p50_latency_s": served.percentile(50), "p99_latency_s": served.percentile(99),
                      "completed": len(served.completed()), "superseded": sum(o.superseded for o in served.outcomes),
                      "ticks": served.ticks, "peak_device_bytes_accounted": served.peak_bytes,
-                     "served_wall_s": served.wall,
+                     "served_wall_s": served.wall, "gpu_busy_s": busy_s,
+                     "gpu_busy_frac": busy_s / max(served.wall, 1e-9),
                      "serial_plain": {"msamples_per_s": serial.msamples_per_s(),
                                       "p50_latency_s": serial.percentile(50), "p99_latency_s": serial.percentile(99),
                                       "completed": len(serial.completed()), "wall_s": serial.wall},
@@ -774,7 +784,8 @@ def run_serve(a):
                                    "scenes (1e3..2e6 triangles log-uniform), resolutions 128^2..1920x1080, spp "
                                    f"targets {{4,16,64,256,1024}}/{a.spp_scale}, 30% camera moves, 150 GB budget",
                        "triangles": tris, "repeats": f"{len(runs)} streams (seeds 3..{2 + len(runs)}); value and "
-                                                    "latencies are the median-ratio run's"},
+                                                    "latencies are the median-ratio run's",
+                       "idle_views_per_scene": a.serve_idle_views},
             "p50_latency_s": mid["p50_latency_s"], "p99_latency_s": mid["p99_latency_s"],
             "throughput_vs_serial": {"median": statistics.median(ratios), "min": min(ratios), "max": max(ratios)},
             "same_alone_and_in_mix": all(all(r["same_alone_and_in_mix"]) for r in runs),

@@ -375,19 +375,6 @@ __device__ __forceinline__ Ray make_ray(f3 o, f3 d) {
     r.valid = finite3(o) && finite3(d) && (d.x != 0.0f || d.y != 0.0f || d.z != 0.0f);
     return r;
 }
-// Three-input minimum / maximum (one instruction on sm_100). Exact, like
-// the nested two-input forms; the slab test never sees a NaN (finite box
-// planes and origins, reciprocals clamped to +-1e30).
-__device__ __forceinline__ float fmax3f(float a, float b, float c) {
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-__device__ __forceinline__ float fmin3f(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
 // Robust slab test (Williams et al. 2005, Ize 2013 far scaling).
 // Returns the entry distance, or -1 when the box is missed.
 __device__ __forceinline__ float slab6(const Ray& r, float lox, float loy, float loz, float hix, float hiy, float hiz,
@@ -397,8 +384,8 @@ __device__ __forceinline__ float slab6(const Ray& r, float lox, float loy, float
     float t0z = (loz - r.o.z) * r.inv.z, t1z = (hiz - r.o.z) * r.inv.z;
     float tnx = fminf(t0x, t1x), tny = fminf(t0y, t1y), tnz = fminf(t0z, t1z);
     float tfx = fmaxf(t0x, t1x), tfy = fmaxf(t0y, t1y), tfz = fmaxf(t0z, t1z);
-    float t0 = fmax3f(fmaxf(0.0f, tnx), tny, tnz);
-    float t1 = fminf(t_max, fmin3f(tfx, tfy, tfz) * 1.0000004f);
+    float t0 = fmaxf(fmaxf(0.0f, tnx), fmaxf(tny, tnz));
+    float t1 = fminf(t_max, fminf(tfx, fminf(tfy, tfz)) * 1.0000004f);
     return t0 <= t1 ? t0 : -1.0f;
 }
 __device__ __forceinline__ float slab(const Ray& r, float4 lo, float4 hi, float t_max) {

@@ -252,10 +252,16 @@ class GpuExecutor:
     refines on one executor context."""
 
     def __init__(self, pkg, owners: List[object], options: Callable[[Request], object], executor=None,
-                 keep: Optional[Callable[[Outcome], bool]] = None):
+                 keep: Optional[Callable[[Outcome], bool]] = None, idle_views: int = 2):
         self.pkg = pkg
         self.owners = owners
         self.options = options
+        # Closed sessions' views wait here for the next request on their
+        # scene: freeing a view's device buffers (and allocating a new
+        # one's) would synchronise the device between queued ticks.
+        self.idle_views = idle_views
+        self.pool: Dict[int, List[object]] = {}
+        self.scene_of: Dict[int, int] = {}
         if executor is None:
             executor = pkg.GpuPathTracer(0)
             # Job-major NEE for mixed batches: a warp's lanes may hold
@@ -279,10 +285,17 @@ class GpuExecutor:
         return r.pixels * 16  # the session's accumulator; scene and tables are the owner's
 
     def open(self, r: Request):
-        v = self.owners[r.scene].view()
+        idle = self.pool.get(r.scene)
+        reused = bool(idle)
+        v = idle.pop() if reused else self.owners[r.scene].view()
         v.sync_view(self.options(r))
         if r.camera is not None:
             v.set_camera(eye=r.camera[0], target=r.camera[1])
+        elif reused:
+            v.set_camera(None)
+        if reused:
+            v.reset()  # same options as the view's last request would keep its samples
+        self.scene_of[id(v)] = r.scene
         return v  # tables and params bind on the first refine
 
     def move(self, v, camera: Optional[Camera], spp: int):
@@ -314,3 +327,7 @@ class GpuExecutor:
 
     def close(self, v):
         v.finish()
+        scene = self.scene_of.pop(id(v), None)
+        idle = self.pool.setdefault(scene, [])
+        if scene is not None and len(idle) < self.idle_views:
+            idle.append(v)
