@@ -1182,28 +1182,38 @@ def main():
     if not a.no_tolerance_plan:
         saved = pt.tuning()
         tv = saved.trace_variant if saved.trace_variant >= 3 else 3
-        pt.set_tuning(trace_variant=tv, closest_walk=1)
-        for _ in range(max(1, a.warmup // 2)):
-            step()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(a.steps):
-            step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        tsec = e0.elapsed_time(e1) / 1e3
-        if world > 1:
-            t = torch.tensor([tsec], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tsec = float(t.item())
+        fast = 1 if saved.mode == 2 else 0  # the fast-math shading build is the split plan's
+
+        def timed_plan(**kw):
+            pt.set_tuning(trace_variant=tv, **kw)
+            for _ in range(max(1, a.warmup // 2)):
+                step()
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(a.steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tsec = e0.elapsed_time(e1) / 1e3
+            if world > 1:
+                t = torch.tensor([tsec], device=f"cuda:{local}", dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                tsec = float(t.item())
+            return tsec
+
+        t_walk = timed_plan(closest_walk=1, fast_shading=0)
+        tsec = timed_plan(closest_walk=1, fast_shading=fast)
         tolerance = {"value": frames * a.steps * paths_step / tsec / 1e6, "unit": "Msamples/s",
                      "ms_per_step": 1e3 * tsec / a.steps, "plan": plan_of(pt),
+                     "closest_walk_only": {"value": frames * a.steps * paths_step / t_walk / 1e6,
+                                           "ms_per_step": 1e3 * t_walk / a.steps},
                      "checks": "tests/test_gpu_tolerance.py, tests/test_gpu_headline.py: ids on 10^6 rays equal "
                                "except ties within 1e-6 relative t; >= 60 dB PSNR against the libm oracle"}
-        pt.set_tuning(trace_variant=saved.trace_variant, closest_walk=saved.closest_walk)
+        pt.set_tuning(trace_variant=saved.trace_variant, closest_walk=saved.closest_walk,
+                      fast_shading=saved.fast_shading)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -1253,7 +1263,8 @@ def plan_of(pt):
             "shade_variant": t.shade_variant, "trace_variant": t.trace_variant, "stack": t.stack,
             "nee_variant": t.nee_variant, "shadow_walk": ["four-wide", "binary"][t.shadow_walk],
             "refill": t.refill, "graphs": t.graphs,
-            "closest_walk": ["binary (exact)", "four-wide (tolerance plan)"][t.closest_walk]}
+            "closest_walk": ["binary (exact)", "four-wide (tolerance plan)"][t.closest_walk],
+            "shading": ["exact build", "fast-math build (tolerance plan)"][t.fast_shading]}
 
 
 class TileGather:

@@ -162,7 +162,12 @@ oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* ctx, int mode);
  *                  binary walk's only between candidates within rounding of
  *                  the same distance, so accumulators match the oracle to
  *                  image tolerance (>= 60 dB PSNR), not bit for bit.
- *   reserved       0.
+ *   fast_shading   0 = the split wavefront's shading kernels as built for
+ *                  bit equality; 1 = their second build with FMA
+ *                  contraction, approximate division and square root and
+ *                  the CUDA library's transcendentals (mode 2 only). With
+ *                  closest_walk 1 this is the tolerance plan: images within
+ *                  >= 60 dB PSNR of the oracle, traversal unchanged.
  */
 enum { OXPT_MODE_MEGAKERNEL = 0, OXPT_MODE_WAVEFRONT = 1, OXPT_MODE_WAVEFRONT_SPLIT = 2 };
 typedef struct oxpt_tuning {
@@ -181,7 +186,7 @@ typedef struct oxpt_tuning {
     uint32_t graphs;
     uint32_t refill;
     uint32_t closest_walk;
-    uint32_t reserved;
+    uint32_t fast_shading;
 } oxpt_tuning;
 oxpt_status oxpt_set_tuning(oxpt_ctx* ctx, const oxpt_tuning* t);
 oxpt_status oxpt_get_tuning(const oxpt_ctx* ctx, oxpt_tuning* t);

@@ -112,7 +112,7 @@ class Tuning(C.Structure):
     _fields_ = [("mode", u32), ("threads", u32), ("blocks_per_sm", u32), ("wave_slots", u32),
                 ("max_paths", u64), ("wave_items", u64), ("check_every", u32), ("shade_variant", u32),
                 ("trace_variant", u32), ("stack", u32), ("nee_variant", u32), ("shadow_walk", u32),
-                ("graphs", u32), ("refill", u32), ("closest_walk", u32), ("reserved", u32)]
+                ("graphs", u32), ("refill", u32), ("closest_walk", u32), ("fast_shading", u32)]
 
 
 MODE_MEGAKERNEL, MODE_WAVEFRONT, MODE_WAVEFRONT_SPLIT = 0, 1, 2

@@ -32,6 +32,12 @@ NVCC_FLAGS = [
     "-Xptxas", "-warn-spills",
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
+# Sources built a second time for the tolerance plan: FMA contraction,
+# approximate division and square root, the CUDA library's transcendentals
+# (launchers in oxd::fast; its results are held to image PSNR, not bits).
+FAST_SOURCES = ("wave_split.cu",)
+FAST_FLAGS = [f for f in NVCC_FLAGS if f not in ("--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false")] \
+    + ["-use_fast_math", "-DOXPT_FAST"]
 
 
 def nvcc() -> str:
@@ -77,6 +83,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         objs.append(obj)
         if _stale(obj, src, headers):
             jobs_list.append([nv, *ARCH, *NVCC_FLAGS, *inc, "-Xptxas", "-v", "-c", str(src), "-o", str(obj)])
+        if src.name in FAST_SOURCES:
+            fobj = BUILD / (src.stem + ".fast.cu.o")
+            objs.append(fobj)
+            if _stale(fobj, src, headers):
+                jobs_list.append([nv, *ARCH, *FAST_FLAGS, *inc, "-Xptxas", "-v", "-c", str(src), "-o", str(fobj)])
     for src in cpp:
         obj = BUILD / (src.stem + ".cpp.o")
         objs.append(obj)

@@ -121,6 +121,7 @@ struct oxpt_ctx {
     uint32_t bvh4_nodes = 0, bvh4_root = 0xffffffffu, bvh4_need = 0;
     uint32_t shadow_walk = 0;
     uint32_t closest_walk = 0;  // 1: continuation rays on the four-wide tree (tolerance plan)
+    uint32_t fast_shading = 0;  // 1: the split kernels' fast-math build (tolerance plan)
     // split plan: per-slot visibility masks instead of a pending record per
     // NEE job (oxpt_diag_set_nee_mask; results are the same either way)
     bool nee_mask = true;
@@ -488,7 +489,11 @@ int enqueue_iteration(oxpt_ctx* c, const oxd::WaveArgs& wa, const oxd::WaveArgs&
         n++;
     };
     *err = cudaMemsetAsync(wa.ctr, 0, 32, st);
-    if (c->mode == OXPT_MODE_WAVEFRONT_SPLIT) {
+    if (c->mode == OXPT_MODE_WAVEFRONT_SPLIT && c->fast_shading) {
+        run(2, [&] { return oxd::fast::launch_split_logic(wa, count, st); });
+        run(5, [&] { return oxd::fast::launch_split_shade(wa, count, (int)c->shade_variant, c->sms, st); });
+        run(6, [&] { return oxd::fast::launch_split_nee(wa, count, (int)c->nee_variant, c->sms, st); });
+    } else if (c->mode == OXPT_MODE_WAVEFRONT_SPLIT) {
         run(2, [&] { return oxd::launch_split_logic(wa, count, st); });
         run(5, [&] { return oxd::launch_split_shade(wa, count, (int)c->shade_variant, c->sms, st); });
         run(6, [&] { return oxd::launch_split_nee(wa, count, (int)c->nee_variant, c->sms, st); });
@@ -1364,6 +1369,10 @@ oxpt_status oxpt_set_tuning(oxpt_ctx* c, const oxpt_tuning* t) {
     if (t->closest_walk && t->trace_variant < 3)
         return fail(c, OXPT_E_INVALID, "closest_walk 1 needs the short-stack traversal kernels (trace_variant 3-5)");
     c->closest_walk = t->closest_walk;
+    if (t->fast_shading > 1) return fail(c, OXPT_E_INVALID, "fast_shading is 0 or 1");
+    if (t->fast_shading && t->mode != OXPT_MODE_WAVEFRONT_SPLIT)
+        return fail(c, OXPT_E_INVALID, "fast_shading 1 needs the split wavefront (mode 2)");
+    c->fast_shading = t->fast_shading;
     c->refill = t->refill ? t->refill : 8u;
     c->shadow_walk = t->shadow_walk;
     c->graphs = t->graphs;
@@ -1392,7 +1401,7 @@ oxpt_status oxpt_get_tuning(const oxpt_ctx* c, oxpt_tuning* t) {
     t->graphs = c->graphs;
     t->refill = c->refill;
     t->closest_walk = c->closest_walk;
-    t->reserved = 0;
+    t->fast_shading = c->fast_shading;
     return OXPT_OK;
 }
 
@@ -1610,7 +1619,7 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
         CK(e, cudaMemset(e->dev_tally, 0, 16), "graph tally");
     }
     if (!e->capture) CK(e, cudaStreamCreateWithFlags(&e->capture, cudaStreamNonBlocking), "capture stream");
-    std::vector<uint64_t> key = {e->mode, e->shade_variant, e->trace_variant, e->nee_variant, (uint64_t)sd,
+    std::vector<uint64_t> key = {e->mode, e->fast_shading, e->shade_variant, e->trace_variant, e->nee_variant, (uint64_t)sd,
                                  four ? 1ull : 0ull, (uint64_t)e->sms, (uint64_t)(uintptr_t)e->wave_mem,
                                  (uint64_t)(uintptr_t)e->out, (uint64_t)(uintptr_t)e->dev_err,
                                  (uint64_t)(uintptr_t)e->stream, args.empty() ? 0 : args[0].vcap,

@@ -27,6 +27,11 @@
 namespace cg = cooperative_groups;
 
 namespace oxd {
+// Built twice: exactly (the launchers in oxd) and with OXPT_FAST and fast
+// math (the tolerance plan's shading; the launchers in oxd::fast).
+#ifdef OXPT_FAST
+namespace fast {
+#endif
 
 namespace {
 
@@ -505,4 +510,7 @@ cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms
     return persistent(count ? nee_fn<true, false>(variant) : nee_fn<false, false>(variant), a, sms, st);
 }
 
+#ifdef OXPT_FAST
+}  // namespace fast
+#endif
 }  // namespace oxd

@@ -196,5 +196,14 @@ cudaError_t launch_wave_continue(cudaGraphConditionalHandle h, uint32_t* ctr, ui
 cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st);
 cudaError_t launch_split_shade(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st);
 cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st);
+// The same three kernels built a second time with FMA contraction,
+// approximate division and square root and the CUDA library's
+// transcendentals (wave_split.cu with OXPT_FAST): the shading of the
+// tolerance plan, held to image PSNR against the oracle instead of bits.
+namespace fast {
+cudaError_t launch_split_logic(const WaveArgs& a, bool count, cudaStream_t st);
+cudaError_t launch_split_shade(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st);
+cudaError_t launch_split_nee(const WaveArgs& a, bool count, int variant, int sms, cudaStream_t st);
+}  // namespace fast
 
 }  // namespace oxd

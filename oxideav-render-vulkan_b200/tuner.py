@@ -37,10 +37,11 @@ class Plan:
     graphs: int = 0
     refill: int = 8
     closest_walk: int = 0  # 1: the tolerance plan (four-wide closest-hit walk), never chosen by the tuner
+    fast_shading: int = 0  # 1: the tolerance plan's fast-math shading kernels, never chosen by the tuner
 
     def key(self):
         return (self.mode, self.shade_variant, self.trace_variant, self.stack, self.wave_slots, self.nee_variant,
-                self.shadow_walk, self.graphs, self.refill, self.closest_walk)
+                self.shadow_walk, self.graphs, self.refill, self.closest_walk, self.fast_shading)
 
 
 SPACE = {
@@ -101,7 +102,7 @@ def apply(tracer, plan: Plan):
     tracer.set_tuning(mode=plan.mode, shade_variant=plan.shade_variant, trace_variant=plan.trace_variant,
                       stack=plan.stack, wave_slots=plan.wave_slots, nee_variant=plan.nee_variant,
                       shadow_walk=plan.shadow_walk, graphs=plan.graphs, refill=plan.refill,
-                      closest_walk=plan.closest_walk)
+                      closest_walk=plan.closest_walk, fast_shading=plan.fast_shading)
 
 
 def tune(tracer, spp: int = 1, repeats: int = 1, log: Optional[list] = None) -> Plan:

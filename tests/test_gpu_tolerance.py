@@ -8,7 +8,10 @@ star's own checks rather than bit equality:
 * images at equal spp are within >= 60 dB PSNR of the oracle built with
   the C library's transcendentals (the CPU tracer's arithmetic), on the
   Cornell box at 256x256, 16 spp, 8 bounces, roulette from 3, and on the
-  layered-material and alpha scenes.
+  layered-material and alpha scenes;
+* the same images with the shading kernels' fast-math build (FMA
+  contraction, approximate division and square root, the CUDA library's
+  transcendentals: fast_shading = 1), the rest of the tolerance plan.
 """
 from __future__ import annotations
 
@@ -72,13 +75,13 @@ def test_four_wide_closest_hit_ids_on_a_million_rays(pkg, oracle, which):
     check_ids(pkg, oracle, t, p, _rays(np.random.default_rng(12), 1_000_000, lo, hi), 100_000)
 
 
-def _psnr_vs_libm(pkg, oracle, scene, opts, spp, env=None, variant=4, mode=2):
+def _psnr_vs_libm(pkg, oracle, scene, opts, spp, env=None, variant=4, mode=2, fast=0):
     t = pkg.GpuPathTracer(0)
     if env is not None:
         t.set_environment(env)
     assert t.sync(scene, opts)
-    t.set_tuning(mode=mode, trace_variant=variant, closest_walk=1)
-    assert t.tuning().closest_walk == 1
+    t.set_tuning(mode=mode, trace_variant=variant, closest_walk=1, fast_shading=fast)
+    assert t.tuning().closest_walk == 1 and t.tuning().fast_shading == fast
     t.refine(spp)
     img = t.image()
     cpu, _ = oracle.render(t.prepared(), spp, libm=True)
@@ -86,16 +89,17 @@ def _psnr_vs_libm(pkg, oracle, scene, opts, spp, env=None, variant=4, mode=2):
     return scenes.psnr_rgb8(img, ref)
 
 
-def test_cornell_256_16spp_psnr_at_least_60db(pkg, oracle):
+@pytest.mark.parametrize("fast", [0, 1])
+def test_cornell_256_16spp_psnr_at_least_60db(pkg, oracle, fast):
     opts = pkg.RenderOptions(width=256, height=256, path_trace=pkg.PathTraceOptions(samples_per_pixel=16,
                                                                                     max_bounces=8, rr_start=3,
                                                                                     seed=0))
-    assert _psnr_vs_libm(pkg, oracle, pkg.Scene.cornell(), opts, 16) >= 60.0
+    assert _psnr_vs_libm(pkg, oracle, pkg.Scene.cornell(), opts, 16, fast=fast) >= 60.0
 
 
-@pytest.mark.parametrize("variant", [3, 5])
+@pytest.mark.parametrize("variant,fast", [(3, 0), (5, 0), (4, 1)])
 @pytest.mark.parametrize("which", ["layered", "alpha", "materials"])
-def test_scenes_psnr_at_least_60db(pkg, oracle, which, variant):
+def test_scenes_psnr_at_least_60db(pkg, oracle, which, variant, fast):
     env = None
     if which == "layered":
         scene = pkg.Scene.icosphere(freq=24, seed=9, n_materials=16, n_textures=4, tex_size=128, n_punctual=4,
@@ -107,10 +111,18 @@ def test_scenes_psnr_at_least_60db(pkg, oracle, which, variant):
         scene = scenes.materials_scene(pkg)
     opts = pkg.RenderOptions(width=64, height=48, path_trace=pkg.PathTraceOptions(samples_per_pixel=16,
                                                                                   max_bounces=10))
-    assert _psnr_vs_libm(pkg, oracle, scene, opts, 16, env, variant) >= 60.0
+    assert _psnr_vs_libm(pkg, oracle, scene, opts, 16, env, variant, fast=fast) >= 60.0
 
 
 def test_tolerance_plan_needs_the_short_stack_kernels(pkg):
     t = pkg.GpuPathTracer(0)
     with pytest.raises(pkg.InvalidOptionsError):
         t.set_tuning(trace_variant=0, closest_walk=1)
+
+
+def test_fast_shading_needs_the_split_wavefront(pkg):
+    t = pkg.GpuPathTracer(0)
+    with pytest.raises(pkg.InvalidOptionsError):
+        t.set_tuning(mode=1, fast_shading=1)
+    t.set_tuning(mode=2, fast_shading=1)
+    assert t.tuning().fast_shading == 1
