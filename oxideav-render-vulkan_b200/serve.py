@@ -259,9 +259,13 @@ class GpuExecutor:
         # Closed sessions' views wait here for the next request on their
         # scene: freeing a view's device buffers (and allocating a new
         # one's) would synchronise the device between queued ticks.
+        # Only views that batched ticks traced are kept: a view that traced
+        # on its own (refine_alone) holds its own wavefront state, gigabytes
+        # that would pile up in the pool.
         self.idle_views = idle_views
         self.pool: Dict[int, List[object]] = {}
         self.scene_of: Dict[int, int] = {}
+        self.alone: set = set()
         if executor is None:
             executor = pkg.GpuPathTracer(0)
             # Job-major NEE for mixed batches: a warp's lanes may hold
@@ -316,6 +320,7 @@ class GpuExecutor:
         self.pkg._native.lib().oxpt_wait_mark(self.exe.ctx, mark)
 
     def refine_alone(self, v, n: int):
+        self.alone.add(id(v))
         v.refine(n)
 
     def sync(self):
@@ -328,6 +333,9 @@ class GpuExecutor:
     def close(self, v):
         v.finish()
         scene = self.scene_of.pop(id(v), None)
+        if id(v) in self.alone:
+            self.alone.discard(id(v))
+            return
         idle = self.pool.setdefault(scene, [])
         if scene is not None and len(idle) < self.idle_views:
             idle.append(v)
