@@ -4,8 +4,10 @@ C++ host layer), written in-tree next to this file.
 Device code is compiled without FMA contraction (``--fmad=false``) and with
 IEEE division and square root, because the estimator's per-sample results
 must match the CPU restatement bit for bit; host code likewise uses
-``-ffp-contract=off``. Objects go to ``_build/`` and are rebuilt only when a
-source or header is newer.
+``-ffp-contract=off``. The one exception is a second build of the split
+wavefront's shading kernels with fast math, which only the tolerance plan
+runs (``FAST_SOURCES``). Objects go to ``_build/`` and are rebuilt only when
+a source or header is newer.
 """
 from __future__ import annotations
 
