@@ -750,7 +750,9 @@ def run_serve(a):
         # device time of the ticks (CUDA events around each batched step)
         L = pkg._native.lib()
         L.oxpt_diag_set_timing(ex.exe.ctx, 1)
+        L.oxpt_diag_timing(ex.exe.ctx, None, None, None, None)
         served = serve.Server(ex, budget, tick_paths=1 << 24).run(reqs)
+        L.oxpt_diag_timing(ex.exe.ctx, None, None, None, None)  # folds the ticks' event pairs
         kms, kn = (C.c_double * 12)(), (C.c_uint64 * 12)()
         L.oxpt_diag_timing_kinds(ex.exe.ctx, kms, kn)
         L.oxpt_diag_set_timing(ex.exe.ctx, 0)
