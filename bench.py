@@ -1208,10 +1208,26 @@ def main():
 
         t_walk = timed_plan(closest_walk=1, fast_shading=0)
         tsec = timed_plan(closest_walk=1, fast_shading=fast)
+        # its kernels, as for the exact plan: frames re-run without the graph
+        tol_steps = min(a.steps, 4)
+        pt.set_tuning(graphs=0)
+        L.oxpt_diag_set_timing(pt.ctx, 1)
+        L.oxpt_diag_timing(pt.ctx, None, None, None, None)
+        for _ in range(tol_steps):
+            step()
+        pt.finish()
+        L.oxpt_diag_timing(pt.ctx, None, None, None, None)
+        L.oxpt_diag_set_timing(pt.ctx, 0)
+        tms_, tn_ = (C.c_double * 12)(), (C.c_uint64 * 12)()
+        L.oxpt_diag_timing_kinds(pt.ctx, tms_, tn_)
+        pt.set_tuning(graphs=saved.graphs)
+        tol_kernels = {name: {"ms_per_step": tms_[k] / tol_steps, "launch_ms": tms_[k] / tn_[k]}
+                       for k, name in kinds if tn_[k]}
         tolerance = {"value": frames * a.steps * paths_step / tsec / 1e6, "unit": "Msamples/s",
                      "ms_per_step": 1e3 * tsec / a.steps, "plan": plan_of(pt),
                      "closest_walk_only": {"value": frames * a.steps * paths_step / t_walk / 1e6,
                                            "ms_per_step": 1e3 * t_walk / a.steps},
+                     "kernels": tol_kernels,
                      "checks": "tests/test_gpu_tolerance.py, tests/test_gpu_headline.py: ids on 10^6 rays equal "
                                "except ties within 1e-6 relative t; >= 60 dB PSNR against the libm oracle"}
         pt.set_tuning(trace_variant=saved.trace_variant, closest_walk=saved.closest_walk,

@@ -3,7 +3,7 @@
  * tracer's own path samples, which ends paths after a few bounces with its
  * prediction of the radiance still to come. No counterpart in the
  * reference (its tracer is the unbiased plain form, which stays the
- * fallback and the judge here too).
+ * fallback here and the image the cache's error is measured against).
  *
  * Network: inputs = position (normalised to the scene bounds), outgoing
  * direction, shading normal (each component mapped to [0, 1]) and
