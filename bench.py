@@ -82,6 +82,9 @@ def parse():
                          "see kernels inside graphs with conditional nodes)")
     ap.add_argument("--shadow-postpone", type=int, default=-1, choices=[-1, 0, 1],
                     help="four-wide shadow walks park leaves until the warp has no node work (1) or not (0)")
+    ap.add_argument("--l2-window", type=int, default=0, choices=[0, 1],
+                    help="1: the traversal kernels mark the tree nodes they read as persisting L2 lines "
+                         "(oxpt_diag_set_l2_window)")
     ap.add_argument("--ray-order", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
                     help="reorder ray queues before the walks: 1 continuation rays (origin cell, direction "
                          "octant), 2 shadow rays (light, origin cell), 3 both")
@@ -1041,6 +1044,9 @@ def main():
         L.oxpt_diag_set_shadow_postpone(pt.ctx, a.shadow_postpone)
     if a.ray_order >= 0:
         L.oxpt_diag_set_ray_order(pt.ctx, a.ray_order)
+    l2_granted = C.c_uint64(0)
+    if a.l2_window:
+        assert L.oxpt_diag_set_l2_window(pt.ctx, 1, C.byref(l2_granted)) == 0, L.oxpt_last_error(pt.ctx).decode()
     prep = pt.prepared()
 
     # Algorithmic bytes per path from the counting build (untimed, 1 spp):
@@ -1207,7 +1213,14 @@ def main():
             return tsec
 
         t_walk = timed_plan(closest_walk=1, fast_shading=0)
-        tsec = timed_plan(closest_walk=1, fast_shading=fast)
+        # the fast build's shading kernel compiles to other register counts,
+        # so its occupancy variant is chosen here by measurement
+        by_shade = {}
+        for sv in ((0, 1, 2) if fast else (saved.shade_variant,)):
+            by_shade[sv] = timed_plan(closest_walk=1, fast_shading=fast, shade_variant=sv)
+        best_sv = min(by_shade, key=by_shade.get)
+        tsec = by_shade[best_sv]
+        pt.set_tuning(shade_variant=best_sv)
         # its kernels, as for the exact plan: frames re-run without the graph
         tol_steps = min(a.steps, 4)
         pt.set_tuning(graphs=0)
@@ -1228,10 +1241,11 @@ def main():
                      "closest_walk_only": {"value": frames * a.steps * paths_step / t_walk / 1e6,
                                            "ms_per_step": 1e3 * t_walk / a.steps},
                      "kernels": tol_kernels,
+                     "ms_per_step_by_shade_variant": {str(k): 1e3 * v / a.steps for k, v in by_shade.items()},
                      "checks": "tests/test_gpu_tolerance.py, tests/test_gpu_headline.py: ids on 10^6 rays equal "
                                "except ties within 1e-6 relative t; >= 60 dB PSNR against the libm oracle"}
         pt.set_tuning(trace_variant=saved.trace_variant, closest_walk=saved.closest_walk,
-                      fast_shading=saved.fast_shading)
+                      fast_shading=saved.fast_shading, shade_variant=saved.shade_variant)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -1244,7 +1258,8 @@ def main():
         line = {"metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
                 "scaling": "strong" if rows_mode else "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": config(a, world, rows_mode),
+                "data": "synthetic", "config": dict(config(a, world, rows_mode),
+                                                    l2_persisting_bytes=int(l2_granted.value)),
                 "mrays_per_s": value * rays_per_path,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": kd["traffic_bytes_per_launch"],

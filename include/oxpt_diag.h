@@ -114,6 +114,14 @@ oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* ctx, int on);
  * walked alone by one lane, so results are the same either way. The
  * reordering launches time as kind 10. */
 oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* ctx, int mode);
+/* on = 1: the short-stack traversal kernels (trace_variant 3-5) of launches
+ * over one scene mark the tree nodes they read (the binary nodes for
+ * closest hits, the four-wide tree for shadow rays) as persisting L2 lines
+ * through an access-policy window, half of the L2 set-aside each; the
+ * process's persisting set-aside is raised to the device maximum, a limit
+ * of this process's CUDA context. *granted (optional) = the set-aside in
+ * bytes. A performance hint only: results are the same bits. 0 = off. */
+oxpt_status oxpt_diag_set_l2_window(oxpt_ctx* ctx, int on, uint64_t* granted);
 
 /*
  * Execution plan of a context, chosen by the autotuner (tuner.py) or left

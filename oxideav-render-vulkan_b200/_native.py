@@ -163,6 +163,7 @@ _SIGS = {
     "oxpt_diag_set_nee_mask": (cint, [vp, cint]),
     "oxpt_diag_set_shadow_postpone": (cint, [vp, cint]),
     "oxpt_diag_set_ray_order": (cint, [vp, cint]),
+    "oxpt_diag_set_l2_window": (cint, [vp, cint, C.POINTER(u64)]),
     "oxpt_diag_launch_count": (cint, [vp, C.POINTER(u64)]),
     "oxpt_diag_set_timing": (cint, [vp, cint]),
     "oxpt_set_tuning": (cint, [vp, C.POINTER(Tuning)]),

@@ -127,6 +127,9 @@ struct oxpt_ctx {
     bool nee_mask = true;
     uint32_t shadow_post = 0;  // four-wide shadow walks with postponed leaves (oxpt_diag_set_shadow_postpone)
     uint32_t ray_order = 0;    // continuation queue reordered before the walk (oxpt_diag_set_ray_order)
+    // tree nodes of the walks as persisting L2 lines (oxpt_diag_set_l2_window):
+    // the set-aside granted and the largest window the device takes
+    uint64_t l2_setaside = 0, l2_max_window = 0;
     uint32_t refill = 8;  // traversal lanes idle in a warp before it fetches rays
     // traversal variants 3-5: stack entries per lane kept in shared memory,
     // top nodes of the binary tree staged per CTA (oxpt_diag_set_walk)
@@ -451,6 +454,8 @@ oxpt_status run_wave(oxpt_ctx* c, const oxd::TraceArgs& ta, bool count, const ox
     wa.walk_stage = c->walk_stage;
     wa.shadow_post = c->shadow_post;
     wa.ray_order = c->ray_order;
+    wa.l2_share = c->l2_setaside / 2;  // two trees: binary for closest hits, four-wide for shadows
+    wa.l2_max_window = c->l2_max_window;
     wa.closest4 = (c->closest_walk && c->trace_variant >= 3 && bvh4_usable(c)) ? 1u : 0u;
     // Stack depth: 32 entries are exact when the BVH has at most 32 levels.
     int sd = c->stack ? (int)c->stack : (c->bvh_depth <= 32 ? 32 : 64);
@@ -1315,6 +1320,30 @@ oxpt_status oxpt_diag_set_ray_order(oxpt_ctx* c, int mode) {
     return OXPT_OK;
 }
 
+oxpt_status oxpt_diag_set_l2_window(oxpt_ctx* c, int on, uint64_t* granted) {
+    if (!c || on < 0 || on > 1) return fail(c, OXPT_E_INVALID, "l2 window is 0 or 1");
+    oxpt_status s = set_device(c);
+    if (s) return s;
+    if (!on) {
+        c->l2_setaside = 0;
+        if (granted) *granted = 0;
+        return OXPT_OK;
+    }
+    int maxp = 0, maxw = 0;
+    CK(c, cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, c->device), "l2 attribute");
+    CK(c, cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, c->device), "l2 attribute");
+    if (maxp <= 0 || maxw <= 0) return fail(c, OXPT_E_LIMIT, "the device has no persisting L2 set-aside");
+    // A limit of this process's context (it ends with the process).
+    size_t cur = 0;
+    CK(c, cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize), "l2 limit");
+    if (cur < (size_t)maxp) CK(c, cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)maxp), "l2 limit");
+    CK(c, cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize), "l2 limit");
+    c->l2_setaside = cur;
+    c->l2_max_window = (uint64_t)maxw;
+    if (granted) *granted = cur;
+    return OXPT_OK;
+}
+
 oxpt_status oxpt_diag_set_shadow_postpone(oxpt_ctx* c, int on) {
     if (!c) return OXPT_E_INVALID;
     c->shadow_post = on ? 1u : 0u;
@@ -1630,7 +1659,7 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
         const oxd::WaveArgs& a0 = args[0];
         key.insert(key.end(), {(uint64_t)(uintptr_t)a0.s.geom, a0.s.geom_vec4, a0.s.P.env[3], a0.one_scene,
                                a0.closest4, a0.walk_lim, a0.walk_stage, (uint64_t)(uintptr_t)a0.st.vis,
-                               a0.shadow_post, a0.ray_order});
+                               a0.shadow_post, a0.ray_order, a0.l2_share, a0.l2_max_window});
     }
     for (size_t k = 0; k < rounds.size(); k++) {
         const oxd::WaveArgs& wa = args[k];
@@ -1891,6 +1920,8 @@ oxpt_status oxpt_refine_batch(oxpt_ctx* e, const oxpt_batch_frame* fr, uint32_t 
         wa.walk_stage = e->walk_stage;
         wa.shadow_post = e->shadow_post;
         wa.ray_order = e->ray_order;
+        wa.l2_share = e->l2_setaside / 2;
+        wa.l2_max_window = e->l2_max_window;
         wa.closest4 = closest4 ? 1u : 0u;
         wa.total = total;
         wa.out = e->out;

@@ -377,7 +377,30 @@ cudaError_t launch_walk(const WaveArgs& a, bool count, bool ext, bool four, int 
     WaveArgs copy = a;
     void* args3[] = {&copy, &staged, &lim};
     void* args2[] = {&copy, &lim};
-    return cudaLaunchKernel(fn, dim3(blocks), dim3(NT), (ext && four) ? args2 : args3, smem, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    // The tree nodes this walk reads as persisting L2 lines, so that the
+    // wavefront state and attributes streaming through L2 between walks do
+    // not evict them (a hint: results do not depend on it).
+    cudaLaunchAttribute attr[1];
+    const float4* base = four ? a.s.bvh4 : a.s.geom;
+    const uint64_t bytes = four ? (uint64_t)a.s.bvh4_nodes * 128u : (uint64_t)a.s.P.env[3] * 32u;
+    if (a.l2_share && a.l2_max_window && base && bytes && (a.nframes == 0 || a.one_scene)) {
+        const uint64_t win = bytes < a.l2_max_window ? bytes : a.l2_max_window;
+        const double ratio = (double)a.l2_share / (double)win;
+        attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[0].val.accessPolicyWindow.base_ptr = (void*)base;
+        attr[0].val.accessPolicyWindow.num_bytes = (size_t)win;
+        attr[0].val.accessPolicyWindow.hitRatio = ratio < 1.0 ? (float)ratio : 1.0f;
+        attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    return cudaLaunchKernelExC(&cfg, fn, (ext && four) ? args2 : args3);
 }
 
 }  // namespace oxd

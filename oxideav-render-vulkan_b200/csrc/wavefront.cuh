@@ -162,6 +162,11 @@ struct WaveArgs {
     // by light and origin cell, read through q.sh_perm by the short-stack
     // shadow walks (same results, other warps)
     uint32_t ray_order = 0u;
+    // traversal variants 3-5 of one-scene launches: bytes of the L2's
+    // persisting set-aside each walk may claim for the tree nodes it reads
+    // (an access-policy window on its launch; 0: none), and the largest
+    // window the device takes
+    unsigned long long l2_share = 0ull, l2_max_window = 0ull;
 };
 
 // Reorders a.q.ext into a.q.ext_sorted / the shadow queue into

@@ -203,3 +203,47 @@ def test_reordered_continuation_rays_in_a_graph_batch(pkg):
         pkg.refine_batch(tracers, [it[4] for it in items], executor=ex)
         for t, w_ in zip(tracers, want):
             assert np.array_equal(t.read_accum().view(np.uint32), w_.view(np.uint32))
+
+
+@pytest.mark.parametrize("which", ["materials", "layered"])
+@pytest.mark.parametrize("mode,variant", [(2, 4), (1, 3)])
+def test_persisting_l2_window_bit_exact(pkg, oracle, which, mode, variant):
+    """The walks' tree nodes marked as persisting L2 lines (an access-policy
+    window on each traversal launch) change only where lines live: the
+    accumulator is the oracle's bit for bit."""
+    import ctypes as C
+    scene, env = _scene(pkg, which)
+    t = _tracer(pkg, scene, env)
+    t.set_tuning(mode=mode, trace_variant=variant, wave_slots=333, wave_items=2000)
+    granted = C.c_uint64(0)
+    assert pkg._native.lib().oxpt_diag_set_l2_window(t.ctx, 1, C.byref(granted)) == 0
+    assert granted.value > 0
+    t.refine(6)
+    cpu, _ = oracle.render(t.prepared(), 6)
+    assert np.array_equal(t.read_accum().view(np.uint32), cpu.view(np.uint32))
+
+
+def test_persisting_l2_window_in_a_graph_batch(pkg):
+    import ctypes as C
+    items = [(scenes.materials_scene(pkg), None, 40, 28, 4), _scene(pkg, "layered") + (48, 32, 5)]
+    want, tracers = [], []
+    for scene, env, w, h, spp in items:
+        alone = _tracer(pkg, scene, env, w, h, spp)
+        alone.refine(spp)
+        want.append(alone.read_accum())
+        tracers.append(_tracer(pkg, scene, env, w, h, spp))
+    ex = pkg.GpuPathTracer(0)
+    ex.set_tuning(mode=2, trace_variant=4, wave_slots=500, graphs=1)
+    assert pkg._native.lib().oxpt_diag_set_l2_window(ex.ctx, 1, None) == 0
+    for _ in range(2):
+        for t in tracers:
+            t.reset()
+        pkg.refine_batch(tracers, [it[4] for it in items], executor=ex)
+        for t, w_ in zip(tracers, want):
+            assert np.array_equal(t.read_accum().view(np.uint32), w_.view(np.uint32))
+    # one scene in the batch: the launches carry the window
+    t = tracers[1]
+    t.reset()
+    pkg.refine_batch([t], [items[1][4]], executor=ex)
+    assert np.array_equal(t.read_accum().view(np.uint32), want[1].view(np.uint32))
+    assert pkg._native.lib().oxpt_diag_set_l2_window(ex.ctx, 0, None) == 0
