@@ -1179,6 +1179,7 @@ def main():
                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                "upload_sync_ms": e2e["upload_sync_ms"], "upload_staged_ms": e2e["upload_staged_ms"],
                "h2d_gbs_sync": e2e["h2d_gbs_sync"], "steps_identical": e2e["steps_identical"],
+               "graph_builds_in_timed_steps": e2e["graph_builds_in_timed_steps"],
                "pipeline": "scene staged into a second buffer set during the previous step's trace; "
                            "image read back on the copy stream"}
 
@@ -1368,11 +1369,14 @@ def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank, tile=None, gather=None
     check(L.oxpt_resolve_wait(ctx))
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0, b1 = C.c_uint64(), C.c_uint64()
+    L.oxpt_diag_graph_builds(ctx, C.byref(b0))
     t0 = time.perf_counter()
     ev0.record(stream)
     for i in range(a.steps):
         step(i)
     check(L.oxpt_resolve_wait(ctx))
+    L.oxpt_diag_graph_builds(ctx, C.byref(b1))
     ev1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
@@ -1381,7 +1385,8 @@ def e2e_measure(pkg, L, pt, prep, a, stream, torch, rank, tile=None, gather=None
     seconds = max(ev0.elapsed_time(ev1) / 1e3, wall)
     same = bool(torch.equal(imgs[0], imgs[1]))  # every step renders the same frame
     return {"seconds": seconds, "h2d": h2d, "d2h": d2h, "upload_sync_ms": sync_ms, "upload_staged_ms": staged_ms,
-            "h2d_gbs_sync": h2d / (sync_ms * 1e-3) / 1e9, "steps_identical": same}
+            "h2d_gbs_sync": h2d / (sync_ms * 1e-3) / 1e9, "steps_identical": same,
+            "graph_builds_in_timed_steps": int(b1.value - b0.value)}
 
 
 if __name__ == "__main__":

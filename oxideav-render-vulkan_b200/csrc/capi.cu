@@ -151,6 +151,10 @@ struct oxpt_ctx {
     cudaStream_t capture = nullptr;  // stream the loop bodies are captured on
     cudaGraphExec_t bgraph = nullptr;
     std::vector<uint64_t> bgraph_key;
+    // the step shape before it: a context that re-stages its scene every
+    // step alternates between its two scene buffer sets, one graph each
+    cudaGraphExec_t bgraph_alt = nullptr;
+    std::vector<uint64_t> bgraph_alt_key;
     uint64_t graph_builds = 0;
     unsigned long long* dev_tally = nullptr;  // graph loops: kernels launched, iterations
     float build_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last oxpt_build_scene: phases, wall, tree, launches
@@ -693,6 +697,7 @@ oxpt_status oxpt_destroy(oxpt_ctx* c) {
     if (c->ready) cudaEventDestroy(c->ready);
     for (cudaEvent_t ev : c->marks) cudaEventDestroy(ev);
     if (c->bgraph) cudaGraphExecDestroy(c->bgraph);
+    if (c->bgraph_alt) cudaGraphExecDestroy(c->bgraph_alt);
     if (c->dev_tally) cudaFree(c->dev_tally);
     if (c->capture) cudaStreamDestroy(c->capture);
     for (void* p : ptrs)
@@ -1670,8 +1675,14 @@ oxpt_status batch_graph_run(oxpt_ctx* e, const std::vector<oxd::WaveArgs>& args,
             key.insert(key.end(), {(uint64_t)(uintptr_t)c->accum, c->w, pc.base, pc.y0, pc.rows, pc.count});
         }
     }
+    if ((key != e->bgraph_key || !e->bgraph) && e->bgraph_alt && key == e->bgraph_alt_key) {
+        std::swap(e->bgraph, e->bgraph_alt);
+        std::swap(e->bgraph_key, e->bgraph_alt_key);
+    }
     if (key != e->bgraph_key || !e->bgraph) {
-        if (e->bgraph) cudaGraphExecDestroy(e->bgraph);
+        if (e->bgraph_alt) cudaGraphExecDestroy(e->bgraph_alt);
+        e->bgraph_alt = e->bgraph;
+        e->bgraph_alt_key = std::move(e->bgraph_key);
         e->bgraph = nullptr;
         e->bgraph_key.clear();
         cudaGraph_t g = nullptr;

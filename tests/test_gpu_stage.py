@@ -126,3 +126,29 @@ def test_stage_rejects_bad_input(pkg):
     d.geom_words = 4
     assert L.oxpt_stage_scene(c.h, C.byref(d), pa.tables.ctypes.data, pa.tables.size) == N.E_INVALID
     c.close()
+
+
+def test_restaging_one_scene_reuses_both_step_graphs(pkg):
+    """A renderer that re-stages the same scene every step alternates
+    between the context's two buffer sets: each set keeps its own step
+    graph, so after the first two steps nothing is captured again, and
+    every step is the same frame."""
+    N = pkg._native
+    L = N.lib()
+    pa = _prepared(pkg, "a")
+    c = Ctx(N)
+    t = N.Tuning()
+    L.oxpt_get_tuning(c.h, C.byref(t))
+    t.mode, t.graphs = 2, 1
+    c.ok(L.oxpt_set_tuning(c.h, C.byref(t)))
+    frames = []
+    for _ in range(6):
+        c.stage(pa)
+        c.refine(pa)
+        frames.append(c.accum())
+    builds = C.c_uint64()
+    c.ok(L.oxpt_diag_graph_builds(c.h, C.byref(builds)))
+    assert builds.value == 2
+    for f in frames[1:]:
+        assert np.array_equal(f.view(np.uint32), frames[0].view(np.uint32))
+    c.close()
