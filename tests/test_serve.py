@@ -182,3 +182,60 @@ def test_batched_loop_beats_serial_plain_on_a_loaded_stream():
     serial = mod.run_serial(eb, reqs, clock=cb, sleep=cb.sleep)
     assert served.msamples_per_s() > serial.msamples_per_s()
     assert served.percentile(99) < serial.percentile(99)
+
+
+class _View:
+    """Stands in for a tracer view: records what the executor asks of it."""
+    made = 0
+
+    def __init__(self, owner):
+        _View.made += 1
+        self.owner, self.calls = owner, []
+
+    def sync_view(self, opts):
+        self.calls.append(("sync", opts))
+
+    def set_camera(self, eye=None, target=None):
+        self.calls.append(("camera", eye))
+
+    def reset(self):
+        self.calls.append(("reset",))
+
+    def refine(self, n):
+        self.calls.append(("refine", n))
+
+    def finish(self):
+        self.calls.append(("finish",))
+
+
+class _Owner:
+    def view(self):
+        return _View(self)
+
+
+def test_gpu_executor_keeps_closed_views_per_scene():
+    """Closed sessions' views wait for the next request on their scene: a
+    reused view is reset and its camera override cleared, at most
+    `idle_views` wait per scene, and views that traced on their own (the
+    serial baseline's) are not kept."""
+    mod = _serve()
+    _View.made = 0
+    owners = [_Owner(), _Owner()]
+    ex = mod.GpuExecutor(pkg=None, owners=owners, options=lambda r: (r.width, r.height), executor=object(),
+                         idle_views=1)
+    r0 = mod.Request(0, 0.0, 0, 64, 64, 4, camera=((1.0, 2.0, 3.0), (0.0, 0.0, 0.0)))
+    v0 = ex.open(r0)
+    ex.close(v0)
+    v1 = ex.open(mod.Request(1, 0.0, 0, 32, 32, 4))          # same scene: the kept view
+    assert v1 is v0 and _View.made == 1
+    assert ("reset",) in v1.calls and ("camera", None) in v1.calls
+    v2 = ex.open(mod.Request(2, 0.0, 1, 32, 32, 4))          # another scene: a new view
+    assert v2 is not v0 and _View.made == 2
+    v3 = ex.open(mod.Request(3, 0.0, 0, 32, 32, 4))          # scene 0's kept view is in use
+    assert _View.made == 3
+    ex.close(v1)
+    ex.close(v3)                                             # one kept per scene
+    assert len(ex.pool[0]) == 1
+    ex.refine_alone(v2, 4)
+    ex.close(v2)                                             # traced alone: not kept
+    assert not ex.pool.get(1)
