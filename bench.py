@@ -100,6 +100,9 @@ def parse():
     ap.add_argument("--spp-scale", type=int, default=16,
                     help="serve workload: spp targets {4..1024} divided by this (one GPU cannot keep up with the "
                          "full stream)")
+    ap.add_argument("--nrc-plain-training", default="0,16", help="nrc workload: comma list of counts of first "
+                    "frames rendered as plain frames whose every path trains the cache (0: cache frames from the "
+                    "first); one arm per pair with --nrc-frames-per-wave")
     ap.add_argument("--serve-idle-views", type=int, default=2, help="serve workload: closed sessions' views kept "
                     "per scene for the next request (0: every session makes and frees its own)")
     ap.add_argument("--frames", type=int, default=512, help="nrc workload: frames of 1 spp")
@@ -912,22 +915,41 @@ def run_nrc(a):
 
     frame_ms = lambda c: 1e3 * c[-1]["seconds"] / c[-1]["frames"]
     runs = {}
-    for per_wave in [int(x) for x in a.nrc_frames_per_wave.split(",")]:
+    arms = [(int(g), int(w)) for g in a.nrc_frames_per_wave.split(",") for w in a.nrc_plain_training.split(",")]
+    for per_wave, warm in arms:
         nt = tracer()
         cache = RadianceCache(nt)
         cache.configure(train_one_in=a.nrc_train_one_in, query_bounce=a.nrc_query_bounce, spread=a.nrc_spread,
                         frames_per_wave=per_wave)
+        state = {"frames": 0}
+
+        def cache_step(n):
+            # the first `warm` frames: every path a training path, so the
+            # frames are the plain tracer's while the cache learns
+            while n > 0:
+                if state["frames"] < warm:
+                    m = min(n, warm - state["frames"])
+                    cache.configure(train_one_in=1, train_suffix=0)
+                    cache.refine(m)
+                    cache.configure(train_one_in=a.nrc_train_one_in, train_suffix=4)
+                else:
+                    m = n
+                    cache.refine(m)
+                state["frames"] += m
+                n -= m
 
         def untrained(n):
             cache.configure(train=0)
             cache.refine(n)
             cache.configure(train=1)
+            state["frames"] = 0
 
-        curve = progress(nt, lambda n: cache.refine(n), untrained)
+        curve = progress(nt, cache_step, untrained)
         q, smp = cache.frame_counts()
-        runs[per_wave] = {"curve": curve, "queries": q, "samples": smp, "seconds_to_35db": time_to(curve, 35.0),
-                          "ms_per_frame": frame_ms(curve),
-                          "kernel_ms_per_frame": breakdown(nt, lambda n: cache.refine(n))}
+        key = str(per_wave) if not warm else f"{per_wave}+plain{warm}"
+        runs[key] = {"per_wave": per_wave, "plain_training_frames": warm, "curve": curve, "queries": q,
+                     "samples": smp, "seconds_to_35db": time_to(curve, 35.0), "ms_per_frame": frame_ms(curve),
+                     "kernel_ms_per_frame": breakdown(nt, lambda n: cache.refine(n))}
         del nt, cache
     best = min(runs, key=lambda g: runs[g]["seconds_to_35db"] if runs[g]["seconds_to_35db"] else 1e30)
     nrc_curve, q, smp = runs[best]["curve"], runs[best]["queries"], runs[best]["samples"]
@@ -949,14 +971,16 @@ def run_nrc(a):
                                 f"bounce {a.nrc_query_bounce} when the path spread exceeds {a.nrc_spread} x the "
                                 "primary vertex's, "
                                 f"1 in {a.nrc_train_one_in} paths trains (suffix of 4 bounces into the cache), "
-                                f"<= 65536 samples and one Adam step (lr 1e-2) per wave of {best} frame(s)",
+                                f"<= 65536 samples and one Adam step (lr 1e-2) per wave of {runs[best]['per_wave']} "
+                                f"frame(s); the first {runs[best]['plain_training_frames']} frames plain, every path "
+                                "training",
                        "timing": "host wall clock with a device sync per checkpoint; one untimed call of every chunk size first"},
             "plain_seconds_to_35db": tp, "ratio_to_plain": (tn / tp) if (tn and tp) else None,
             "plain_ms_per_frame": frame_ms(plain_curve), "cache_ms_per_frame": frame_ms(nrc_curve),
             "plain": plain_curve, "cache": nrc_curve,
             "last_frame_queries": q, "last_frame_training_samples": smp,
             "kernel_ms_per_frame": {"plain": plain_ms, "cache": cache_ms},
-            "frames_per_wave": best,
+            "frames_per_wave": runs[best]["per_wave"], "plain_training_frames": runs[best]["plain_training_frames"],
             "by_frames_per_wave": {str(g): {"seconds_to_35db": r["seconds_to_35db"], "ms_per_frame": r["ms_per_frame"],
                                             "psnr_db_last": r["curve"][-1]["psnr_db"],
                                             "rel_mse_last": r["curve"][-1]["rel_mse"],
