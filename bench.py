@@ -929,9 +929,7 @@ def run_nrc(a):
             while n > 0:
                 if state["frames"] < warm:
                     m = min(n, warm - state["frames"])
-                    cache.configure(train_one_in=1, train_suffix=0)
-                    cache.refine(m)
-                    cache.configure(train_one_in=a.nrc_train_one_in, train_suffix=4)
+                    cache.refine_training(m)
                 else:
                     m = n
                     cache.refine(m)

@@ -69,6 +69,18 @@ class RadianceCache:
             _raise(st, N.lib().oxpt_tracer_last_error(t._h).decode())
         return l.value if loss else None
 
+    def refine_training(self, frames: int, loss: bool = False) -> Optional[float]:
+        """`frames` frames whose every path is a training path that runs to
+        its end: the frames are the plain tracer's (bit for bit) while the
+        cache learns from all of them. Rendering the first frames this way
+        keeps an untrained cache's predictions out of the average."""
+        saved = (self.cfg.train_one_in, self.cfg.train_suffix)
+        self.configure(train_one_in=1, train_suffix=0)
+        try:
+            return self.refine(frames, loss)
+        finally:
+            self.configure(train_one_in=saved[0], train_suffix=saved[1])
+
     def frame_counts(self):
         q, s = N.u32(), N.u32()
         self._check(N.lib().oxpt_nrc_frame_counts(self._h, C.byref(q), C.byref(s)))

@@ -211,6 +211,18 @@ def test_training_paths_are_the_plain_tracer(pkg):
     assert q == 0 and s > 100
 
 
+def test_training_frames_helper_is_the_plain_tracer_and_restores_the_config(pkg):
+    from oxideav_render_vulkan_b200.nrc import RadianceCache
+    t = _tracer(pkg)
+    cache = RadianceCache(t)
+    cache.configure(train_one_in=4, train_suffix=4)
+    cache.refine_training(2)
+    plain = _tracer(pkg)
+    plain.refine(2)
+    assert np.array_equal(t.read_accum().view(np.uint32), plain.read_accum().view(np.uint32))
+    assert (cache.cfg.train_one_in, cache.cfg.train_suffix) == (4, 4)
+
+
 def test_path_spread_decides_where_paths_end(pkg):
     """The path-spread heuristic: a spread no path reaches ends no path
     (the frames are the plain tracer's, bit for bit); the default ends
